@@ -1,0 +1,42 @@
+/*
+ * Extensions of the vkzg C API exported by this library.  None of these
+ * replaces a reference function; each says what in the reference it relates to.
+ */
+#ifndef VKZG_B200_H
+#define VKZG_B200_H
+
+#include "vkzg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Generates the FK20 setup tables on the GPU from 4096 compressed G1 monomial
+ * points ([tau^i]G1, 48 bytes each) and writes them to `out_path` in the
+ * reference's precomputed_tables.bin format (src/precomputed_tables.cpp:16-58),
+ * which the reference ships prebuilt and its Java binding extracts to
+ * $VKZG_TABLES_PATH (Vkzg.java:80-93).  A synthetic setup is selected the same
+ * way: generate its file, point VKZG_TABLES_PATH at it.
+ */
+vkzg_result vkzg_b200_write_tables(const uint8_t *g1_monomial_compressed, const char *out_path);
+
+/* Where the prover's tables came from: "file:<path>" or "generated:<setup path>". */
+const char *vkzg_b200_prover_tables_source(const vkzg_prover *p);
+
+/*
+ * Per-stage device time of the last proof or recovery chunk, in milliseconds,
+ * from CUDA events (the reference's bench/profile.cpp wall-clocks each stage by
+ * flushing the queue between dispatches, src/profile.h:12-28).  Fills up to
+ * `cap` entries and returns the number of stages; names via
+ * vkzg_b200_stage_name.  Timing is recorded only while enabled.
+ */
+void vkzg_b200_set_stage_timing(vkzg_prover *p, int enabled);
+int vkzg_b200_last_stage_times(const vkzg_prover *p, int recovery, double *ms, int cap);
+const char *vkzg_b200_stage_name(int recovery, int i);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* VKZG_B200_H */

@@ -1,0 +1,103 @@
+// Host build of the device arithmetic headers (the PTX carry chains run on the
+// host through their emulated carry flag), exposed to tests/test_host_arith.py.
+#include "../vkzg_b200/csrc/curve.cuh"
+
+#include <string.h>
+
+using namespace vkzg;
+
+extern "C" {
+void shim_fp_mul(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fp x, y;
+    memcpy(x.v, a, 48);
+    memcpy(y.v, b, 48);
+    memcpy(r, fp_mul(x, y).v, 48);
+}
+void shim_fp_add(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fp x, y;
+    memcpy(x.v, a, 48);
+    memcpy(y.v, b, 48);
+    memcpy(r, fp_add(x, y).v, 48);
+}
+void shim_fp_sub(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fp x, y;
+    memcpy(x.v, a, 48);
+    memcpy(y.v, b, 48);
+    memcpy(r, fp_sub(x, y).v, 48);
+}
+void shim_fr_mul(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fr x, y;
+    memcpy(x.v, a, 32);
+    memcpy(y.v, b, 32);
+    memcpy(r, fr_mul(x, y).v, 32);
+}
+void shim_fr_add(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fr x, y;
+    memcpy(x.v, a, 32);
+    memcpy(y.v, b, 32);
+    memcpy(r, fr_add(x, y).v, 32);
+}
+void shim_fr_sub(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fr x, y;
+    memcpy(x.v, a, 32);
+    memcpy(y.v, b, 32);
+    memcpy(r, fr_sub(x, y).v, 32);
+}
+void shim_fr_from_raw(const uint32_t *a, uint32_t *r) {
+    Fr x;
+    memcpy(x.v, a, 32);
+    memcpy(r, fr_from_canonical(x).v, 32);
+}
+void shim_fp_inv(const uint32_t *a, uint32_t *r) {
+    Fp x;
+    memcpy(x.v, a, 48);
+    memcpy(r, fp_inv(x).v, 48);
+}
+void shim_fr_inv(const uint32_t *a, uint32_t *r) {
+    Fr x;
+    memcpy(x.v, a, 32);
+    memcpy(r, fr_inv(x).v, 32);
+}
+// compressed in -> (2 P + Q) compressed out, through dbl / add / madd
+int shim_g1_ops(const uint8_t *p48, const uint8_t *q48, uint8_t *out_dbl_add, uint8_t *out_madd) {
+    G1A p, q;
+    if (!g1_decompress(p, p48) || !g1_decompress(q, q48)) return -1;
+    const G1J pj = g1_from_affine(p);
+    const G1J r1 = g1_add(g1_dbl(pj), g1_from_affine(q));
+    const G1J r2 = g1_madd(g1_add(pj, pj), q);
+    const G1J rs[2] = {r1, r2};
+    uint8_t *outs[2] = {out_dbl_add, out_madd};
+    for (int k = 0; k < 2; k++) {
+        G1A a;
+        if (fp_is_zero(rs[k].z)) {
+            a.x = fp_zero();
+            a.y = fp_zero();
+        } else {
+            const Fp zi = fp_inv(rs[k].z), z2 = fp_sqr(zi);
+            a.x = fp_mul(rs[k].x, z2);
+            a.y = fp_mul(rs[k].y, fp_mul(z2, zi));
+        }
+        g1_compress(outs[k], a);
+    }
+    return 0;
+}
+// k * P (canonical scalar as 8 LE words)
+int shim_g1_mul(const uint8_t *p48, const uint32_t *k, uint8_t *out48) {
+    G1A p;
+    if (!g1_decompress(p, p48)) return -1;
+    Fr s;
+    memcpy(s.v, k, 32);
+    const G1J r = g1_mul_scalar(g1_from_affine(p), s);
+    G1A a;
+    if (fp_is_zero(r.z)) {
+        a.x = fp_zero();
+        a.y = fp_zero();
+    } else {
+        const Fp zi = fp_inv(r.z), z2 = fp_sqr(zi);
+        a.x = fp_mul(r.x, z2);
+        a.y = fp_mul(r.y, fp_mul(z2, zi));
+    }
+    g1_compress(out48, a);
+    return 0;
+}
+}

@@ -1,0 +1,80 @@
+"""The device arithmetic headers (field.cuh, curve.cuh) built for the host --
+the PTX carry-chain multiply runs with its carry flag emulated -- checked
+against Python integers and the oracle (CPU only)."""
+import ctypes
+import os
+import random
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+P_MOD = 0x1A0111EA397FE69A4B1BA7B6434BACD764774B84F38512BF6730D2A0F6B0F6241EABFFFEB153FFFFB9FEFFFFFFFFAAAB
+R_MOD = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+
+
+@pytest.fixture(scope="module")
+def shim(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("shim") / "libshim.so")
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-o", out,
+                           os.path.join(ROOT, "tests", "host_shim.cpp")])
+    return ctypes.CDLL(out)
+
+
+def words(x, n):
+    return (ctypes.c_uint32 * n)(*[(x >> (32 * i)) & 0xFFFFFFFF for i in range(n)])
+
+
+def value(a, n):
+    return sum(a[i] << (32 * i) for i in range(n))
+
+
+@pytest.mark.parametrize("field", ["fp", "fr"])
+def test_field_ops(shim, field):
+    mod, n, radix = (P_MOD, 12, 1 << 384) if field == "fp" else (R_MOD, 8, 1 << 256)
+    rinv = pow(radix, -1, mod)
+    rng = random.Random(7)
+    edge = [0, 1, 2, mod - 1, mod - 2, radix % mod, radix * radix % mod, mod // 2, (mod + 1) // 2]
+    vals = edge + [rng.randrange(mod) for _ in range(2000)]
+    out = (ctypes.c_uint32 * n)()
+    for k, a in enumerate(vals):
+        b = vals[(7 * k + 3) % len(vals)]
+        getattr(shim, f"shim_{field}_mul")(words(a, n), words(b, n), out)
+        assert value(out, n) == a * b * rinv % mod
+        getattr(shim, f"shim_{field}_add")(words(a, n), words(b, n), out)
+        assert value(out, n) == (a + b) % mod
+        getattr(shim, f"shim_{field}_sub")(words(a, n), words(b, n), out)
+        assert value(out, n) == (a - b) % mod
+    for a in vals[1:60]:
+        if a == 0:
+            continue
+        getattr(shim, f"shim_{field}_inv")(words(a * radix % mod, n), out)
+        assert value(out, n) == pow(a, -1, mod) * radix % mod
+
+
+def test_fr_from_raw_noncanonical(shim):
+    """Raw 256-bit words (cells are not canonicity-checked) reduce mod r."""
+    rng = random.Random(3)
+    out = (ctypes.c_uint32 * 8)()
+    for v in [R_MOD, R_MOD + 5, (1 << 256) - 1, 2 * R_MOD - 1] + [rng.randrange(1 << 256) for _ in range(500)]:
+        shim.shim_fr_from_raw(words(v, 8), out)
+        assert value(out, 8) == v % R_MOD * (1 << 256) % R_MOD
+
+
+def test_curve_ops(shim, oracle, mainnet_setup):
+    pts = [mainnet_setup[48 * i:48 * (i + 1)] for i in (0, 1, 17, 4095)]
+    for p in pts:
+        for q in pts:
+            o1 = ctypes.create_string_buffer(48)
+            o2 = ctypes.create_string_buffer(48)
+            assert shim.shim_g1_ops(p, q, o1, o2) == 0
+            _, two_p = oracle.g1_mul(p, (2).to_bytes(32, "big"))
+            _, want = oracle.g1_add(two_p, q)
+            assert o1.raw == want and o2.raw == want
+    rng = random.Random(5)
+    for _ in range(5):
+        k = rng.randrange(R_MOD)
+        o = ctypes.create_string_buffer(48)
+        assert shim.shim_g1_mul(pts[1], words(k, 8), o) == 0
+        _, want = oracle.g1_mul(pts[1], k.to_bytes(32, "big"))
+        assert o.raw == want

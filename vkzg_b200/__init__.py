@@ -1,0 +1,252 @@
+"""vkzg on one NVIDIA B200: EIP-7594 cell KZG proofs and cell recovery.
+
+The product is libvkzg.so (C ABI of include/vkzg.h, hand-written CUDA for
+sm_100a).  This module loads it with ctypes and mirrors the reference's Java
+binding (bindings/java/src/main/java/vkzg/Vkzg.java): a global prover opened
+with init(), computeCellKzgProofsBatch / recoverCellsBatch taking packed byte
+buffers, VkzgException(code, message) on any nonzero status.  Prover is the
+same interface as an object, for callers that want more than one.
+
+There is no CPU fallback: if libvkzg.so is missing or the GPU is unusable,
+every entry point raises.
+"""
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvkzg.so")
+
+FIELD_ELEMENTS_PER_BLOB = 4096
+BYTES_PER_FIELD_ELEMENT = 32
+BYTES_PER_BLOB = FIELD_ELEMENTS_PER_BLOB * BYTES_PER_FIELD_ELEMENT
+CELL_PROOFS_PER_BLOB = 128
+BYTES_PER_PROOF = 48
+FIELD_ELEMENTS_PER_CELL = 64
+BYTES_PER_CELL = FIELD_ELEMENTS_PER_CELL * BYTES_PER_FIELD_ELEMENT
+BYTES_PER_EXT_BLOB = CELL_PROOFS_PER_BLOB * BYTES_PER_CELL
+
+OK, ERR_BADARGS, ERR_MALLOC, ERR_IO, ERR_SETUP, ERR_GPU, ERR_INVALID_BLOB = range(7)
+
+# every symbol declared in include/vkzg.h and include/vkzg_b200.h
+EXPORTED_SYMBOLS = (
+    "vkzg_error_string", "vkzg_options_default", "vkzg_prover_new", "vkzg_prover_free",
+    "vkzg_prover_device_name", "vkzg_prover_gpu_core_count", "vkzg_compute_proofs_batch",
+    "vkzg_recover_cells_batch",
+    "vkzg_b200_write_tables", "vkzg_b200_prover_tables_source", "vkzg_b200_set_stage_timing",
+    "vkzg_b200_last_stage_times", "vkzg_b200_stage_name",
+)
+
+
+class VkzgException(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("max_batch_size", ctypes.c_uint32)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def library():
+    """Loads libvkzg.so (raises OSError when it has not been built)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise OSError(f"{LIB_PATH} not built; run python -m vkzg_b200.build")
+            L = ctypes.CDLL(LIB_PATH)
+            vp, u8p = ctypes.c_void_p, ctypes.c_void_p
+            L.vkzg_error_string.argtypes = [ctypes.c_int]
+            L.vkzg_error_string.restype = ctypes.c_char_p
+            L.vkzg_options_default.argtypes = [ctypes.POINTER(_Options)]
+            L.vkzg_options_default.restype = None
+            L.vkzg_prover_new.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_Options)]
+            L.vkzg_prover_new.restype = ctypes.c_int
+            L.vkzg_prover_free.argtypes = [vp]
+            L.vkzg_prover_free.restype = None
+            L.vkzg_prover_device_name.argtypes = [vp]
+            L.vkzg_prover_device_name.restype = ctypes.c_char_p
+            L.vkzg_prover_gpu_core_count.argtypes = [vp]
+            L.vkzg_prover_gpu_core_count.restype = ctypes.c_uint32
+            L.vkzg_compute_proofs_batch.argtypes = [vp, u8p, u8p, ctypes.c_size_t]
+            L.vkzg_compute_proofs_batch.restype = ctypes.c_int
+            L.vkzg_recover_cells_batch.argtypes = [vp, u8p, u8p, u8p, ctypes.c_size_t]
+            L.vkzg_recover_cells_batch.restype = ctypes.c_int
+            L.vkzg_b200_write_tables.argtypes = [u8p, ctypes.c_char_p]
+            L.vkzg_b200_write_tables.restype = ctypes.c_int
+            L.vkzg_b200_prover_tables_source.argtypes = [vp]
+            L.vkzg_b200_prover_tables_source.restype = ctypes.c_char_p
+            L.vkzg_b200_set_stage_timing.argtypes = [vp, ctypes.c_int]
+            L.vkzg_b200_set_stage_timing.restype = None
+            L.vkzg_b200_last_stage_times.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+            L.vkzg_b200_last_stage_times.restype = ctypes.c_int
+            L.vkzg_b200_stage_name.argtypes = [ctypes.c_int, ctypes.c_int]
+            L.vkzg_b200_stage_name.restype = ctypes.c_char_p
+            _lib = L
+    return _lib
+
+
+def error_string(code):
+    return library().vkzg_error_string(code).decode()
+
+
+def _check(rc):
+    if rc != OK:
+        raise VkzgException(rc, error_string(rc))
+
+
+def _ptr(buf):
+    """Address of a bytes-like / numpy / ctypes buffer without copying when possible."""
+    if buf is None:
+        return None
+    if hasattr(buf, "ctypes"):  # numpy
+        return buf.ctypes.data_as(ctypes.c_void_p)
+    if isinstance(buf, (bytearray, memoryview)):
+        mv = memoryview(buf)
+        if mv.readonly:
+            return ctypes.cast(ctypes.c_char_p(bytes(mv)), ctypes.c_void_p)
+        return ctypes.addressof((ctypes.c_char * mv.nbytes).from_buffer(mv))
+    if isinstance(buf, bytes):
+        return ctypes.cast(ctypes.c_char_p(buf), ctypes.c_void_p)
+    if isinstance(buf, int):
+        return ctypes.c_void_p(buf)
+    return ctypes.cast(buf, ctypes.c_void_p)
+
+
+class Prover:
+    """One vkzg_prover (a CUDA stream, device-resident setup tables, a working set)."""
+
+    def __init__(self, max_batch_size=0):
+        L = library()
+        opts = _Options()
+        L.vkzg_options_default(ctypes.byref(opts))
+        if max_batch_size:
+            opts.max_batch_size = int(max_batch_size)
+        h = ctypes.c_void_p()
+        _check(L.vkzg_prover_new(ctypes.byref(h), ctypes.byref(opts)))
+        self._h = h
+        self._lib = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.vkzg_prover_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_name(self):
+        return self._lib.vkzg_prover_device_name(self._h).decode()
+
+    def gpu_core_count(self):
+        return int(self._lib.vkzg_prover_gpu_core_count(self._h))
+
+    def tables_source(self):
+        return self._lib.vkzg_b200_prover_tables_source(self._h).decode()
+
+    def compute_proofs_raw(self, proofs_out, blobs, n):
+        """C-ABI call on caller-owned buffers (numpy arrays or addresses); returns the status."""
+        return self._lib.vkzg_compute_proofs_batch(self._h, _ptr(proofs_out), _ptr(blobs), n)
+
+    def recover_cells_raw(self, cells_out, cells, present, n):
+        return self._lib.vkzg_recover_cells_batch(self._h, _ptr(cells_out), _ptr(cells), _ptr(present), n)
+
+    def compute_cell_kzg_proofs_batch(self, blobs, blob_count):
+        """Vkzg.computeCellKzgProofsBatch (Vkzg.java:204-229)."""
+        if len(blobs) != blob_count * BYTES_PER_BLOB:
+            raise ValueError(f"blobs length must be blob_count * {BYTES_PER_BLOB}")
+        out = bytearray(blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF)
+        src = bytes(blobs)
+        _check(self._lib.vkzg_compute_proofs_batch(self._h, _ptr(out) if out else None, _ptr(src), blob_count))
+        return bytes(out)
+
+    def recover_cells_batch(self, cells, cell_present, blob_count):
+        """Vkzg.recoverCellsBatch (Vkzg.java:248-281)."""
+        if len(cells) != blob_count * BYTES_PER_EXT_BLOB:
+            raise ValueError(f"cells length must be blob_count * {BYTES_PER_EXT_BLOB}")
+        if len(cell_present) != blob_count * CELL_PROOFS_PER_BLOB:
+            raise ValueError(f"cell_present length must be blob_count * {CELL_PROOFS_PER_BLOB}")
+        out = bytearray(len(cells))
+        c, pr = bytes(cells), bytes(cell_present)
+        _check(self._lib.vkzg_recover_cells_batch(self._h, _ptr(out) if out else None, _ptr(c), _ptr(pr),
+                                                  blob_count))
+        return bytes(out)
+
+    def set_stage_timing(self, enabled):
+        self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)
+
+    def last_stage_times(self, recovery=False):
+        buf = (ctypes.c_double * 32)()
+        n = self._lib.vkzg_b200_last_stage_times(self._h, 1 if recovery else 0, buf, 32)
+        return {self._lib.vkzg_b200_stage_name(1 if recovery else 0, i).decode(): buf[i] for i in range(n)}
+
+
+def write_tables(g1_monomial_compressed, out_path):
+    """Generates the FK20 tables on the GPU from a G1 monomial setup and writes them
+    in the reference's precomputed_tables.bin format."""
+    setup = bytes(g1_monomial_compressed)
+    if len(setup) != 4096 * 48:
+        raise ValueError("expected 4096 compressed G1 points")
+    _check(library().vkzg_b200_write_tables(_ptr(setup), out_path.encode()))
+
+
+# ---------------------------------------------------------------- Vkzg.java mirror
+_global = None
+_global_lock = threading.Lock()
+
+
+def init(max_batch_size=0):
+    """Vkzg.init (Vkzg.java:164-184)."""
+    global _global
+    with _global_lock:
+        if _global is not None:
+            raise RuntimeError("already initialized")
+        _global = Prover(max_batch_size)
+
+
+def deinit():
+    global _global
+    with _global_lock:
+        _loaded().close()
+        _global = None
+
+
+def _loaded():
+    if _global is None:
+        raise RuntimeError("not initialized; call init() first")
+    return _global
+
+
+def computeCellKzgProofsBatch(blobs, blob_count):  # noqa: N802 (reference name)
+    with _global_lock:
+        return _loaded().compute_cell_kzg_proofs_batch(blobs, blob_count)
+
+
+def recoverCellsBatch(cells, cell_present, blob_count):  # noqa: N802
+    with _global_lock:
+        return _loaded().recover_cells_batch(cells, cell_present, blob_count)
+
+
+def deviceName():  # noqa: N802
+    with _global_lock:
+        return _loaded().device_name()
+
+
+def gpuCoreCount():  # noqa: N802
+    with _global_lock:
+        return _loaded().gpu_core_count()

@@ -1,0 +1,161 @@
+// Device helpers shared by the proof, recovery and setup kernels: 16-byte
+// vector loads/stores of field elements and points, block-wide batch
+// inversion, and radix-2 NTT stages over a tile in shared memory.
+#pragma once
+
+#include "curve.cuh"
+
+namespace vkzg {
+
+// ------------------------------------------------------------ loads/stores
+template <typename T>
+__device__ __forceinline__ T ld_vec(const T *p) {
+    static_assert(sizeof(T) % 16 == 0, "16-byte multiple");
+    T r;
+    const uint4 *s = reinterpret_cast<const uint4 *>(p);
+    uint4 *d = reinterpret_cast<uint4 *>(&r);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); i++) d[i] = s[i];
+    return r;
+}
+// read-only path (table data that no kernel in flight writes)
+template <typename T>
+__device__ __forceinline__ T ldg_vec(const T *p) {
+    T r;
+    const uint4 *s = reinterpret_cast<const uint4 *>(p);
+    uint4 *d = reinterpret_cast<uint4 *>(&r);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); i++) d[i] = __ldg(s + i);
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ void st_vec(T *p, const T &v) {
+    const uint4 *s = reinterpret_cast<const uint4 *>(&v);
+    uint4 *d = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); i++) d[i] = s[i];
+}
+
+__device__ __forceinline__ G1J g1_shfl_down(const G1J &p, int delta) {
+    G1J r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+        r.x.v[i] = __shfl_down_sync(0xffffffffu, p.x.v[i], delta);
+        r.y.v[i] = __shfl_down_sync(0xffffffffu, p.y.v[i], delta);
+        r.z.v[i] = __shfl_down_sync(0xffffffffu, p.z.v[i], delta);
+    }
+    return r;
+}
+
+// ------------------------------------------------------- batch inversion
+// Inverts one Fp per thread across a block of NT threads (power of two) with a
+// product tree in shared memory: NT-1 multiplies up, one Fermat inversion at
+// the root, 2(NT-1) down.  Zero inputs must be replaced by one by the caller.
+// `tree` holds 2*NT Fp.
+template <int NT>
+__device__ Fp block_batch_inverse_fp(const Fp &z, Fp *tree) {
+    const int t = threadIdx.x;
+    // leaves at [NT, 2NT), node k has children 2k, 2k+1, root at 1
+    st_vec(&tree[NT + t], z);
+    __syncthreads();
+    for (int width = NT / 2; width >= 1; width >>= 1) {
+        if (t < width) {
+            const int k = width + t;
+            st_vec(&tree[k], fp_mul(ld_vec(&tree[2 * k]), ld_vec(&tree[2 * k + 1])));
+        }
+        __syncthreads();
+    }
+    if (t == 0) st_vec(&tree[1], fp_inv(ld_vec(&tree[1])));
+    __syncthreads();
+    // push inverses down: inv(child) = inv(parent) * sibling
+    for (int width = 1; width < NT; width <<= 1) {
+        if (t < width) {
+            const int k = width + t;
+            const Fp ip = ld_vec(&tree[k]);
+            const Fp l = ld_vec(&tree[2 * k]), r = ld_vec(&tree[2 * k + 1]);
+            st_vec(&tree[2 * k], fp_mul(ip, r));
+            st_vec(&tree[2 * k + 1], fp_mul(ip, l));
+        }
+        __syncthreads();
+    }
+    const Fp res = ld_vec(&tree[NT + t]);
+    __syncthreads();
+    return res;
+}
+
+template <int NT>
+__device__ Fr block_batch_inverse_fr(const Fr &z, Fr *tree) {
+    const int t = threadIdx.x;
+    st_vec(&tree[NT + t], z);
+    __syncthreads();
+    for (int width = NT / 2; width >= 1; width >>= 1) {
+        if (t < width) {
+            const int k = width + t;
+            st_vec(&tree[k], fr_mul(ld_vec(&tree[2 * k]), ld_vec(&tree[2 * k + 1])));
+        }
+        __syncthreads();
+    }
+    if (t == 0) st_vec(&tree[1], fr_inv(ld_vec(&tree[1])));
+    __syncthreads();
+    for (int width = 1; width < NT; width <<= 1) {
+        if (t < width) {
+            const int k = width + t;
+            const Fr ip = ld_vec(&tree[k]);
+            const Fr l = ld_vec(&tree[2 * k]), r = ld_vec(&tree[2 * k + 1]);
+            st_vec(&tree[2 * k], fr_mul(ip, r));
+            st_vec(&tree[2 * k + 1], fr_mul(ip, l));
+        }
+        __syncthreads();
+    }
+    const Fr res = ld_vec(&tree[NT + t]);
+    __syncthreads();
+    return res;
+}
+
+// ------------------------------------------------------------ NTT stages
+// roots: w_8192^(+-i), i < 8192 (Montgomery).  A transform of length n uses
+// w_len^j = roots[j * 8192 / len].
+//
+// DIT (Cooley-Tukey): bit-reversed input, natural output, lengths 2..n.
+// DIF (Gentleman-Sande): natural input, bit-reversed output, lengths n..2.
+// Each call runs stages [len_lo, len_hi] over `count` independent n-point
+// transforms laid out back to back in `s`, with all NT threads cooperating.
+template <int NT>
+__device__ void smem_dit(Fr *s, int log_n, int count, int len_lo, int len_hi, const Fr *__restrict__ roots) {
+    const int n = 1 << log_n;
+    const int total = (n >> 1) * count;
+    for (int len = len_lo; len <= len_hi; len <<= 1) {
+        const int h = len >> 1, stride = 8192 / len;
+        for (int q = threadIdx.x; q < total; q += NT) {
+            const int tr = q >> (log_n - 1), k = q & ((n >> 1) - 1);
+            const int blk = k / h, j = k - blk * h;
+            Fr *base = s + tr * n + blk * len + j;
+            const Fr x = ld_vec(base);
+            const Fr y = fr_mul(ld_vec(base + h), ldg_vec(&roots[j * stride]));
+            st_vec(base, fr_add(x, y));
+            st_vec(base + h, fr_sub(x, y));
+        }
+        __syncthreads();
+    }
+}
+
+template <int NT>
+__device__ void smem_dif(Fr *s, int log_n, int count, int len_hi, int len_lo, const Fr *__restrict__ roots) {
+    const int n = 1 << log_n;
+    const int total = (n >> 1) * count;
+    for (int len = len_hi; len >= len_lo; len >>= 1) {
+        const int h = len >> 1, stride = 8192 / len;
+        for (int q = threadIdx.x; q < total; q += NT) {
+            const int tr = q >> (log_n - 1), k = q & ((n >> 1) - 1);
+            const int blk = k / h, j = k - blk * h;
+            Fr *base = s + tr * n + blk * len + j;
+            const Fr x = ld_vec(base);
+            const Fr y = ld_vec(base + h);
+            st_vec(base, fr_add(x, y));
+            st_vec(base + h, fr_mul(fr_sub(x, y), ldg_vec(&roots[j * stride])));
+        }
+        __syncthreads();
+    }
+}
+
+} // namespace vkzg

@@ -1,0 +1,447 @@
+// BLS12-381 base field Fp (381-bit, 12 x 32-bit limbs) and scalar field Fr
+// (255-bit, 8 x 32-bit limbs), little-endian limbs in Montgomery form with
+// R = 2^384 / 2^256.  The memory image of a value is identical to the
+// reference's (src/shaders/field.glsl.inc:1-4), so its setup tables load as-is.
+//
+// Multiplication is word-serial Montgomery (CIOS).  On the device it is a PTX
+// carry chain: each 32x32 partial product is one mad.lo.cc / madc.hi.cc, with
+// the even-index and odd-index products of a row on two separate chains
+// (their 64-bit results never overlap, so a row is two passes of n
+// instructions instead of n wide multiplies plus carry fix-ups).  The same
+// code compiles for the host with the carry flag emulated in a local
+// variable, which is how the CPU tests check the exact instruction sequence
+// against the oracle.
+#pragma once
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define VK_HD __host__ __device__ __forceinline__
+#define VK_D __device__ __forceinline__
+#else
+#define VK_HD inline
+#define VK_D inline
+#endif
+
+namespace vkzg {
+
+// ------------------------------------------------------------- constants
+// p = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
+// r = 0x73eda753299d7d483339d80809a1d80553bda402fffe5bfeffffffff00000001
+#define VK_FP_P                                                                                       \
+    {0xffffaaabu, 0xb9feffffu, 0xb153ffffu, 0x1eabfffeu, 0xf6b0f624u, 0x6730d2a0u, 0xf38512bfu,         \
+     0x64774b84u, 0x434bacd7u, 0x4b1ba7b6u, 0x397fe69au, 0x1a0111eau}
+#define VK_FP_ONE                                                                                     \
+    {0x0002fffdu, 0x76090000u, 0xc40c0002u, 0xebf4000bu, 0x53c758bau, 0x5f489857u, 0x70525745u,         \
+     0x77ce5853u, 0xa256ec6du, 0x5c071a97u, 0xfa80e493u, 0x15f65ec3u}
+#define VK_FP_R2                                                                                      \
+    {0x1c341746u, 0xf4df1f34u, 0x09d104f1u, 0x0a76e6a6u, 0x4c95b6d5u, 0x8de5476cu, 0x939d83c0u,         \
+     0x67eb88a9u, 0xb519952du, 0x9a793e85u, 0x92cae3aau, 0x11988fe5u}
+#define VK_FP_N0 0xfffcfffdu
+#define VK_FR_P {0x00000001u, 0xffffffffu, 0xfffe5bfeu, 0x53bda402u, 0x09a1d805u, 0x3339d808u, 0x299d7d48u, 0x73eda753u}
+#define VK_FR_ONE {0xfffffffeu, 0x00000001u, 0x00034802u, 0x5884b7fau, 0xecbc4ff5u, 0x998c4fefu, 0xacc5056fu, 0x1824b159u}
+#define VK_FR_R2 {0xf3f29c6du, 0xc999e990u, 0x87925c23u, 0x2b6cedcbu, 0x7254398fu, 0x05d31496u, 0x9f59ff11u, 0x0748d9d9u}
+#define VK_FR_N0 0xffffffffu
+
+struct alignas(16) Fp {
+    uint32_t v[12];
+};
+struct alignas(16) Fr {
+    uint32_t v[8];
+};
+
+// Modulus words as immediates: a switch on a compile-time index lets the
+// compiler fold them into the instruction stream (no constant-bank loads).
+VK_HD constexpr uint32_t fp_p(int i) {
+    return i == 0 ? 0xffffaaabu : i == 1 ? 0xb9feffffu : i == 2 ? 0xb153ffffu : i == 3 ? 0x1eabfffeu
+         : i == 4 ? 0xf6b0f624u : i == 5 ? 0x6730d2a0u : i == 6 ? 0xf38512bfu : i == 7 ? 0x64774b84u
+         : i == 8 ? 0x434bacd7u : i == 9 ? 0x4b1ba7b6u : i == 10 ? 0x397fe69au : 0x1a0111eau;
+}
+VK_HD constexpr uint32_t fr_p(int i) {
+    return i == 0 ? 0x00000001u : i == 1 ? 0xffffffffu : i == 2 ? 0xfffe5bfeu : i == 3 ? 0x53bda402u
+         : i == 4 ? 0x09a1d805u : i == 5 ? 0x3339d808u : i == 6 ? 0x299d7d48u : 0x73eda753u;
+}
+template <int N>
+VK_HD constexpr uint32_t mod_word(int i) {
+    return N == 12 ? fp_p(i) : fr_p(i);
+}
+template <int N>
+VK_HD constexpr uint32_t mod_n0() {
+    return N == 12 ? VK_FP_N0 : VK_FR_N0;
+}
+
+// ------------------------------------------------------------- carry ops
+// PTX extended-precision primitives.  On the host, `cf` is the carry flag.
+#if defined(__CUDA_ARCH__)
+#define CARRY_DECL
+#define MAD_LO_CC(d, a, b, c) asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c))
+#define MADC_LO_CC(d, a, b, c) asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c))
+#define MADC_HI_CC(d, a, b, c) asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c))
+#define MADC_HI(d, a, b, c) asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c))
+#define ADD_CC(d, a, b) asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define ADDC_CC(d, a, b) asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define ADDC(d, a, b) asm volatile("addc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUB_CC(d, a, b) asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUBC_CC(d, a, b) asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUBC(d, a, b) asm volatile("subc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#else
+#define CARRY_DECL uint32_t cf = 0;
+#define MAD_LO_CC(d, a, b, c)                                                                         \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)((uint64_t)(a) * (b)) + (uint32_t)(c);                      \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 32);                                                                    \
+    } while (0)
+#define MADC_LO_CC(d, a, b, c)                                                                        \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)((uint64_t)(a) * (b)) + (uint32_t)(c) + cf;                 \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 32);                                                                    \
+    } while (0)
+#define MADC_HI_CC(d, a, b, c)                                                                        \
+    do {                                                                                              \
+        uint64_t _t = (((uint64_t)(a) * (b)) >> 32) + (uint32_t)(c) + cf;                             \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 32);                                                                    \
+    } while (0)
+#define MADC_HI(d, a, b, c)                                                                           \
+    do {                                                                                              \
+        d = (uint32_t)((((uint64_t)(a) * (b)) >> 32) + (uint32_t)(c) + cf);                           \
+    } while (0)
+#define ADD_CC(d, a, b)                                                                               \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)(a) + (uint32_t)(b);                                        \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 32);                                                                    \
+    } while (0)
+#define ADDC_CC(d, a, b)                                                                              \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)(a) + (uint32_t)(b) + cf;                                   \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 32);                                                                    \
+    } while (0)
+#define ADDC(d, a, b)                                                                                 \
+    do {                                                                                              \
+        d = (uint32_t)((uint64_t)(uint32_t)(a) + (uint32_t)(b) + cf);                                 \
+    } while (0)
+#define SUB_CC(d, a, b)                                                                               \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)(a) - (uint32_t)(b);                                        \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 63);                                                                    \
+    } while (0)
+#define SUBC_CC(d, a, b)                                                                              \
+    do {                                                                                              \
+        uint64_t _t = (uint64_t)(uint32_t)(a) - (uint32_t)(b) - cf;                                   \
+        d = (uint32_t)_t;                                                                             \
+        cf = (uint32_t)(_t >> 63);                                                                    \
+    } while (0)
+#define SUBC(d, a, b)                                                                                 \
+    do {                                                                                              \
+        d = (uint32_t)((uint64_t)(uint32_t)(a) - (uint32_t)(b) - cf);                                 \
+    } while (0)
+#endif
+
+// ------------------------------------------------------- generic n-limb ops
+// r = a + b mod m (a, b < m; m < 2^(32n-1) so the raw sum fits in n words).
+template <int N>
+VK_HD void mod_add(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+    CARRY_DECL
+    uint32_t t[N], s[N];
+    ADD_CC(t[0], a[0], b[0]);
+#pragma unroll
+    for (int i = 1; i < N; i++) ADDC_CC(t[i], a[i], b[i]);
+    SUB_CC(s[0], t[0], mod_word<N>(0));
+#pragma unroll
+    for (int i = 1; i < N; i++) SUBC_CC(s[i], t[i], mod_word<N>(i));
+    uint32_t borrow;
+    SUBC(borrow, 0u, 0u); // 0xffffffff when t < m
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = borrow ? t[i] : s[i];
+}
+
+// r = a - b mod m
+template <int N>
+VK_HD void mod_sub(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+    CARRY_DECL
+    uint32_t t[N];
+    SUB_CC(t[0], a[0], b[0]);
+#pragma unroll
+    for (int i = 1; i < N; i++) SUBC_CC(t[i], a[i], b[i]);
+    uint32_t mask;
+    SUBC(mask, 0u, 0u); // all ones on borrow
+    ADD_CC(r[0], t[0], mod_word<N>(0) & mask);
+#pragma unroll
+    for (int i = 1; i < N; i++) ADDC_CC(r[i], t[i], mod_word<N>(i) & mask);
+}
+
+// Montgomery product, CIOS.  Invariant: the running value t < 2m after each
+// row, and t + a*b_i + q*m < 2^(32(n+1)), so n+1 words hold it and the odd
+// chain's top word needs no carry-out.
+template <int N>
+VK_HD void mont_mul(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+    CARRY_DECL
+    uint32_t t[N + 1];
+#pragma unroll
+    for (int i = 0; i < N + 1; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint32_t bi = b[i];
+        // even products: lo -> t[j], hi -> t[j+1]
+        MAD_LO_CC(t[0], a[0], bi, t[0]);
+        MADC_HI_CC(t[1], a[0], bi, t[1]);
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            MADC_LO_CC(t[j], a[j], bi, t[j]);
+            MADC_HI_CC(t[j + 1], a[j], bi, t[j + 1]);
+        }
+        ADDC(t[N], t[N], 0u);
+        // odd products: lo -> t[j], hi -> t[j+1]
+        MAD_LO_CC(t[1], a[1], bi, t[1]);
+        MADC_HI_CC(t[2], a[1], bi, t[2]);
+#pragma unroll
+        for (int j = 3; j < N - 1; j += 2) {
+            MADC_LO_CC(t[j], a[j], bi, t[j]);
+            MADC_HI_CC(t[j + 1], a[j], bi, t[j + 1]);
+        }
+        MADC_LO_CC(t[N - 1], a[N - 1], bi, t[N - 1]);
+        MADC_HI(t[N], a[N - 1], bi, t[N]);
+        // reduction row
+        const uint32_t q = t[0] * mod_n0<N>();
+        MAD_LO_CC(t[0], q, mod_word<N>(0), t[0]);
+        MADC_HI_CC(t[1], q, mod_word<N>(0), t[1]);
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            MADC_LO_CC(t[j], q, mod_word<N>(j), t[j]);
+            MADC_HI_CC(t[j + 1], q, mod_word<N>(j), t[j + 1]);
+        }
+        ADDC(t[N], t[N], 0u);
+        MAD_LO_CC(t[1], q, mod_word<N>(1), t[1]);
+        MADC_HI_CC(t[2], q, mod_word<N>(1), t[2]);
+#pragma unroll
+        for (int j = 3; j < N - 1; j += 2) {
+            MADC_LO_CC(t[j], q, mod_word<N>(j), t[j]);
+            MADC_HI_CC(t[j + 1], q, mod_word<N>(j), t[j + 1]);
+        }
+        MADC_LO_CC(t[N - 1], q, mod_word<N>(N - 1), t[N - 1]);
+        MADC_HI(t[N], q, mod_word<N>(N - 1), t[N]);
+        // t[0] == 0: shift one word
+#pragma unroll
+        for (int j = 0; j < N; j++) t[j] = t[j + 1];
+        t[N] = 0;
+    }
+    // t < 2m < 2^(32n): one conditional subtraction
+    uint32_t s[N];
+    SUB_CC(s[0], t[0], mod_word<N>(0));
+#pragma unroll
+    for (int i = 1; i < N; i++) SUBC_CC(s[i], t[i], mod_word<N>(i));
+    uint32_t borrow;
+    SUBC(borrow, 0u, 0u);
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = borrow ? t[i] : s[i];
+}
+
+template <int N>
+VK_HD bool limbs_is_zero(const uint32_t *a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) acc |= a[i];
+    return acc == 0;
+}
+
+template <int N>
+VK_HD bool limbs_eq(const uint32_t *a, const uint32_t *b) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) acc |= a[i] ^ b[i];
+    return acc == 0;
+}
+
+// ------------------------------------------------------------------- Fp
+VK_HD Fp fp_zero() {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) r.v[i] = 0;
+    return r;
+}
+VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
+// On the device the 12-limb product is an out-of-line call by default: inlined,
+// every point formula becomes thousands of straight-line instructions (an
+// instruction-cache and compile-time cost); VKZG_FP_INLINE=1 inlines it.
+#ifndef VKZG_FP_INLINE
+#define VKZG_FP_INLINE 0
+#endif
+#if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
+__device__ __noinline__ Fp fp_mul_call(Fp a, Fp b) {
+    Fp r;
+    mont_mul<12>(r.v, a.v, b.v);
+    return r;
+}
+#endif
+VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
+#if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
+    return fp_mul_call(a, b);
+#else
+    Fp r;
+    mont_mul<12>(r.v, a.v, b.v);
+    return r;
+#endif
+}
+VK_HD Fp fp_sqr(const Fp &a) { return fp_mul(a, a); }
+VK_HD Fp fp_add(const Fp &a, const Fp &b) {
+    Fp r;
+    mod_add<12>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD Fp fp_sub(const Fp &a, const Fp &b) {
+    Fp r;
+    mod_sub<12>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD Fp fp_dbl(const Fp &a) { return fp_add(a, a); }
+VK_HD bool fp_is_zero(const Fp &a) { return limbs_is_zero<12>(a.v); }
+VK_HD bool fp_eq(const Fp &a, const Fp &b) { return limbs_eq<12>(a.v, b.v); }
+// -0 = 0 (field.glsl.inc:99-102)
+VK_HD Fp fp_neg(const Fp &a) { return fp_is_zero(a) ? a : fp_sub(fp_zero(), a); }
+VK_HD Fp fp_cneg(const Fp &a, bool neg) { return neg ? fp_neg(a) : a; }
+
+// a^e for a little-endian exponent of `words` 32-bit words (square-and-multiply)
+VK_HD Fp fp_pow_words(const Fp &a, const uint32_t *e, int words) {
+    Fp acc = fp_one();
+    for (int i = words - 1; i >= 0; i--) {
+        for (int b = 31; b >= 0; b--) {
+            acc = fp_sqr(acc);
+            if ((e[i] >> b) & 1u) acc = fp_mul(acc, a);
+        }
+    }
+    return acc;
+}
+// a^(p-2); zero maps to zero (field.glsl.inc:528-547)
+VK_HD Fp fp_inv(const Fp &a) {
+    const uint32_t e[12] = {0xffffaaa9u, 0xb9feffffu, 0xb153ffffu, 0x1eabfffeu, 0xf6b0f624u, 0x6730d2a0u,
+                            0xf38512bfu, 0x64774b84u, 0x434bacd7u, 0x4b1ba7b6u, 0x397fe69au, 0x1a0111eau};
+    return fp_pow_words(a, e, 12);
+}
+VK_HD Fp fp_to_canonical(const Fp &a) {
+    Fp one = fp_zero();
+    one.v[0] = 1;
+    return fp_mul(a, one);
+}
+VK_HD Fp fp_from_canonical(const Fp &a) { return fp_mul(Fp{VK_FP_R2}, a); }
+// canonical > (p-1)/2 (field.glsl.inc:549-562)
+VK_HD bool fp_is_lex_largest(const Fp &c) {
+    const uint32_t h[12] = {0xffffd555u, 0xdcff7fffu, 0x58a9ffffu, 0x0f55ffffu, 0x7b587b12u, 0xb3986950u,
+                            0x79c2895fu, 0xb23ba5c2u, 0x21a5d66bu, 0x258dd3dbu, 0x1cbff34du, 0x0d0088f5u};
+    for (int i = 11; i >= 0; i--) {
+        if (c.v[i] != h[i]) return c.v[i] > h[i];
+    }
+    return false;
+}
+VK_HD bool fp_is_canonical(const Fp &a) {
+    for (int i = 11; i >= 0; i--) {
+        if (a.v[i] != fp_p(i)) return a.v[i] < fp_p(i);
+    }
+    return false;
+}
+// p = 3 mod 4: sqrt(a) = a^((p+1)/4); returns false when a is not a square
+VK_HD bool fp_sqrt(Fp &out, const Fp &a) {
+    const uint32_t e[12] = {0xffffeaabu, 0xee7fbfffu, 0xac54ffffu, 0x07aaffffu, 0x3dac3d89u, 0xd9cc34a8u,
+                            0x3ce144afu, 0xd91dd2e1u, 0x90d2eb35u, 0x92c6e9edu, 0x8e5ff9a6u, 0x0680447au};
+    Fp s = fp_pow_words(a, e, 12);
+    if (!fp_eq(fp_sqr(s), a)) return false;
+    out = s;
+    return true;
+}
+
+// ------------------------------------------------------------------- Fr
+VK_HD Fr fr_zero() {
+    Fr r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = 0;
+    return r;
+}
+VK_HD Fr fr_one() { return Fr{VK_FR_ONE}; }
+VK_HD Fr fr_mul(const Fr &a, const Fr &b) {
+    Fr r;
+    mont_mul<8>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD Fr fr_sqr(const Fr &a) { return fr_mul(a, a); }
+VK_HD Fr fr_add(const Fr &a, const Fr &b) {
+    Fr r;
+    mod_add<8>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD Fr fr_sub(const Fr &a, const Fr &b) {
+    Fr r;
+    mod_sub<8>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD Fr fr_neg(const Fr &a) { return fr_sub(fr_zero(), a); }
+VK_HD bool fr_is_zero(const Fr &a) { return limbs_is_zero<8>(a.v); }
+VK_HD bool fr_eq(const Fr &a, const Fr &b) { return limbs_eq<8>(a.v, b.v); }
+VK_HD Fr fr_pow_words(const Fr &a, const uint32_t *e, int words) {
+    Fr acc = fr_one();
+    for (int i = words - 1; i >= 0; i--) {
+        for (int b = 31; b >= 0; b--) {
+            acc = fr_sqr(acc);
+            if ((e[i] >> b) & 1u) acc = fr_mul(acc, a);
+        }
+    }
+    return acc;
+}
+// a^(r-2) (field.glsl.inc:257-275)
+VK_HD Fr fr_inv(const Fr &a) {
+    const uint32_t e[8] = {0xffffffffu, 0xfffffffeu, 0xfffe5bfeu, 0x53bda402u,
+                           0x09a1d805u, 0x3339d808u, 0x299d7d48u, 0x73eda753u};
+    return fr_pow_words(a, e, 8);
+}
+VK_HD Fr fr_to_canonical(const Fr &a) {
+    Fr one = fr_zero();
+    one.v[0] = 1;
+    return fr_mul(a, one);
+}
+// mont_mul needs its first operand below the modulus; the second may be any
+// n-word value (the result is still < 2m before the final subtraction).  So a
+// raw 256-bit input, canonical or not, goes second: fr_from_canonical(v) is
+// v mod r in Montgomery form for every v < 2^256 (k_cells_to_fr.comp relies on
+// the same property).
+VK_HD Fr fr_from_canonical(const Fr &a) { return fr_mul(Fr{VK_FR_R2}, a); }
+VK_HD bool fr_is_canonical(const Fr &a) {
+    for (int i = 7; i >= 0; i--) {
+        if (a.v[i] != fr_p(i)) return a.v[i] < fr_p(i);
+    }
+    return false;
+}
+VK_HD Fr fr_from_u32(uint32_t x) {
+    Fr c = fr_zero();
+    c.v[0] = x;
+    return fr_from_canonical(c);
+}
+
+// 32 big-endian bytes <-> 8 little-endian words
+VK_HD Fr fr_load_be(const uint8_t *b) {
+    Fr v;
+#pragma unroll
+    for (int limb = 0; limb < 8; limb++) {
+        const int off = (7 - limb) * 4;
+        v.v[limb] = ((uint32_t)b[off] << 24) | ((uint32_t)b[off + 1] << 16) | ((uint32_t)b[off + 2] << 8) |
+                    (uint32_t)b[off + 3];
+    }
+    return v;
+}
+VK_HD uint32_t bswap32(uint32_t x) {
+    return (x >> 24) | ((x >> 8) & 0xff00u) | ((x << 8) & 0xff0000u) | (x << 24);
+}
+
+VK_HD uint32_t brev_bits(uint32_t x, int bits) {
+#if defined(__CUDA_ARCH__)
+    return __brev(x) >> (32 - bits);
+#else
+    uint32_t r = 0;
+    for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+#endif
+}
+
+} // namespace vkzg

@@ -1,0 +1,74 @@
+// Host-side declarations of the kernel launchers (plain pointers and sizes).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace vkzg {
+
+struct Fr;
+struct Fp;
+struct G1A;
+struct G1J;
+
+constexpr int kBlobElems = 4096;
+constexpr int kExtElems = 8192;
+constexpr int kCells = 128;        // cells per blob = proofs per blob = circulant size
+constexpr int kCellElems = 64;     // field elements per cell = terms per phase-A output
+constexpr int kDigits = 32;        // signed 8-bit windows per scalar
+constexpr int kBuckets = 128;      // |digit| in 1..128
+constexpr int kHalf = 64;
+constexpr size_t kBlobBytes = 131072;
+constexpr size_t kProofBytes = 48;
+constexpr size_t kCellBytes = 2048;
+constexpr size_t kPositionPoints = (size_t)kCells * kCellElems * kDigits; // 262144
+
+// Setup-derived device tables (immutable once built).
+struct DeviceTables {
+    G1A *pos = nullptr;             // [128 j][64 i][32 d] affine, 2^(8d) X[j][i]
+    Fr *roots_fwd = nullptr;        // w_8192^i
+    Fr *roots_inv = nullptr;        // w_8192^-i
+    uint32_t *tap_items[2] = {nullptr, nullptr};  // e | d<<8 | neg<<16, grouped by bucket
+    uint32_t *tap_offsets[2] = {nullptr, nullptr}; // [129]
+    uint32_t *tap_perm[2] = {nullptr, nullptr};    // [128] buckets by descending load
+    Fr *shift_fwd = nullptr;        // 7^k / 8192                (recovery)
+    Fr *shift_inv = nullptr;        // 7^-k / 8192 / R           (recovery; output lands canonical)
+    Fr *inv_blob_r2 = nullptr;      // [1] (1/4096) in Montgomery form
+};
+
+// Per-batch working set for proofs, capacity `cap` blobs.
+struct ProofWork {
+    uint8_t *blobs = nullptr;   // [cap][131072]
+    Fr *coeffs = nullptr;       // [cap][4096] Montgomery
+    Fr *scalars = nullptr;      // [cap][128 j][64 i] canonical
+    G1J *buckets = nullptr;     // [cap][128][128]
+    G1J *points = nullptr;      // [cap][128] reduce outputs
+    G1J *ladder = nullptr;      // [cap][128][32]
+    G1J *folded = nullptr;      // [cap][128][32]
+    G1A *ladder_aff = nullptr;  // [cap][128][32]
+    uint8_t *proofs = nullptr;  // [cap][128][48]
+    uint32_t *err = nullptr;    // [cap]
+};
+
+struct RecoverWork {
+    uint8_t *cells = nullptr;     // [cap][8192*32]
+    uint8_t *present = nullptr;   // [cap][128]
+    uint8_t *out = nullptr;       // [cap][8192*32]
+    Fr *scratch = nullptr;        // [cap][8192]
+    Fr *zv = nullptr;             // [cap][128]  Z on the domain (x R)
+    Fr *inv_zc = nullptr;         // [cap][128]  1 / Z on the coset
+};
+
+// Proof pipeline over `n` blobs already resident in w.blobs.
+cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s);
+// Recovery pipeline over `n` blobs already resident in w.cells / w.present.
+cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s);
+// Table generation from 4096 compressed monomial points already on the device.
+// Writes t.pos; needs `scratch` of at least setup_scratch_bytes().
+size_t setup_scratch_bytes();
+cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
+                                uint32_t *d_err, cudaStream_t s);
+cudaError_t configure_kernels();
+
+} // namespace vkzg

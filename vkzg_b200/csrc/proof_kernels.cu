@@ -1,0 +1,349 @@
+// FK20 cell-proof pipeline (reference: src/vkzg.cpp:899-1039 and the k_*.comp
+// kernels it dispatches).  Stages:
+//   1 k_blob_to_coeffs   blob bytes -> Fr, canonicity flag, inverse NTT-4096 in
+//                        shared memory, x 1/4096            (k_blob_to_fr, k_ntt_pass x2)
+//   2 k_circulant        64 circulant columns, forward NTT-128, canonical
+//                        scalars coeffs[j][i]               (k_build_circulant)
+//   3 k_phase_a          per output j: signed-digit recode, bucket sort in
+//                        shared memory, fixed-base bucket accumulation over the
+//                        position table                     (k_phase_a_sort, k_phase_a)
+//   4 k_reduce           sum_k k * B_k, 8 lanes per output  (k_bucket_reduce)
+//   5 k_ladder           L[j][d] = 2^(8d) u[j]              (k_ladder)
+//   6 k_fold             L+- = L[j] +- L[j+64]              (k_fold_ladder)
+//   7 k_normalize        Jacobian -> affine, block batch inversion (k_normalize)
+//   8 k_phase_b          split-circulant bucket MSM with the fixed taps (k_phase_b_split)
+//   4'k_reduce
+//   9 k_finish           combine C+ +- C-, normalise, compress, write slot brev7(a)
+//                                                           (k_combine_split, k_normalize, k_compress_proofs)
+#include "device_util.cuh"
+#include "kernels.h"
+
+namespace vkzg {
+
+// ---------------------------------------------------------------- stage 1
+constexpr int kNttThreads = 512;
+
+__global__ void __launch_bounds__(kNttThreads) k_blob_to_coeffs(const uint8_t *__restrict__ blobs, Fr *coeffs,
+                                                                 const Fr *__restrict__ roots_inv,
+                                                                 const Fr *__restrict__ inv_blob_r2, uint32_t *err) {
+    extern __shared__ uint4 smem_raw[];
+    Fr *s = reinterpret_cast<Fr *>(smem_raw);
+    const int b = blockIdx.x;
+    const uint8_t *src = blobs + (size_t)b * kBlobBytes;
+    bool bad = false;
+    // The blob holds f(w_4096^brev12(i)) at slot i: already the bit-reversed
+    // order a DIT transform wants.
+    for (int i = threadIdx.x; i < kBlobElems; i += kNttThreads) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(src + 32 * (size_t)i);
+        const uint4 lo = p[0], hi = p[1];
+        Fr v;
+        v.v[7] = bswap32(lo.x); v.v[6] = bswap32(lo.y); v.v[5] = bswap32(lo.z); v.v[4] = bswap32(lo.w);
+        v.v[3] = bswap32(hi.x); v.v[2] = bswap32(hi.y); v.v[1] = bswap32(hi.z); v.v[0] = bswap32(hi.w);
+        bad |= !fr_is_canonical(v);
+        st_vec(&s[i], fr_from_canonical(v));
+    }
+    if (bad) atomicOr(&err[b], 1u);
+    __syncthreads();
+    smem_dit<kNttThreads>(s, 12, 1, 2, 4096, roots_inv);
+    const Fr scale = ldg_vec(inv_blob_r2);
+    Fr *dst = coeffs + (size_t)b * kBlobElems;
+    for (int i = threadIdx.x; i < kBlobElems; i += kNttThreads) st_vec(&dst[i], fr_mul(ld_vec(&s[i]), scale));
+}
+
+// ---------------------------------------------------------------- stage 2
+// c_i[0] = f[4095-i]; c_i[128-j'] = f[4095-i-64j'] for j' = 1..62; zero
+// elsewhere (k_build_circulant.comp:31-41).  8 columns per block.
+constexpr int kCircCols = 8;
+__global__ void __launch_bounds__(kCircCols * 64) k_circulant(const Fr *__restrict__ coeffs, Fr *scalars,
+                                                             const Fr *__restrict__ roots_fwd) {
+    __shared__ Fr s[kCircCols * kCells];
+    const int b = blockIdx.y, i0 = blockIdx.x * kCircCols;
+    const Fr *f = coeffs + (size_t)b * kBlobElems;
+    for (int q = threadIdx.x; q < kCircCols * kCells; q += blockDim.x) {
+        const int c = q >> 7, t = q & 127, i = i0 + c;
+        Fr v = fr_zero();
+        if (t == 0) v = ld_vec(&f[kBlobElems - 1 - i]);
+        else if (t >= 66) v = ld_vec(&f[kBlobElems - 1 - i - (kCells - t) * kCellElems]);
+        st_vec(&s[q], v);
+    }
+    __syncthreads();
+    smem_dif<kCircCols * 64>(s, 7, kCircCols, 128, 2, roots_fwd);
+    // s[c][pos] holds coeffs at j = brev7(pos); store canonical coeffs[j][i]
+    Fr *out = scalars + (size_t)b * kCells * kCellElems;
+    for (int q = threadIdx.x; q < kCircCols * kCells; q += blockDim.x) {
+        const int c = q >> 7, pos = q & 127, j = (int)brev_bits((uint32_t)pos, 7);
+        st_vec(&out[j * kCellElems + i0 + c], fr_to_canonical(ld_vec(&s[q])));
+    }
+}
+
+// ---------------------------------------------------------------- stage 3
+// Signed base-256 digit dd of a canonical scalar (k_phase_a_sort.comp:31-40).
+__device__ __forceinline__ int recode_digit(const Fr &c, int dd, int &carry) {
+    int v = (int)((c.v[dd >> 2] >> ((dd & 3) * 8)) & 0xffu) + carry;
+    carry = 0;
+    if (v > kBuckets) {
+        v -= 2 * kBuckets;
+        carry = 1;
+    }
+    return v;
+}
+
+// Ranks buckets by descending load so that each warp's threads get similar
+// trip counts (the reference's load-class ordering, k_phase_a_sort.comp:74-101).
+__device__ __forceinline__ void rank_buckets(const uint32_t *cnt, uint8_t *perm) {
+    const int k = threadIdx.x;
+    const uint32_t mine = cnt[k];
+    int rank = 0;
+    for (int q = 0; q < kBuckets; q++) {
+        const uint32_t o = cnt[q];
+        rank += (o > mine) || (o == mine && q < k);
+    }
+    perm[rank] = (uint8_t)k;
+}
+
+__global__ void __launch_bounds__(kBuckets) k_phase_a(const Fr *__restrict__ scalars, const G1A *__restrict__ pos,
+                                                     G1J *buckets) {
+    __shared__ uint32_t cnt[kBuckets], start[kBuckets + 1];
+    __shared__ uint16_t items[kCellElems * kDigits];
+    __shared__ uint8_t perm[kBuckets];
+    const int j = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    cnt[tid] = 0;
+    __syncthreads();
+    Fr sc;
+    if (tid < kCellElems) {
+        sc = ld_vec(&scalars[((size_t)b * kCells + j) * kCellElems + tid]);
+        int carry = 0;
+        for (int dd = 0; dd < kDigits; dd++) {
+            const int v = recode_digit(sc, dd, carry);
+            if (v) atomicAdd(&cnt[abs(v) - 1], 1u);
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t acc = 0;
+        for (int k = 0; k < kBuckets; k++) {
+            start[k] = acc;
+            acc += cnt[k];
+        }
+        start[kBuckets] = acc;
+    }
+    rank_buckets(cnt, perm);
+    __syncthreads();
+    cnt[tid] = start[tid];
+    __syncthreads();
+    if (tid < kCellElems) {
+        int carry = 0;
+        for (int dd = 0; dd < kDigits; dd++) {
+            const int v = recode_digit(sc, dd, carry);
+            if (v) {
+                const uint32_t slot = atomicAdd(&cnt[abs(v) - 1], 1u);
+                items[slot] = (uint16_t)((tid << 6) | (dd << 1) | (v < 0 ? 1 : 0));
+            }
+        }
+    }
+    __syncthreads();
+    const int bucket = perm[tid];
+    const G1A *tj = pos + (size_t)j * kCellElems * kDigits;
+    G1J acc = g1_identity();
+    for (uint32_t it = start[bucket]; it < start[bucket + 1]; it++) {
+        const uint32_t packed = items[it];
+        G1A pt = ldg_vec(&tj[(packed >> 6) * kDigits + ((packed >> 1) & 31u)]);
+        if (packed & 1u) pt.y = fp_neg(pt.y);
+        acc = g1_madd(acc, pt);
+    }
+    st_vec(&buckets[((size_t)b * kCells + j) * kBuckets + bucket], acc);
+}
+
+// ---------------------------------------------------------------- stage 4
+// out[o] = sum_{k=1..128} k * B[o][k-1] with 8 lanes per output: lane l runs
+// the serial running sum over buckets [16l, 16l+16) giving S_l = sum B and
+// W_l = sum (k - 16l + 1) B; then total = sum_l W_l + 16 * sum_l l * S_l
+// (the decomposition of field.glsl.inc:478-517), the cross-lane part done by
+// lane 0 from shared memory so that only two points per thread stay live.
+constexpr int kReduceLanes = 8;
+constexpr int kReduceThreads = 128;
+__global__ void __launch_bounds__(kReduceThreads) k_reduce(const G1J *__restrict__ buckets, G1J *out, int n_outputs) {
+    __shared__ G1J sh_s[kReduceThreads], sh_w[kReduceThreads];
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = gid / kReduceLanes, lane = gid % kReduceLanes;
+    constexpr int per = kBuckets / kReduceLanes;
+    G1J s = g1_identity(), w = g1_identity();
+    if (o < n_outputs) {
+        const G1J *bk = buckets + (size_t)o * kBuckets + lane * per;
+        for (int k = per - 1; k >= 0; k--) {
+            s = g1_add(s, ld_vec(&bk[k]));
+            w = g1_add(w, s);
+        }
+    }
+    st_vec(&sh_s[threadIdx.x], s);
+    st_vec(&sh_w[threadIdx.x], w);
+    __syncthreads();
+    if (lane != 0 || o >= n_outputs) return;
+    // running sums over lanes 7..1: acc = sum_l l * S_l
+    G1J run = g1_identity(), acc = g1_identity();
+    for (int l = kReduceLanes - 1; l >= 1; l--) {
+        run = g1_add(run, ld_vec(&sh_s[threadIdx.x + l]));
+        acc = g1_add(acc, run);
+        w = g1_add(w, ld_vec(&sh_w[threadIdx.x + l]));
+    }
+    for (int q = 0; q < 4; q++) acc = g1_dbl(acc); // x 16
+    st_vec(&out[o], g1_add(w, acc));
+}
+
+// ---------------------------------------------------------------- stage 5
+__global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *ladder, int n_points) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n_points) return;
+    G1J acc = ld_vec(&u[gid]);
+    G1J *dst = ladder + (size_t)gid * kDigits;
+    for (int d = 0; d < kDigits; d++) {
+        st_vec(&dst[d], acc);
+        if (d + 1 < kDigits)
+            for (int q = 0; q < 8; q++) acc = g1_dbl(acc);
+    }
+}
+
+// ---------------------------------------------------------------- stage 6
+__global__ void __launch_bounds__(128) k_fold(const G1J *__restrict__ ladder, G1J *folded, int n_blobs) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n_blobs * kHalf * kDigits) return;
+    const int b = gid / (kHalf * kDigits), r = gid % (kHalf * kDigits);
+    const int j = r / kDigits, d = r % kDigits;
+    const size_t base = (size_t)b * kCells * kDigits;
+    const G1J a = ld_vec(&ladder[base + j * kDigits + d]);
+    const G1J c = ld_vec(&ladder[base + (j + kHalf) * kDigits + d]);
+    st_vec(&folded[base + j * kDigits + d], g1_add(a, c));
+    st_vec(&folded[base + (j + kHalf) * kDigits + d], g1_sub(a, c));
+}
+
+// ---------------------------------------------------------------- stage 7
+constexpr int kNormThreads = 256;
+__global__ void __launch_bounds__(kNormThreads) k_normalize(const G1J *__restrict__ in, G1A *out, int n_points) {
+    __shared__ Fp tree[2 * kNormThreads];
+    const int gid = blockIdx.x * kNormThreads + threadIdx.x;
+    G1J p = gid < n_points ? ld_vec(&in[gid]) : g1_identity();
+    const bool inf = fp_is_zero(p.z);
+    const Fp zi = block_batch_inverse_fp<kNormThreads>(inf ? fp_one() : p.z, tree);
+    if (gid >= n_points) return;
+    G1A a;
+    if (inf) {
+        a.x = fp_zero();
+        a.y = fp_zero();
+    } else {
+        const Fp z2 = fp_sqr(zi);
+        a.x = fp_mul(p.x, z2);
+        a.y = fp_mul(p.y, fp_mul(z2, zi));
+    }
+    st_vec(&out[gid], a);
+}
+
+// ---------------------------------------------------------------- stage 8
+// Block a < 64: cyclic half, a >= 64: negacyclic half; a tap that wraps past
+// index 0 flips sign in the negacyclic half (k_phase_b_split.comp:43-55).
+__global__ void __launch_bounds__(kBuckets) k_phase_b(const G1A *__restrict__ ladder_aff,
+                                                     const uint32_t *__restrict__ items_p,
+                                                     const uint32_t *__restrict__ off_p,
+                                                     const uint32_t *__restrict__ perm_p,
+                                                     const uint32_t *__restrict__ items_m,
+                                                     const uint32_t *__restrict__ off_m,
+                                                     const uint32_t *__restrict__ perm_m, G1J *buckets) {
+    const int a = blockIdx.x, b = blockIdx.y;
+    const bool minus = a >= kHalf;
+    const int aa = a & (kHalf - 1);
+    const uint32_t *items = minus ? items_m : items_p;
+    const uint32_t *off = minus ? off_m : off_p;
+    const int bucket = (int)__ldg(&(minus ? perm_m : perm_p)[threadIdx.x]);
+    const G1A *lad = ladder_aff + ((size_t)b * kCells + (minus ? kHalf : 0)) * kDigits;
+    G1J acc = g1_identity();
+    const uint32_t lo = __ldg(&off[bucket]), hi = __ldg(&off[bucket + 1]);
+    for (uint32_t it = lo; it < hi; it++) {
+        const uint32_t packed = __ldg(&items[it]);
+        const int e = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
+        const bool neg = ((packed >> 16) & 1u) != (minus && e > aa);
+        G1A pt = ld_vec(&lad[((aa - e) & (kHalf - 1)) * kDigits + d]);
+        if (neg) pt.y = fp_neg(pt.y);
+        acc = g1_madd(acc, pt);
+    }
+    st_vec(&buckets[((size_t)b * kCells + a) * kBuckets + bucket], acc);
+}
+
+// ---------------------------------------------------------------- stage 9
+__global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, uint8_t *proofs) {
+    __shared__ Fp tree[2 * kCells];
+    __shared__ G1J outp[kCells];
+    const int b = blockIdx.x, t = threadIdx.x;
+    if (t < kHalf) {
+        const G1J cp = ld_vec(&c[(size_t)b * kCells + t]);
+        const G1J cm = ld_vec(&c[(size_t)b * kCells + t + kHalf]);
+        st_vec(&outp[t], g1_add(cp, cm));
+        st_vec(&outp[t + kHalf], g1_sub(cp, cm));
+    }
+    __syncthreads();
+    const G1J p = ld_vec(&outp[t]);
+    const bool inf = fp_is_zero(p.z);
+    const Fp zi = block_batch_inverse_fp<kCells>(inf ? fp_one() : p.z, tree);
+    G1A a;
+    if (inf) {
+        a.x = fp_zero();
+        a.y = fp_zero();
+    } else {
+        const Fp z2 = fp_sqr(zi);
+        a.x = fp_mul(p.x, z2);
+        a.y = fp_mul(p.y, fp_mul(z2, zi));
+    }
+    alignas(16) uint8_t enc[48];
+    g1_compress(enc, a);
+    uint4 *dst = reinterpret_cast<uint4 *>(proofs + ((size_t)b * kCells + brev_bits((uint32_t)t, 7)) * kProofBytes);
+    const uint4 *e4 = reinterpret_cast<const uint4 *>(enc);
+    dst[0] = e4[0];
+    dst[1] = e4[1];
+    dst[2] = e4[2];
+}
+
+// ---------------------------------------------------------------- launcher
+// ev (nullable): kProofStages + 1 events recorded around the stages.
+cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev) {
+    if (n <= 0) return cudaSuccess;
+    int k = 0;
+    auto mark = [&]() {
+        if (ev) cudaEventRecord(ev[k++], s);
+    };
+    const size_t smem_ntt = (size_t)kBlobElems * sizeof(Fr);
+    const int n_out = n * kCells;
+    const int red_blocks = (n_out * kReduceLanes + kReduceThreads - 1) / kReduceThreads;
+    const int n_lad = n * kCells * kDigits;
+    mark();
+    k_blob_to_coeffs<<<n, kNttThreads, smem_ntt, s>>>(w.blobs, w.coeffs, t.roots_inv, t.inv_blob_r2, w.err);
+    mark();
+    k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
+    mark();
+    k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
+    mark();
+    k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    mark();
+    k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
+    mark();
+    k_fold<<<(n * kHalf * kDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
+    mark();
+    k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
+    mark();
+    k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0], t.tap_perm[0],
+                                                   t.tap_items[1], t.tap_offsets[1], t.tap_perm[1], w.buckets);
+    mark();
+    k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    mark();
+    k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
+    mark();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    return launch_proofs_timed(t, w, n, s, nullptr);
+}
+
+cudaError_t configure_proof_kernels() {
+    return cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kBlobElems * sizeof(Fr)));
+}
+
+} // namespace vkzg

@@ -1,0 +1,538 @@
+// C ABI of include/vkzg.h and include/vkzg_b200.h over the CUDA kernels.
+//
+// Reference counterpart: src/vkzg.cpp (Vulkan instance, pipelines, buffers and
+// the per-call command buffer).  Here a prover owns one CUDA stream, the setup
+// tables resident in device memory, and a working set sized for
+// max_batch_size blobs; each API call copies a chunk in, launches the stage
+// kernels on the stream, and copies the chunk out.  Calls on one prover are
+// serialised by a mutex (src/vkzg.cpp:1188,1206).
+#include "../../include/vkzg.h"
+#include "../../include/vkzg_b200.h"
+#include "device_util.cuh"
+#include "kernels.h"
+
+#include <dlfcn.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace vkzg;
+
+namespace vkzg {
+cudaError_t configure_proof_kernels();
+cudaError_t configure_recover_kernels();
+cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s,
+                                cudaEvent_t *ev);
+cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
+                                 cudaEvent_t *ev);
+} // namespace vkzg
+
+static constexpr int kProofStages = 10;
+static constexpr int kRecoverStages = 2;
+static const char *kProofStageNames[kProofStages] = {"blob_to_coeffs", "circulant", "phase_a",  "reduce_a",
+                                                     "ladder",         "fold",      "normalize", "phase_b",
+                                                     "reduce_b",       "finish"};
+static const char *kRecoverStageNames[kRecoverStages] = {"recover_prep", "recover_main"};
+
+struct vkzg_prover {
+    int device = 0;
+    std::string name;
+    uint32_t sm_count = 0;
+    std::string tables_source;
+    cudaStream_t stream = nullptr;
+    std::mutex mutex;
+    DeviceTables t;
+    std::vector<void *> allocs;
+    uint32_t cap = 0;
+    ProofWork pw;
+    RecoverWork rw;
+    uint32_t *h_err = nullptr; // pinned, cap words
+    bool timing = false;
+    cudaEvent_t ev[kProofStages + 1] = {};
+    double last_proof_ms[kProofStages] = {};
+    double last_recover_ms[kRecoverStages] = {};
+
+    ~vkzg_prover() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *a : allocs) cudaFree(a);
+        if (h_err) cudaFreeHost(h_err);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    template <typename T>
+    bool alloc(T *&ptr, size_t count) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, count * sizeof(T) + 16) != cudaSuccess) return false;
+        allocs.push_back(p);
+        ptr = reinterpret_cast<T *>(p);
+        return true;
+    }
+};
+
+// ------------------------------------------------------------------ utils
+
+const char *vkzg_error_string(vkzg_result r) {
+    switch (r) {
+    case VKZG_OK: return "ok";
+    case VKZG_ERR_BADARGS: return "invalid argument";
+    case VKZG_ERR_MALLOC: return "allocation failed";
+    case VKZG_ERR_IO: return "i/o error";
+    case VKZG_ERR_SETUP: return "malformed trusted setup";
+    case VKZG_ERR_GPU: return "gpu error";
+    case VKZG_ERR_INVALID_BLOB: return "blob contains a non-canonical field element";
+    }
+    return "unknown error";
+}
+
+void vkzg_options_default(vkzg_options *opts) {
+    if (opts) opts->max_batch_size = 0;
+}
+
+const char *vkzg_prover_device_name(const vkzg_prover *p) { return p ? p->name.c_str() : ""; }
+uint32_t vkzg_prover_gpu_core_count(const vkzg_prover *p) { return p ? p->sm_count : 0; }
+const char *vkzg_b200_prover_tables_source(const vkzg_prover *p) { return p ? p->tables_source.c_str() : ""; }
+
+// --------------------------------------------------------- host-side tables
+namespace {
+
+std::string library_dir() {
+    Dl_info info;
+    if (dladdr((void *)&vkzg_prover_new, &info) && info.dli_fname) {
+        std::string s(info.dli_fname);
+        const size_t k = s.rfind('/');
+        if (k != std::string::npos) return s.substr(0, k);
+    }
+    return ".";
+}
+
+// w_8192 = 7^((r-1)/8192) and its powers (the reference's roots tables,
+// src/precomputed_tables.cpp:43-44)
+void host_roots(std::vector<Fr> &fwd, std::vector<Fr> &inv) {
+    // (r-1)/8192
+    const uint32_t e[8] = {0xfff80000u, 0xdff7ffffu, 0x2017fff2u, 0xc02a9dedu,
+                           0xc0404d0eu, 0xea4199ceu, 0x3a994cebu, 0x00039f6du};
+    const Fr w = fr_pow_words(fr_from_u32(7), e, 8);
+    const Fr wi = fr_inv(w);
+    fwd.resize(kExtElems);
+    inv.resize(kExtElems);
+    fwd[0] = inv[0] = fr_one();
+    for (int i = 1; i < kExtElems; i++) {
+        fwd[i] = fr_mul(fwd[i - 1], w);
+        inv[i] = fr_mul(inv[i - 1], wi);
+    }
+}
+
+// Phase-B half taps c+-[e] = (c[e] +- c[e+64]) / 2, c[e] = (1/128) sum_{t<64} w_128^(e t),
+// recoded into signed base-256 digits and grouped by bucket (the reference's
+// kernel_items/offsets/perm tables, src/precomputed_tables.cpp:45-49).
+void host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2], uint32_t offsets[2][kBuckets + 1],
+                     uint32_t perm[2][kBuckets]) {
+    Fr c[kCells];
+    const Fr inv128 = fr_inv(fr_from_u32(128)), inv2 = fr_inv(fr_from_u32(2));
+    for (int e = 0; e < kCells; e++) {
+        Fr acc = fr_zero();
+        for (int t = 0; t < kHalf; t++) acc = fr_add(acc, fwd[((e * t) % kCells) * (kExtElems / kCells)]);
+        c[e] = fr_mul(acc, inv128);
+    }
+    for (int h = 0; h < 2; h++) {
+        int dig[kHalf][kDigits];
+        uint32_t count[kBuckets] = {0};
+        for (int e = 0; e < kHalf; e++) {
+            const Fr tap = fr_mul(h == 0 ? fr_add(c[e], c[e + kHalf]) : fr_sub(c[e], c[e + kHalf]), inv2);
+            const Fr can = fr_to_canonical(tap);
+            int carry = 0;
+            for (int d = 0; d < kDigits; d++) {
+                int v = (int)((can.v[d >> 2] >> ((d & 3) * 8)) & 0xffu) + carry;
+                carry = 0;
+                if (v > kBuckets) {
+                    v -= 2 * kBuckets;
+                    carry = 1;
+                }
+                dig[e][d] = v;
+                if (v) count[abs(v) - 1]++;
+            }
+        }
+        uint32_t acc = 0;
+        for (int k = 0; k < kBuckets; k++) {
+            offsets[h][k] = acc;
+            acc += count[k];
+        }
+        offsets[h][kBuckets] = acc;
+        items[h].assign(acc, 0);
+        uint32_t cur[kBuckets];
+        memcpy(cur, offsets[h], sizeof cur);
+        for (int e = 0; e < kHalf; e++)
+            for (int d = 0; d < kDigits; d++) {
+                const int v = dig[e][d];
+                if (!v) continue;
+                items[h][cur[abs(v) - 1]++] = (uint32_t)e | ((uint32_t)d << 8) | ((v < 0 ? 1u : 0u) << 16);
+            }
+        // buckets by descending load, stable
+        std::vector<int> order(kBuckets);
+        for (int k = 0; k < kBuckets; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return std::min(count[a], 63u) > std::min(count[b], 63u);
+        });
+        for (int k = 0; k < kBuckets; k++) perm[h][k] = (uint32_t)order[k];
+    }
+}
+
+struct HostTables {
+    std::vector<uint8_t> pos; // may be empty when generated on the device
+    std::vector<Fr> roots_fwd, roots_inv;
+    std::vector<uint32_t> items[2];
+    uint32_t offsets[2][kBuckets + 1];
+    uint32_t perm[2][kBuckets];
+    Fr inv_blob;
+};
+
+bool read_exact(FILE *f, void *p, size_t n) { return fread(p, 1, n, f) == n; }
+
+// precomputed_tables.bin, format v1 (src/precomputed_tables.cpp:16-58)
+vkzg_result load_tables_file(const char *path, HostTables &h) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return VKZG_ERR_IO;
+    vkzg_result rc = VKZG_ERR_SETUP;
+    uint32_t hdr[4];
+    if (read_exact(f, hdr, 16) && hdr[0] == 0x475A4B56u && hdr[1] == 1u && hdr[2] <= (1u << 20) &&
+        hdr[3] <= (1u << 20)) {
+        h.pos.resize(kPositionPoints * sizeof(G1A));
+        h.roots_fwd.resize(kExtElems);
+        h.roots_inv.resize(kExtElems);
+        h.items[0].resize(hdr[2]);
+        h.items[1].resize(hdr[3]);
+        if (read_exact(f, h.pos.data(), h.pos.size()) && read_exact(f, h.roots_fwd.data(), kExtElems * sizeof(Fr)) &&
+            read_exact(f, h.roots_inv.data(), kExtElems * sizeof(Fr)) &&
+            read_exact(f, h.items[0].data(), 4 * (size_t)hdr[2]) &&
+            read_exact(f, h.items[1].data(), 4 * (size_t)hdr[3]) && read_exact(f, h.offsets[0], sizeof h.offsets[0]) &&
+            read_exact(f, h.offsets[1], sizeof h.offsets[1]) && read_exact(f, h.perm[0], sizeof h.perm[0]) &&
+            read_exact(f, h.perm[1], sizeof h.perm[1]) && read_exact(f, &h.inv_blob, sizeof h.inv_blob)) {
+            rc = VKZG_OK;
+            // index sanity: offsets monotone within the item counts, perm a permutation
+            for (int s = 0; s < 2 && rc == VKZG_OK; s++) {
+                if (h.offsets[s][0] != 0 || h.offsets[s][kBuckets] != hdr[2 + s]) rc = VKZG_ERR_SETUP;
+                for (int k = 0; k < kBuckets && rc == VKZG_OK; k++)
+                    if (h.offsets[s][k] > h.offsets[s][k + 1] || h.perm[s][k] >= (uint32_t)kBuckets) rc = VKZG_ERR_SETUP;
+                for (uint32_t it = 0; it < hdr[2 + s] && rc == VKZG_OK; it++)
+                    if ((h.items[s][it] & 0xffu) >= (uint32_t)kHalf || ((h.items[s][it] >> 8) & 0xffu) >= (uint32_t)kDigits)
+                        rc = VKZG_ERR_SETUP;
+            }
+        }
+    }
+    fclose(f);
+    return rc;
+}
+
+vkzg_result read_file(const std::string &path, std::vector<uint8_t> &out) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return VKZG_ERR_IO;
+    fseek(f, 0, SEEK_END);
+    const long n = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    out.resize(n > 0 ? (size_t)n : 0);
+    const bool ok = n > 0 && read_exact(f, out.data(), out.size());
+    fclose(f);
+    return ok ? VKZG_OK : VKZG_ERR_SETUP;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        if ((call) != cudaSuccess) return VKZG_ERR_GPU;                                               \
+    } while (0)
+
+vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
+    DeviceTables &t = p->t;
+    if (!p->alloc(t.roots_fwd, kExtElems) || !p->alloc(t.roots_inv, kExtElems) || !p->alloc(t.shift_fwd, kExtElems) ||
+        !p->alloc(t.shift_inv, kExtElems) || !p->alloc(t.inv_blob_r2, 1))
+        return VKZG_ERR_MALLOC;
+    for (int s = 0; s < 2; s++) {
+        if (!p->alloc(t.tap_items[s], std::max<size_t>(1, h.items[s].size())) || !p->alloc(t.tap_offsets[s], kBuckets + 1) ||
+            !p->alloc(t.tap_perm[s], kBuckets))
+            return VKZG_ERR_MALLOC;
+        CK(cudaMemcpy(t.tap_items[s], h.items[s].data(), 4 * h.items[s].size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.tap_offsets[s], h.offsets[s], sizeof h.offsets[s], cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.tap_perm[s], h.perm[s], sizeof h.perm[s], cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(t.roots_fwd, h.roots_fwd.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.roots_inv, h.roots_inv.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.inv_blob_r2, &h.inv_blob, sizeof(Fr), cudaMemcpyHostToDevice));
+    // recovery coset-shift tables (the reference's k_pow_seq, src/vkzg.cpp:757-774),
+    // with 1/8192 folded in and, for the inverse, an extra 1/R (see recover_kernels.cu)
+    std::vector<Fr> sf(kExtElems), si(kExtElems);
+    const Fr inv_n = fr_inv(fr_from_u32(kExtElems)), seven = fr_from_u32(7), inv7 = fr_inv(seven);
+    Fr a = inv_n, b = inv_n;
+    for (int k = 0; k < kExtElems; k++) {
+        sf[k] = a;
+        si[k] = fr_to_canonical(b);
+        a = fr_mul(a, seven);
+        b = fr_mul(b, inv7);
+    }
+    CK(cudaMemcpy(t.shift_fwd, sf.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.shift_inv, si.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
+    return VKZG_OK;
+}
+
+// Position table from a setup on the device.
+vkzg_result generate_position_table(vkzg_prover *p, const std::vector<uint8_t> &setup) {
+    if (setup.size() != (size_t)kBlobElems * 48) return VKZG_ERR_SETUP;
+    uint8_t *d_setup = nullptr;
+    void *scratch = nullptr;
+    uint32_t *d_err = nullptr;
+    vkzg_result rc = VKZG_OK;
+    if (cudaMalloc(&d_setup, setup.size()) != cudaSuccess || cudaMalloc(&scratch, setup_scratch_bytes()) != cudaSuccess ||
+        cudaMalloc(&d_err, 4) != cudaSuccess) {
+        rc = VKZG_ERR_MALLOC;
+    } else {
+        uint32_t h_err = 0;
+        if (cudaMemcpy(d_setup, setup.data(), setup.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(d_err, 0, 4) != cudaSuccess ||
+            launch_setup_tables(d_setup, p->t.pos, p->t.roots_fwd, scratch, d_err, p->stream) != cudaSuccess ||
+            cudaStreamSynchronize(p->stream) != cudaSuccess ||
+            cudaMemcpy(&h_err, d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            rc = VKZG_ERR_GPU;
+        } else if (h_err) {
+            rc = VKZG_ERR_SETUP;
+        }
+    }
+    cudaFree(d_setup);
+    cudaFree(scratch);
+    cudaFree(d_err);
+    return rc;
+}
+
+void computed_small_tables(HostTables &h) {
+    host_roots(h.roots_fwd, h.roots_inv);
+    host_tap_tables(h.roots_fwd, h.items, h.offsets, h.perm);
+    h.inv_blob = fr_inv(fr_from_u32(kBlobElems));
+}
+
+vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
+    p->cap = cap;
+    ProofWork &w = p->pw;
+    RecoverWork &r = p->rw;
+    const size_t B = cap;
+    bool ok = p->alloc(w.blobs, B * kBlobBytes) && p->alloc(w.coeffs, B * kBlobElems) &&
+              p->alloc(w.scalars, B * kCells * kCellElems) && p->alloc(w.buckets, B * kCells * kBuckets) &&
+              p->alloc(w.points, B * kCells) && p->alloc(w.ladder, B * kCells * kDigits) &&
+              p->alloc(w.folded, B * kCells * kDigits) && p->alloc(w.ladder_aff, B * kCells * kDigits) &&
+              p->alloc(w.proofs, B * kCells * kProofBytes) && p->alloc(w.err, B) &&
+              p->alloc(r.cells, B * kExtElems * 32) && p->alloc(r.present, B * kCells) &&
+              p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.scratch, B * kExtElems) &&
+              p->alloc(r.zv, B * kCells) && p->alloc(r.inv_zc, B * kCells);
+    if (!ok) return VKZG_ERR_MALLOC;
+    if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
+    return VKZG_OK;
+}
+
+} // namespace
+
+// -------------------------------------------------------------- lifecycle
+
+vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
+    if (!out) return VKZG_ERR_BADARGS;
+    *out = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return VKZG_ERR_GPU;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return VKZG_ERR_GPU;
+    if (configure_proof_kernels() != cudaSuccess || configure_recover_kernels() != cudaSuccess) return VKZG_ERR_GPU;
+
+    vkzg_prover *p = new (std::nothrow) vkzg_prover();
+    if (!p) return VKZG_ERR_MALLOC;
+    p->device = dev;
+    p->name = prop.name;
+    p->sm_count = (uint32_t)prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete p;
+        return VKZG_ERR_GPU;
+    }
+    for (auto &e : p->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete p;
+            return VKZG_ERR_GPU;
+        }
+
+    // Setup tables: file first, in the reference's search order, then device generation.
+    const std::string libdir = library_dir();
+    std::vector<std::string> files;
+    if (const char *env = getenv("VKZG_TABLES_PATH")) files.push_back(env);
+    files.push_back(libdir + "/precomputed_tables.bin");
+    HostTables h;
+    vkzg_result rc = VKZG_ERR_IO;
+    bool seen_malformed = false;
+    for (const auto &f : files) {
+        rc = load_tables_file(f.c_str(), h);
+        if (rc == VKZG_OK) {
+            p->tables_source = "file:" + f;
+            break;
+        }
+        if (rc == VKZG_ERR_SETUP) seen_malformed = true;
+    }
+    if (rc == VKZG_OK) {
+        if (!p->alloc(p->t.pos, kPositionPoints)) rc = VKZG_ERR_MALLOC;
+        else if (cudaMemcpy(p->t.pos, h.pos.data(), h.pos.size(), cudaMemcpyHostToDevice) != cudaSuccess) rc = VKZG_ERR_GPU;
+        else rc = upload_small_tables(p, h);
+    } else {
+        const char *envs = getenv("VKZG_SETUP_PATH");
+        const std::string setup_path = envs ? std::string(envs) : libdir + "/data/trusted_setup_g1_monomial.bin";
+        std::vector<uint8_t> setup;
+        rc = read_file(setup_path, setup);
+        if (rc == VKZG_OK) {
+            computed_small_tables(h);
+            rc = upload_small_tables(p, h);
+            if (rc == VKZG_OK && !p->alloc(p->t.pos, kPositionPoints)) rc = VKZG_ERR_MALLOC;
+            if (rc == VKZG_OK) rc = generate_position_table(p, setup);
+            if (rc == VKZG_OK) p->tables_source = "generated:" + setup_path;
+        } else if (seen_malformed) {
+            rc = VKZG_ERR_SETUP;
+        }
+    }
+    if (rc == VKZG_OK) rc = alloc_working_set(p, opts && opts->max_batch_size ? opts->max_batch_size : 256);
+    if (rc == VKZG_OK && cudaStreamSynchronize(p->stream) != cudaSuccess) rc = VKZG_ERR_GPU;
+    if (rc != VKZG_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return VKZG_OK;
+}
+
+void vkzg_prover_free(vkzg_prover *p) { delete p; }
+
+// ---------------------------------------------------------------- compute
+
+namespace {
+
+void collect_times(vkzg_prover *p, int stages, double *dst) {
+    for (int i = 0; i < stages; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]);
+        dst[i] = ms;
+    }
+}
+
+vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
+    cudaStream_t s = p->stream;
+    CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+    CK(launch_proofs_timed(p->t, p->pw, (int)n, s, p->timing ? p->ev : nullptr));
+    CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (p->timing) collect_times(p, kProofStages, p->last_proof_ms);
+    for (uint32_t b = 0; b < n; b++)
+        if (p->h_err[b]) return VKZG_ERR_INVALID_BLOB;
+    CK(cudaMemcpyAsync(proofs, p->pw.proofs, (size_t)n * kCells * kProofBytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return VKZG_OK;
+}
+
+vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, const uint8_t *present, uint32_t n) {
+    // more than 64 missing cells in any blob of the chunk: BADARGS before any
+    // device work for it (src/vkzg.cpp:1093-1105)
+    for (uint32_t b = 0; b < n; b++) {
+        int miss = 0;
+        for (int i = 0; i < kCells; i++) miss += present[(size_t)b * kCells + i] == 0;
+        if (miss > kCellElems) return VKZG_ERR_BADARGS;
+    }
+    cudaStream_t s = p->stream;
+    const size_t bytes = (size_t)n * kExtElems * 32;
+    CK(cudaMemcpyAsync(p->rw.cells, cells, bytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
+    CK(launch_recover_timed(p->t, p->rw, (int)n, s, p->timing ? p->ev : nullptr));
+    CK(cudaMemcpyAsync(out, p->rw.out, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (p->timing) collect_times(p, kRecoverStages, p->last_recover_ms);
+    return VKZG_OK;
+}
+
+} // namespace
+
+vkzg_result vkzg_compute_proofs_batch(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, size_t num_blobs) {
+    if (!p || !blobs || !proofs) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        const vkzg_result rc = proofs_chunk(p, proofs + done * kCells * kProofBytes, blobs + done * kBlobBytes, n);
+        if (rc != VKZG_OK) return rc;
+        done += n;
+    }
+    return VKZG_OK;
+}
+
+vkzg_result vkzg_recover_cells_batch(vkzg_prover *p, uint8_t *cells_out, const uint8_t *cells,
+                                     const uint8_t *cell_present, size_t num_blobs) {
+    if (!p || !cells_out || !cells || !cell_present) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    const size_t blob_bytes = (size_t)kExtElems * 32;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        const vkzg_result rc = recover_chunk(p, cells_out + done * blob_bytes, cells + done * blob_bytes,
+                                             cell_present + done * kCells, n);
+        if (rc != VKZG_OK) return rc;
+        done += n;
+    }
+    return VKZG_OK;
+}
+
+// ------------------------------------------------------------- extensions
+
+void vkzg_b200_set_stage_timing(vkzg_prover *p, int enabled) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    p->timing = enabled != 0;
+}
+
+int vkzg_b200_last_stage_times(const vkzg_prover *p, int recovery, double *ms, int cap) {
+    if (!p || !ms) return 0;
+    const int n = recovery ? kRecoverStages : kProofStages;
+    const double *src = recovery ? p->last_recover_ms : p->last_proof_ms;
+    for (int i = 0; i < n && i < cap; i++) ms[i] = src[i];
+    return n;
+}
+
+const char *vkzg_b200_stage_name(int recovery, int i) {
+    if (recovery) return (i >= 0 && i < kRecoverStages) ? kRecoverStageNames[i] : "";
+    return (i >= 0 && i < kProofStages) ? kProofStageNames[i] : "";
+}
+
+vkzg_result vkzg_b200_write_tables(const uint8_t *g1_monomial_compressed, const char *out_path) {
+    if (!g1_monomial_compressed || !out_path) return VKZG_ERR_BADARGS;
+    vkzg_prover tmp; // table storage and stream only
+    if (cudaGetDevice(&tmp.device) != cudaSuccess) return VKZG_ERR_GPU;
+    if (cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking) != cudaSuccess) return VKZG_ERR_GPU;
+    HostTables h;
+    computed_small_tables(h);
+    vkzg_result rc = upload_small_tables(&tmp, h);
+    if (rc == VKZG_OK && !tmp.alloc(tmp.t.pos, kPositionPoints)) rc = VKZG_ERR_MALLOC;
+    if (rc != VKZG_OK) return rc;
+    std::vector<uint8_t> setup(g1_monomial_compressed, g1_monomial_compressed + (size_t)kBlobElems * 48);
+    rc = generate_position_table(&tmp, setup);
+    if (rc != VKZG_OK) return rc;
+    std::vector<uint8_t> pos(kPositionPoints * sizeof(G1A));
+    if (cudaMemcpy(pos.data(), tmp.t.pos, pos.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return VKZG_ERR_GPU;
+    FILE *f = fopen(out_path, "wb");
+    if (!f) return VKZG_ERR_IO;
+    const uint32_t hdr[4] = {0x475A4B56u, 1u, (uint32_t)h.items[0].size(), (uint32_t)h.items[1].size()};
+    bool ok = fwrite(hdr, 1, 16, f) == 16 && fwrite(pos.data(), 1, pos.size(), f) == pos.size() &&
+              fwrite(h.roots_fwd.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
+              fwrite(h.roots_inv.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
+              fwrite(h.items[0].data(), 4, h.items[0].size(), f) == h.items[0].size() &&
+              fwrite(h.items[1].data(), 4, h.items[1].size(), f) == h.items[1].size() &&
+              fwrite(h.offsets[0], 1, sizeof h.offsets[0], f) == sizeof h.offsets[0] &&
+              fwrite(h.offsets[1], 1, sizeof h.offsets[1], f) == sizeof h.offsets[1] &&
+              fwrite(h.perm[0], 1, sizeof h.perm[0], f) == sizeof h.perm[0] &&
+              fwrite(h.perm[1], 1, sizeof h.perm[1], f) == sizeof h.perm[1] &&
+              fwrite(&h.inv_blob, 1, sizeof h.inv_blob, f) == sizeof h.inv_blob;
+    fclose(f);
+    return ok ? VKZG_OK : VKZG_ERR_IO;
+}
