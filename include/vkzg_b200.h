@@ -35,6 +35,31 @@ void vkzg_b200_set_stage_timing(vkzg_prover *p, int enabled);
 int vkzg_b200_last_stage_times(const vkzg_prover *p, int recovery, double *ms, int cap);
 const char *vkzg_b200_stage_name(int recovery, int i);
 
+/*
+ * Device-resident forms of vkzg_compute_proofs_batch / vkzg_recover_cells_batch
+ * (include/vkzg.h:103-104, 120-121) for callers whose data already lives in
+ * device memory: same layouts, device pointers, no host copies.  The work is
+ * ordered after everything already enqueued on `stream` (a cudaStream_t; NULL
+ * = the legacy default stream) and everything enqueued on `stream` afterwards
+ * is ordered after it; the call returns once the work is enqueued.
+ * d_err (num_blobs words) receives a nonzero word for each blob with a
+ * non-canonical element (proofs) or more than 64 missing cells (recovery);
+ * those blobs' outputs are unspecified.
+ */
+vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, const uint8_t *d_blobs,
+                                            uint32_t *d_err, size_t num_blobs, void *stream);
+vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,
+                                           const uint8_t *d_cell_present, uint32_t *d_err, size_t num_blobs,
+                                           void *stream);
+
+/*
+ * Throughput probes on the current device, for roofline denominators (the
+ * reference has none).  which = 0: 32-bit integer multiply-add issue rate in
+ * tera-ops/s; 1: this library's Fp (381-bit) Montgomery multiplies in giga-ops/s;
+ * 2: Fr (255-bit) multiplies in giga-ops/s.  Best of three timed launches.
+ */
+vkzg_result vkzg_b200_microbench(int which, double *result);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

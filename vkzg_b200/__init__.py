@@ -34,7 +34,8 @@ EXPORTED_SYMBOLS = (
     "vkzg_prover_device_name", "vkzg_prover_gpu_core_count", "vkzg_compute_proofs_batch",
     "vkzg_recover_cells_batch",
     "vkzg_b200_write_tables", "vkzg_b200_prover_tables_source", "vkzg_b200_set_stage_timing",
-    "vkzg_b200_last_stage_times", "vkzg_b200_stage_name",
+    "vkzg_b200_last_stage_times", "vkzg_b200_stage_name", "vkzg_b200_compute_proofs_device",
+    "vkzg_b200_recover_cells_device", "vkzg_b200_microbench",
 )
 
 
@@ -87,6 +88,12 @@ def library():
             L.vkzg_b200_last_stage_times.restype = ctypes.c_int
             L.vkzg_b200_stage_name.argtypes = [ctypes.c_int, ctypes.c_int]
             L.vkzg_b200_stage_name.restype = ctypes.c_char_p
+            L.vkzg_b200_compute_proofs_device.argtypes = [vp, vp, vp, vp, ctypes.c_size_t, vp]
+            L.vkzg_b200_compute_proofs_device.restype = ctypes.c_int
+            L.vkzg_b200_recover_cells_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
+            L.vkzg_b200_recover_cells_device.restype = ctypes.c_int
+            L.vkzg_b200_microbench.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            L.vkzg_b200_microbench.restype = ctypes.c_int
             _lib = L
     return _lib
 
@@ -187,6 +194,13 @@ class Prover:
                                                   blob_count))
         return bytes(out)
 
+    def compute_proofs_device(self, d_proofs, d_blobs, d_err, n, stream=None):
+        """Device pointers (ints); enqueued on `stream` (cudaStream_t as int, None = default stream)."""
+        return self._lib.vkzg_b200_compute_proofs_device(self._h, d_proofs, d_blobs, d_err, n, stream)
+
+    def recover_cells_device(self, d_out, d_cells, d_present, d_err, n, stream=None):
+        return self._lib.vkzg_b200_recover_cells_device(self._h, d_out, d_cells, d_present, d_err, n, stream)
+
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)
 
@@ -194,6 +208,13 @@ class Prover:
         buf = (ctypes.c_double * 32)()
         n = self._lib.vkzg_b200_last_stage_times(self._h, 1 if recovery else 0, buf, 32)
         return {self._lib.vkzg_b200_stage_name(1 if recovery else 0, i).decode(): buf[i] for i in range(n)}
+
+
+def microbench(which):
+    """0: IMAD issue rate (T/s); 1: Fp multiplies (G/s); 2: Fr multiplies (G/s)."""
+    out = ctypes.c_double()
+    _check(library().vkzg_b200_microbench(int(which), ctypes.byref(out)))
+    return out.value
 
 
 def write_tables(g1_monomial_compressed, out_path):

@@ -58,6 +58,7 @@ struct RecoverWork {
     Fr *scratch = nullptr;        // [cap][8192]
     Fr *zv = nullptr;             // [cap][128]  Z on the domain (x R)
     Fr *inv_zc = nullptr;         // [cap][128]  1 / Z on the coset
+    uint32_t *err = nullptr;      // [cap] more than 64 cells missing
 };
 
 // Proof pipeline over `n` blobs already resident in w.blobs.

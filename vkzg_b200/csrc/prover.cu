@@ -54,8 +54,13 @@ struct vkzg_prover {
     uint32_t *h_err = nullptr; // pinned, cap words
     bool timing = false;
     cudaEvent_t ev[kProofStages + 1] = {};
-    double last_proof_ms[kProofStages] = {};
-    double last_recover_ms[kRecoverStages] = {};
+    cudaEvent_t ev_rec[kRecoverStages + 1] = {};
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr; // stream handshakes of the device-pointer API
+    // stage times: filled after a blocking call, or lazily (pending_kind) after
+    // a device-pointer call once the caller has synchronised
+    mutable double last_proof_ms[kProofStages] = {};
+    mutable double last_recover_ms[kRecoverStages] = {};
+    mutable bool pending_proof = false, pending_recover = false;
 
     ~vkzg_prover() {
         if (stream) cudaStreamSynchronize(stream);
@@ -63,6 +68,10 @@ struct vkzg_prover {
         if (h_err) cudaFreeHost(h_err);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto &e : ev_rec)
+            if (e) cudaEventDestroy(e);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
     }
     template <typename T>
@@ -324,7 +333,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
               p->alloc(w.proofs, B * kCells * kProofBytes) && p->alloc(w.err, B) &&
               p->alloc(r.cells, B * kExtElems * 32) && p->alloc(r.present, B * kCells) &&
               p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.scratch, B * kExtElems) &&
-              p->alloc(r.zv, B * kCells) && p->alloc(r.inv_zc, B * kCells);
+              p->alloc(r.zv, B * kCells) && p->alloc(r.inv_zc, B * kCells) && p->alloc(r.err, B);
     if (!ok) return VKZG_ERR_MALLOC;
     if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
     return VKZG_OK;
@@ -352,11 +361,21 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
         delete p;
         return VKZG_ERR_GPU;
     }
+    for (auto &e : p->ev_rec)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete p;
+            return VKZG_ERR_GPU;
+        }
     for (auto &e : p->ev)
         if (cudaEventCreate(&e) != cudaSuccess) {
             delete p;
             return VKZG_ERR_GPU;
         }
+    if (cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+        delete p;
+        return VKZG_ERR_GPU;
+    }
 
     // Setup tables: file first, in the reference's search order, then device generation.
     const std::string libdir = library_dir();
@@ -409,10 +428,10 @@ void vkzg_prover_free(vkzg_prover *p) { delete p; }
 
 namespace {
 
-void collect_times(vkzg_prover *p, int stages, double *dst) {
+void collect_times(const cudaEvent_t *ev, int stages, double *dst) {
     for (int i = 0; i < stages; i++) {
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]);
+        cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
         dst[i] = ms;
     }
 }
@@ -424,7 +443,7 @@ vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, 
     CK(launch_proofs_timed(p->t, p->pw, (int)n, s, p->timing ? p->ev : nullptr));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (p->timing) collect_times(p, kProofStages, p->last_proof_ms);
+    if (p->timing) collect_times(p->ev, kProofStages, p->last_proof_ms);
     for (uint32_t b = 0; b < n; b++)
         if (p->h_err[b]) return VKZG_ERR_INVALID_BLOB;
     CK(cudaMemcpyAsync(proofs, p->pw.proofs, (size_t)n * kCells * kProofBytes, cudaMemcpyDeviceToHost, s));
@@ -444,10 +463,10 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
     const size_t bytes = (size_t)n * kExtElems * 32;
     CK(cudaMemcpyAsync(p->rw.cells, cells, bytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
-    CK(launch_recover_timed(p->t, p->rw, (int)n, s, p->timing ? p->ev : nullptr));
+    CK(launch_recover_timed(p->t, p->rw, (int)n, s, p->timing ? p->ev_rec : nullptr));
     CK(cudaMemcpyAsync(out, p->rw.out, bytes, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (p->timing) collect_times(p, kRecoverStages, p->last_recover_ms);
+    if (p->timing) collect_times(p->ev_rec, kRecoverStages, p->last_recover_ms);
     return VKZG_OK;
 }
 
@@ -494,6 +513,14 @@ void vkzg_b200_set_stage_timing(vkzg_prover *p, int enabled) {
 
 int vkzg_b200_last_stage_times(const vkzg_prover *p, int recovery, double *ms, int cap) {
     if (!p || !ms) return 0;
+    if (p->pending_proof && cudaEventQuery(p->ev[kProofStages]) == cudaSuccess) {
+        collect_times(p->ev, kProofStages, p->last_proof_ms);
+        p->pending_proof = false;
+    }
+    if (p->pending_recover && cudaEventQuery(p->ev_rec[kRecoverStages]) == cudaSuccess) {
+        collect_times(p->ev_rec, kRecoverStages, p->last_recover_ms);
+        p->pending_recover = false;
+    }
     const int n = recovery ? kRecoverStages : kProofStages;
     const double *src = recovery ? p->last_recover_ms : p->last_proof_ms;
     for (int i = 0; i < n && i < cap; i++) ms[i] = src[i];
@@ -535,4 +562,70 @@ vkzg_result vkzg_b200_write_tables(const uint8_t *g1_monomial_compressed, const 
               fwrite(&h.inv_blob, 1, sizeof h.inv_blob, f) == sizeof h.inv_blob;
     fclose(f);
     return ok ? VKZG_OK : VKZG_ERR_IO;
+}
+
+// ------------------------------------------------- device-pointer entry points
+
+namespace {
+
+// caller stream -> prover stream -> caller stream
+vkzg_result enter_stream(vkzg_prover *p, cudaStream_t caller) {
+    CK(cudaEventRecord(p->ev_in, caller));
+    CK(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+    return VKZG_OK;
+}
+vkzg_result leave_stream(vkzg_prover *p, cudaStream_t caller) {
+    CK(cudaEventRecord(p->ev_out, p->stream));
+    CK(cudaStreamWaitEvent(caller, p->ev_out, 0));
+    return VKZG_OK;
+}
+
+} // namespace
+
+vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, const uint8_t *d_blobs,
+                                            uint32_t *d_err, size_t num_blobs, void *stream) {
+    if (!p || !d_proofs || !d_blobs || !d_err) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    cudaStream_t caller = (cudaStream_t)stream;
+    vkzg_result rc = enter_stream(p, caller);
+    if (rc != VKZG_OK) return rc;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        ProofWork w = p->pw;
+        w.blobs = const_cast<uint8_t *>(d_blobs) + done * kBlobBytes;
+        w.proofs = d_proofs + done * kCells * kProofBytes;
+        w.err = d_err + done;
+        CK(cudaMemsetAsync(w.err, 0, n * sizeof(uint32_t), p->stream));
+        CK(launch_proofs_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev : nullptr));
+        done += n;
+    }
+    if (p->timing) p->pending_proof = true;
+    return leave_stream(p, caller);
+}
+
+vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,
+                                           const uint8_t *d_cell_present, uint32_t *d_err, size_t num_blobs,
+                                           void *stream) {
+    if (!p || !d_cells_out || !d_cells || !d_cell_present || !d_err) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    cudaStream_t caller = (cudaStream_t)stream;
+    vkzg_result rc = enter_stream(p, caller);
+    if (rc != VKZG_OK) return rc;
+    const size_t blob_bytes = (size_t)kExtElems * 32;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        RecoverWork w = p->rw;
+        w.cells = const_cast<uint8_t *>(d_cells) + done * blob_bytes;
+        w.present = const_cast<uint8_t *>(d_cell_present) + done * kCells;
+        w.out = d_cells_out + done * blob_bytes;
+        w.err = d_err + done;
+        CK(launch_recover_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev_rec : nullptr));
+        done += n;
+    }
+    if (p->timing) p->pending_recover = true;
+    return leave_stream(p, caller);
 }

@@ -31,7 +31,7 @@ constexpr int kRecThreads = 512;
 // inv_zc[c] = 1 / Zs(7^64 w_128^brev7(c))
 __global__ void __launch_bounds__(kCells) k_recover_prep(const uint8_t *__restrict__ present,
                                                         const Fr *__restrict__ roots_fwd, Fr seven64, Fr *zv,
-                                                        Fr *inv_zc) {
+                                                        Fr *inv_zc, uint32_t *err) {
     __shared__ uint8_t miss_root[kCells];
     __shared__ int n_miss;
     __shared__ Fr tree[2 * kCells];
@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(kCells) k_recover_prep(const uint8_t *__restri
         for (int i = 0; i < kCells; i++)
             if (!present[(size_t)b * kCells + i]) miss_root[n++] = (uint8_t)brev_bits((uint32_t)i, 7);
         n_miss = n;
+        if (err) err[b] = n > kCellElems ? 1u : 0u;
     }
     __syncthreads();
     const Fr x = ldg_vec(&roots_fwd[brev_bits((uint32_t)c, 7) * 64]);
@@ -149,7 +150,7 @@ cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, in
     if (n <= 0) return cudaSuccess;
     static const Fr seven64 = host_seven64();
     if (ev) cudaEventRecord(ev[0], s);
-    k_recover_prep<<<n, kCells, 0, s>>>(w.present, t.roots_fwd, seven64, w.zv, w.inv_zc);
+    k_recover_prep<<<n, kCells, 0, s>>>(w.present, t.roots_fwd, seven64, w.zv, w.inv_zc, w.err);
     if (ev) cudaEventRecord(ev[1], s);
     k_recover_main<<<n, kRecThreads, kBlobElems * sizeof(Fr), s>>>(w.cells, w.out, w.scratch, w.zv, w.inv_zc,
                                                                    t.roots_fwd, t.roots_inv, t.shift_fwd,
