@@ -53,6 +53,35 @@ vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out,
                                            void *stream);
 
 /*
+ * Allocation-free form of vkzg_b200_recover_cells_device.  No counterpart in
+ * the reference.
+ *
+ * For callers that must not allocate device memory at call time: code running
+ * where a framework's pool owns nearly all of HBM (an extra cudaMalloc would
+ * fail), latency-critical loops that cannot absorb the device-wide
+ * synchronisation a cudaMalloc/cudaFree can imply, and code that enqueues work
+ * on a stream it does not own.  This call allocates nothing and frees nothing:
+ * its scratch is a fixed array compiled into the library's device code (4.125
+ * MiB, resident on every GPU that loads the library until the process exits).
+ * Inputs and outputs are the caller's device buffers, laid out as for
+ * vkzg_b200_recover_cells_device; the work is enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) and the call returns after
+ * enqueueing.  The prover's device must be current.
+ *
+ * Limits: at most VKZG_B200_NOALLOC_MAX_BLOBS blobs per call; more returns
+ * VKZG_ERR_BADARGS without enqueueing anything.  The first call on a device
+ * looks up the scratch array's device address (cudaGetSymbolAddress) and caches
+ * it; make that first call before any stream capture.  Every call uses the same
+ * scratch, so calls whose work overlaps on the GPU (different streams with no
+ * ordering between them, or several threads) race and corrupt each other's
+ * results; order them on one stream.
+ */
+#define VKZG_B200_NOALLOC_MAX_BLOBS 16
+vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,
+                                                   const uint8_t *d_cell_present, uint32_t *d_err,
+                                                   size_t num_blobs, void *stream);
+
+/*
  * Throughput probes on the current device, for roofline denominators (the
  * reference has none).  which = 0: 32-bit integer multiply-add issue rate in
  * tera-ops/s; 1: this library's Fp (381-bit) Montgomery multiplies in giga-ops/s;

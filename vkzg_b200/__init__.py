@@ -35,8 +35,9 @@ EXPORTED_SYMBOLS = (
     "vkzg_recover_cells_batch",
     "vkzg_b200_write_tables", "vkzg_b200_prover_tables_source", "vkzg_b200_set_stage_timing",
     "vkzg_b200_last_stage_times", "vkzg_b200_stage_name", "vkzg_b200_compute_proofs_device",
-    "vkzg_b200_recover_cells_device", "vkzg_b200_microbench",
+    "vkzg_b200_recover_cells_device", "vkzg_b200_microbench", "vkzg_b200_recover_cells_device_noalloc",
 )
+NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
 
 class VkzgException(RuntimeError):
@@ -94,6 +95,8 @@ def library():
             L.vkzg_b200_recover_cells_device.restype = ctypes.c_int
             L.vkzg_b200_microbench.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
             L.vkzg_b200_microbench.restype = ctypes.c_int
+            L.vkzg_b200_recover_cells_device_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
+            L.vkzg_b200_recover_cells_device_noalloc.restype = ctypes.c_int
             _lib = L
     return _lib
 
@@ -200,6 +203,12 @@ class Prover:
 
     def recover_cells_device(self, d_out, d_cells, d_present, d_err, n, stream=None):
         return self._lib.vkzg_b200_recover_cells_device(self._h, d_out, d_cells, d_present, d_err, n, stream)
+
+    def recover_cells_device_noalloc(self, d_out, d_cells, d_present, d_err, n, stream=None):
+        """Allocation-free recovery on caller-owned device buffers (at most NOALLOC_MAX_BLOBS blobs);
+        scratch is a fixed array in the library's device memory shared by every call."""
+        return self._lib.vkzg_b200_recover_cells_device_noalloc(self._h, d_out, d_cells, d_present, d_err, n,
+                                                                stream)
 
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)

@@ -629,3 +629,26 @@ vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out,
     if (p->timing) p->pending_recover = true;
     return leave_stream(p, caller);
 }
+
+// ------------------------------------------------ allocation-free recovery
+
+namespace vkzg {
+int noalloc_max_blobs();
+cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, const uint8_t *present, uint8_t *out,
+                                   uint32_t *err, int n, cudaStream_t s);
+} // namespace vkzg
+
+vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,
+                                                   const uint8_t *d_cell_present, uint32_t *d_err,
+                                                   size_t num_blobs, void *stream) {
+    if (!p || !d_cells_out || !d_cells || !d_cell_present || !d_err) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    if (num_blobs > (size_t)noalloc_max_blobs()) return VKZG_ERR_BADARGS;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return VKZG_ERR_GPU;
+    if (dev != p->device) return VKZG_ERR_BADARGS;
+    if (launch_recover_noalloc(p->t, d_cells, d_cell_present, d_cells_out, d_err, (int)num_blobs,
+                               (cudaStream_t)stream) != cudaSuccess)
+        return VKZG_ERR_GPU;
+    return VKZG_OK;
+}

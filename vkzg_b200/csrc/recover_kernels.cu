@@ -22,6 +22,8 @@
 #include "device_util.cuh"
 #include "kernels.h"
 
+#include <mutex>
+
 namespace vkzg {
 
 constexpr int kRecThreads = 512;
@@ -166,6 +168,62 @@ cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, c
 cudaError_t configure_recover_kernels() {
     return cudaFuncSetAttribute(k_recover_main, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(kBlobElems * sizeof(Fr)));
+}
+
+// ------------------------------------------ allocation-free recovery variant
+// Scratch for vkzg_b200_recover_cells_device_noalloc: a fixed array in the
+// module's device memory instead of the prover's cudaMalloc'd working set.
+// Per blob: the 8192-element transform buffer, then Z on the domain and
+// 1/Z on the coset (128 elements each).  Every GPU that loads this library
+// holds it (4.125 MiB) until the process exits; all calls share it.
+constexpr int kNoAllocMaxBlobs = 16;
+constexpr size_t kNoAllocPerBlob = kExtElems + 2 * kCells;
+static __device__ __align__(256) Fr g_noalloc_scratch[kNoAllocMaxBlobs * kNoAllocPerBlob];
+
+namespace {
+std::mutex g_noalloc_mutex;
+Fr *g_noalloc_addr[64] = {};
+} // namespace
+
+// Device address of g_noalloc_scratch on the current device.  The host-side
+// symbol is only a stand-in; the address is fetched once per device.
+static cudaError_t noalloc_scratch_address(Fr **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[dev] = reinterpret_cast<Fr *>(ptr);
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+int noalloc_max_blobs() { return kNoAllocMaxBlobs; }
+
+// Same two kernels as launch_recover, with the per-blob scratch carved out of
+// g_noalloc_scratch.  Nothing in the scratch needs to start at zero: the prep
+// kernel writes zv / inv_zc and the main kernel writes each transform buffer
+// before reading it.
+cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, const uint8_t *present, uint8_t *out,
+                                   uint32_t *err, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    if (n > kNoAllocMaxBlobs) return cudaErrorInvalidValue;
+    Fr *base = nullptr;
+    cudaError_t e = noalloc_scratch_address(&base);
+    if (e != cudaSuccess) return e;
+    Fr *work = base;
+    Fr *zv = base + (size_t)kNoAllocMaxBlobs * kExtElems;
+    Fr *inv_zc = zv + (size_t)kNoAllocMaxBlobs * kCells;
+    static const Fr seven64 = host_seven64();
+    k_recover_prep<<<n, kCells, 0, s>>>(present, t.roots_fwd, seven64, zv, inv_zc, err);
+    k_recover_main<<<n, kRecThreads, kBlobElems * sizeof(Fr), s>>>(cells, out, work, zv, inv_zc, t.roots_fwd,
+                                                                   t.roots_inv, t.shift_fwd, t.shift_inv);
+    return cudaGetLastError();
 }
 
 } // namespace vkzg
