@@ -82,12 +82,34 @@ vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_ce
                                                    size_t num_blobs, void *stream);
 
 /*
+ * The 128 cells of each blob (the 2x Reed-Solomon extension, 128 x 2048 bytes
+ * per blob in cell order), and cells plus proofs in one call sharing one upload
+ * (the consensus specs' compute_cells_and_kzg_proofs).  The reference computes
+ * proofs only and leaves cells out (include/vkzg.h:16-18).  Same blob format and
+ * error rules as vkzg_compute_proofs_batch.
+ */
+vkzg_result vkzg_b200_compute_cells_batch(vkzg_prover *p, uint8_t *cells, const uint8_t *blobs, size_t num_blobs);
+vkzg_result vkzg_b200_compute_cells_and_proofs_batch(vkzg_prover *p, uint8_t *cells, uint8_t *proofs,
+                                                     const uint8_t *blobs, size_t num_blobs);
+
+/*
  * Throughput probes on the current device, for roofline denominators (the
  * reference has none).  which = 0: 32-bit integer multiply-add issue rate in
  * tera-ops/s; 1: this library's Fp (381-bit) Montgomery multiplies in giga-ops/s;
  * 2: Fr (255-bit) multiplies in giga-ops/s.  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
+
+/*
+ * Self-test of the batched-affine bucket summation the proof kernels use (the
+ * reference sums buckets serially, k_phase_a.comp:37-42): sums n <= 2048 affine
+ * points (96 bytes each, x || y canonical big-endian, all-zero = infinity) into
+ * 128 buckets (bucket_of[i] < 128) on the current device and writes the 128
+ * sums in the same encoding.  For tests of the doubling, cancellation and
+ * infinity cases that random inputs never reach.
+ */
+vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, const uint32_t *bucket_of, size_t n,
+                                           uint8_t *sums_xy);
 
 #ifdef __cplusplus
 } /* extern "C" */

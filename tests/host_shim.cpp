@@ -101,3 +101,17 @@ int shim_g1_mul(const uint8_t *p48, const uint32_t *k, uint8_t *out48) {
     return 0;
 }
 }
+
+#include "../vkzg_b200/csrc/inverse.cuh"
+extern "C" {
+void shim_fp_inv_fast(const uint32_t *a, uint32_t *r) {
+    Fp x;
+    memcpy(x.v, a, 48);
+    memcpy(r, fp_inv_fast(x).v, 48);
+}
+void shim_fr_inv_fast(const uint32_t *a, uint32_t *r) {
+    Fr x;
+    memcpy(x.v, a, 32);
+    memcpy(r, fr_inv_fast(x).v, 32);
+}
+}

@@ -141,3 +141,33 @@ def test_java_style_global_api(golden_proofs):
             vkzg_b200.computeCellKzgProofsBatch(b"\0" * 10, 1)
     finally:
         vkzg_b200.deinit()
+
+
+def test_cells_vectors(prover, golden_proofs):
+    """The vectors' 128 cells (present in tests/vectors, skipped by tests/vectors.h:88-95)."""
+    import hashlib
+    blobs = golden_proofs["valid_blobs"]
+    cells = prover.compute_cells_batch(blobs.tobytes(), len(blobs))
+    for k in range(len(blobs)):
+        digest = hashlib.sha256(cells[k * 262144:(k + 1) * 262144]).digest()
+        assert digest == golden_proofs["valid_cells_sha256"][k].tobytes(), k
+    cells2, proofs = prover.compute_cells_and_kzg_proofs_batch(blobs.tobytes(), len(blobs))
+    assert cells2 == cells
+    assert proofs == golden_proofs["valid_proofs"].tobytes()
+    with pytest.raises(vkzg_b200.VkzgException) as e:
+        prover.compute_cells_batch(golden_proofs["invalid_blob_0"].tobytes(), 1)
+    assert e.value.code == vkzg_b200.ERR_INVALID_BLOB
+
+
+def test_cells_then_recover_roundtrip(prover, golden_proofs):
+    """compute_cells -> erase half -> recover gives the cells back (size-independent check)."""
+    blobs = golden_proofs["valid_blobs"][2:5]
+    cells = np.frombuffer(prover.compute_cells_batch(blobs.tobytes(), 3), np.uint8).reshape(3, 128, 2048).copy()
+    present = np.ones((3, 128), np.uint8)
+    present[0, 64:] = 0
+    present[1, ::2] = 0
+    present[2, [3, 9, 77]] = 0
+    erased = cells.copy()
+    erased[present == 0] = 0x5A
+    out = prover.recover_cells_batch(erased.tobytes(), present.tobytes(), 3)
+    assert out == cells.tobytes()

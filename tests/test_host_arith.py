@@ -78,3 +78,19 @@ def test_curve_ops(shim, oracle, mainnet_setup):
         assert shim.shim_g1_mul(pts[1], words(k, 8), o) == 0
         _, want = oracle.g1_mul(pts[1], k.to_bytes(32, "big"))
         assert o.raw == want
+
+
+@pytest.mark.parametrize("field", ["fp", "fr"])
+def test_divstep_inverse(shim, field):
+    """Batched-divstep inversion (Montgomery in, Montgomery out) equals x^-1."""
+    mod, n, radix = (P_MOD, 12, 1 << 384) if field == "fp" else (R_MOD, 8, 1 << 256)
+    rng = random.Random(11)
+    vals = [1, 2, 3, mod - 1, mod - 2, (mod - 1) // 2, 1 << 200, (1 << 250) + 1, radix % mod]
+    vals += [rng.randrange(1, mod) for _ in range(3000)]
+    out = (ctypes.c_uint32 * n)()
+    fn = getattr(shim, f"shim_{field}_inv_fast")
+    for x in vals:
+        fn(words(x * radix % mod, n), out)
+        assert value(out, n) == pow(x, -1, mod) * radix % mod, hex(x)
+    fn(words(0, n), out)
+    assert value(out, n) == 0

@@ -36,6 +36,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_write_tables", "vkzg_b200_prover_tables_source", "vkzg_b200_set_stage_timing",
     "vkzg_b200_last_stage_times", "vkzg_b200_stage_name", "vkzg_b200_compute_proofs_device",
     "vkzg_b200_recover_cells_device", "vkzg_b200_microbench", "vkzg_b200_recover_cells_device_noalloc",
+    "vkzg_b200_bucket_sums_selftest", "vkzg_b200_compute_cells_batch", "vkzg_b200_compute_cells_and_proofs_batch",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -97,6 +98,12 @@ def library():
             L.vkzg_b200_microbench.restype = ctypes.c_int
             L.vkzg_b200_recover_cells_device_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
             L.vkzg_b200_recover_cells_device_noalloc.restype = ctypes.c_int
+            L.vkzg_b200_bucket_sums_selftest.argtypes = [vp, vp, ctypes.c_size_t, vp]
+            L.vkzg_b200_bucket_sums_selftest.restype = ctypes.c_int
+            L.vkzg_b200_compute_cells_batch.argtypes = [vp, vp, vp, ctypes.c_size_t]
+            L.vkzg_b200_compute_cells_batch.restype = ctypes.c_int
+            L.vkzg_b200_compute_cells_and_proofs_batch.argtypes = [vp, vp, vp, vp, ctypes.c_size_t]
+            L.vkzg_b200_compute_cells_and_proofs_batch.restype = ctypes.c_int
             _lib = L
     return _lib
 
@@ -210,6 +217,27 @@ class Prover:
         return self._lib.vkzg_b200_recover_cells_device_noalloc(self._h, d_out, d_cells, d_present, d_err, n,
                                                                 stream)
 
+    def compute_cells_batch(self, blobs, blob_count):
+        """The 128 cells of each blob (2x Reed-Solomon extension), wire order."""
+        if len(blobs) != blob_count * BYTES_PER_BLOB:
+            raise ValueError(f"blobs length must be blob_count * {BYTES_PER_BLOB}")
+        out = bytearray(max(1, blob_count * BYTES_PER_EXT_BLOB))
+        src = bytes(blobs) or b"\0"
+        _check(self._lib.vkzg_b200_compute_cells_batch(self._h, _ptr(out), _ptr(src), blob_count))
+        return bytes(out[:blob_count * BYTES_PER_EXT_BLOB])
+
+    def compute_cells_and_kzg_proofs_batch(self, blobs, blob_count):
+        """(cells, proofs) of each blob: the consensus specs' compute_cells_and_kzg_proofs."""
+        if len(blobs) != blob_count * BYTES_PER_BLOB:
+            raise ValueError(f"blobs length must be blob_count * {BYTES_PER_BLOB}")
+        cells = bytearray(max(1, blob_count * BYTES_PER_EXT_BLOB))
+        proofs = bytearray(max(1, blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF))
+        src = bytes(blobs) or b"\0"
+        _check(self._lib.vkzg_b200_compute_cells_and_proofs_batch(self._h, _ptr(cells), _ptr(proofs), _ptr(src),
+                                                                  blob_count))
+        return (bytes(cells[:blob_count * BYTES_PER_EXT_BLOB]),
+                bytes(proofs[:blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF]))
+
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)
 
@@ -224,6 +252,17 @@ def microbench(which):
     out = ctypes.c_double()
     _check(library().vkzg_b200_microbench(int(which), ctypes.byref(out)))
     return out.value
+
+
+def bucket_sums_selftest(points_xy, bucket_of):
+    """Sums affine points (n x 96 bytes, x || y canonical big-endian) into 128 buckets
+    with the device's batched-affine routine; returns 128 x 96 bytes."""
+    import numpy as np
+    pts = np.ascontiguousarray(np.frombuffer(bytes(points_xy), np.uint8))
+    idx = np.ascontiguousarray(np.asarray(bucket_of, dtype=np.uint32))
+    out = np.zeros(128 * 96, np.uint8)
+    _check(library().vkzg_b200_bucket_sums_selftest(_ptr(pts), _ptr(idx), len(idx), _ptr(out)))
+    return out.tobytes()
 
 
 def write_tables(g1_monomial_compressed, out_path):

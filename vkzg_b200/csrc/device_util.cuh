@@ -4,6 +4,7 @@
 #pragma once
 
 #include "curve.cuh"
+#include "inverse.cuh"
 
 namespace vkzg {
 
@@ -49,8 +50,9 @@ __device__ __forceinline__ G1J g1_shfl_down(const G1J &p, int delta) {
 
 // ------------------------------------------------------- batch inversion
 // Inverts one Fp per thread across a block of NT threads (power of two) with a
-// product tree in shared memory: NT-1 multiplies up, one Fermat inversion at
-// the root, 2(NT-1) down.  Zero inputs must be replaced by one by the caller.
+// product tree in shared memory: NT-1 multiplies up, one divstep inversion
+// (inverse.cuh) at the root, 2(NT-1) down.  Zero inputs must be replaced by
+// one by the caller.
 // `tree` holds 2*NT Fp.
 template <int NT>
 __device__ Fp block_batch_inverse_fp(const Fp &z, Fp *tree) {
@@ -65,7 +67,7 @@ __device__ Fp block_batch_inverse_fp(const Fp &z, Fp *tree) {
         }
         __syncthreads();
     }
-    if (t == 0) st_vec(&tree[1], fp_inv(ld_vec(&tree[1])));
+    if (t == 0) st_vec(&tree[1], fp_inv_fast(ld_vec(&tree[1])));
     __syncthreads();
     // push inverses down: inv(child) = inv(parent) * sibling
     for (int width = 1; width < NT; width <<= 1) {
@@ -95,7 +97,7 @@ __device__ Fr block_batch_inverse_fr(const Fr &z, Fr *tree) {
         }
         __syncthreads();
     }
-    if (t == 0) st_vec(&tree[1], fr_inv(ld_vec(&tree[1])));
+    if (t == 0) st_vec(&tree[1], fr_inv_fast(ld_vec(&tree[1])));
     __syncthreads();
     for (int width = 1; width < NT; width <<= 1) {
         if (t < width) {

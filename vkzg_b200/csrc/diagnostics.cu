@@ -2,8 +2,11 @@
 // rate and the library's own Fp / Fr Montgomery multiply rates.  The reference
 // has no counterpart; its README quotes only end-to-end timings.
 #include "../../include/vkzg_b200.h"
+#include "bucket_sum.cuh"
 #include "device_util.cuh"
 #include "kernels.h"
+
+#include <vector>
 
 namespace vkzg {
 
@@ -50,9 +53,103 @@ __global__ void __launch_bounds__(256) k_probe_fr(uint32_t seed, int iters, uint
     if ((a.v[0] ^ b.v[0]) == 0x12345678u) sink[0] = a.v[1];
 }
 
+// Sums caller-chosen points into 128 buckets with the batch-affine routine of
+// the proof kernels (one block), so tests can drive its special cases: repeated
+// points (doubling), P + -P, the point at infinity.
+__global__ void __launch_bounds__(kBAThreads) k_bucket_sums_selftest(const G1A *points, const uint32_t *start,
+                                                                     G1A *sums, G1A *scratch) {
+    __shared__ BucketSumShared<kBABuckets> sh;
+    if (threadIdx.x < kBABuckets) sh.cnt[threadIdx.x] = start[threadIdx.x + 1] - start[threadIdx.x];
+    __syncthreads();
+    auto src0 = [points, start](int k, uint32_t i) { return ld_vec(&points[start[k] + i]); };
+    int slot = 0;
+    const G1A *res = ba_bucket_sums<kBABuckets, 4>(sh, src0, scratch, scratch + 1088, slot);
+    if (threadIdx.x < kBABuckets) {
+        G1A v;
+        if (sh.cnt[threadIdx.x]) {
+            v = ld_vec(&res[sh.base[slot][threadIdx.x]]);
+        } else {
+            v.x = fp_zero();
+            v.y = fp_zero();
+        }
+        st_vec(&sums[threadIdx.x], v);
+    }
+}
+
 } // namespace vkzg
 
 using namespace vkzg;
+
+// points_xy: n affine points, 96 bytes each (x || y, canonical big-endian; all
+// zero = infinity); bucket_of: n bucket indices < 128.  sums_xy: 128 x 96 bytes.
+// At most 2048 points.
+extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, const uint32_t *bucket_of, size_t n,
+                                                      uint8_t *sums_xy) {
+    if (!points_xy || !bucket_of || !sums_xy || n > 2048) return VKZG_ERR_BADARGS;
+    std::vector<uint32_t> start(kBABuckets + 1, 0);
+    for (size_t i = 0; i < n; i++) {
+        if (bucket_of[i] >= (uint32_t)kBABuckets) return VKZG_ERR_BADARGS;
+        start[bucket_of[i] + 1]++;
+    }
+    for (int k = 0; k < kBABuckets; k++) start[k + 1] += start[k];
+    std::vector<uint32_t> cur(start.begin(), start.end() - 1);
+    std::vector<G1A> pts(n > 0 ? n : 1);
+    for (size_t i = 0; i < n; i++) {
+        G1A a;
+        bool inf = true;
+        for (int c = 0; c < 2; c++) {
+            Fp v;
+            for (int limb = 0; limb < 12; limb++) {
+                const uint8_t *b = points_xy + 96 * i + 48 * c + (11 - limb) * 4;
+                v.v[limb] = ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | b[3];
+            }
+            inf &= fp_is_zero(v);
+            (c == 0 ? a.x : a.y) = fp_from_canonical(v);
+        }
+        if (inf) a.x = a.y = fp_zero();
+        pts[cur[bucket_of[i]]++] = a;
+    }
+    G1A *d_pts = nullptr, *d_sums = nullptr, *d_scratch = nullptr;
+    uint32_t *d_start = nullptr;
+    vkzg_result rc = VKZG_OK;
+    if (cudaMalloc(&d_pts, pts.size() * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&d_sums, kBABuckets * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&d_scratch, (1088 + 608) * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&d_start, start.size() * 4) != cudaSuccess) {
+        rc = VKZG_ERR_MALLOC;
+    } else {
+        std::vector<G1A> sums(kBABuckets);
+        if (cudaMemcpy(d_pts, pts.data(), pts.size() * sizeof(G1A), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+            rc = VKZG_ERR_GPU;
+        } else {
+            k_bucket_sums_selftest<<<1, kBAThreads>>>(d_pts, d_start, d_sums, d_scratch);
+            if (cudaDeviceSynchronize() != cudaSuccess ||
+                cudaMemcpy(sums.data(), d_sums, kBABuckets * sizeof(G1A), cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = VKZG_ERR_GPU;
+        }
+        if (rc == VKZG_OK) {
+            for (int k = 0; k < kBABuckets; k++) {
+                const bool inf = g1a_is_identity(sums[k]);
+                for (int c = 0; c < 2; c++) {
+                    const Fp v = inf ? fp_zero() : fp_to_canonical(c == 0 ? sums[k].x : sums[k].y);
+                    for (int limb = 0; limb < 12; limb++) {
+                        uint8_t *b = sums_xy + 96 * k + 48 * c + (11 - limb) * 4;
+                        b[0] = (uint8_t)(v.v[limb] >> 24);
+                        b[1] = (uint8_t)(v.v[limb] >> 16);
+                        b[2] = (uint8_t)(v.v[limb] >> 8);
+                        b[3] = (uint8_t)v.v[limb];
+                    }
+                }
+            }
+        }
+    }
+    cudaFree(d_pts);
+    cudaFree(d_sums);
+    cudaFree(d_scratch);
+    cudaFree(d_start);
+    return rc;
+}
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {

@@ -1,0 +1,220 @@
+// Modular inversion by batched divsteps (Bernstein & Yang, "Fast constant-time
+// gcd computation and modular inversion", 2019), variable-time form.
+//
+// Fermat inversion (a^(m-2), what the reference uses: field.glsl.inc:257-275,
+// 528-547) is ~570 dependent Fp multiplies; on one GPU thread that is close to a
+// millisecond of latency, paid at the root of every batch inversion.  Divsteps
+// instead work on 30-bit digits: 30 divsteps on the low words of (f, g) give a
+// 2x2 integer matrix with entries below 2^30 in magnitude, which is then applied
+// to the full-width (f, g) and to the cofactors (d, e) (the latter modulo m,
+// divided by 2^30 with a Montgomery-style correction).  Invariants:
+//   f == d * x (mod m),  g == e * x (mod m),  f odd,  d, e in (-2m, m).
+// Starting from f = m, g = x, d = 0, e = 1, when g reaches 0, f = +-1 and
+// x^-1 = +-d.  Numbers are signed radix-2^30 limbs: limbs 0..L-2 in [0, 2^30),
+// the top limb signed.
+#pragma once
+
+#include "field.cuh"
+
+namespace vkzg {
+
+// m in radix 2^30 and m^-1 mod 2^30, for Fp (13 limbs) and Fr (9 limbs).
+VK_HD constexpr int32_t fp_m30(int i) {
+    return i == 0 ? 1073719979 : i == 1 ? 670826495 : i == 2 ? 356515835 : i == 3 ? 721420204
+         : i == 4 ? 821437470 : i == 5 ? 55215066 : i == 6 ? 288093811 : i == 7 ? 316751073
+         : i == 8 ? 752313463 : i == 9 ? 517541166 : i == 10 ? 698659258 : i == 11 ? 982409209 : 1704209;
+}
+VK_HD constexpr int32_t fr_m30(int i) {
+    return i == 0 ? 1 : i == 1 ? 1073741820 : i == 2 ? 1072021487 : i == 3 ? 795410623
+         : i == 4 ? 567805267 : i == 5 ? 660611110 : i == 6 ? 399803187 : i == 7 ? 701811303 : 29677;
+}
+template <int N>
+VK_HD constexpr int32_t mod_m30(int i) {
+    return N == 12 ? fp_m30(i) : fr_m30(i);
+}
+template <int N>
+VK_HD constexpr uint32_t mod_minv30() {
+    return N == 12 ? 196611u : 1u;
+}
+
+constexpr uint32_t kMask30 = (1u << 30) - 1;
+
+// 30 divsteps on the low words.  delta as in the paper (starts at 1).  Returns
+// the transition matrix scaled by 2^30: 2^30 [f', g'] = [[u, v], [q, r]] [f, g].
+VK_HD void divsteps30(int32_t &delta, uint32_t f, uint32_t g, int32_t &u, int32_t &v, int32_t &q, int32_t &r) {
+    u = 1; v = 0; q = 0; r = 1;
+    for (int i = 0; i < 30; i++) {
+        const uint32_t odd = g & 1u;
+        const uint32_t swap = odd & (delta > 0 ? 1u : 0u);
+        const uint32_t m_odd = 0u - odd, m_swap = 0u - swap;
+        // with a swap the pair becomes (g, (g - f) / 2); otherwise (f, (g + odd*f) / 2)
+        const uint32_t fs = (f ^ m_swap) - m_swap;      // -f on a swap
+        const int32_t us = (int32_t)(((uint32_t)u ^ m_swap) - m_swap);
+        const int32_t vs = (int32_t)(((uint32_t)v ^ m_swap) - m_swap);
+        const uint32_t g_new = (g + (fs & m_odd)) >> 1;  // only the low bits matter
+        const int32_t q_new = q + (int32_t)((uint32_t)us & m_odd);
+        const int32_t r_new = r + (int32_t)((uint32_t)vs & m_odd);
+        const uint32_t f_new = swap ? g : f;
+        const int32_t u_new = swap ? q : u, v_new = swap ? r : v;
+        delta = swap ? 1 - delta : 1 + delta;
+        f = f_new;
+        g = g_new;
+        u = u_new * 2;
+        v = v_new * 2;
+        q = q_new;
+        r = r_new;
+    }
+}
+
+// (f, g) <- ([[u, v], [q, r]] (f, g)) / 2^30, exact.
+template <int L>
+VK_HD void update_fg30(int32_t *f, int32_t *g, int32_t u, int32_t v, int32_t q, int32_t r) {
+    int64_t cf = (int64_t)u * f[0] + (int64_t)v * g[0];
+    int64_t cg = (int64_t)q * f[0] + (int64_t)r * g[0];
+    cf >>= 30;
+    cg >>= 30;
+    for (int i = 1; i < L; i++) {
+        cf += (int64_t)u * f[i] + (int64_t)v * g[i];
+        cg += (int64_t)q * f[i] + (int64_t)r * g[i];
+        f[i - 1] = (int32_t)((uint32_t)cf & kMask30);
+        g[i - 1] = (int32_t)((uint32_t)cg & kMask30);
+        cf >>= 30;
+        cg >>= 30;
+    }
+    f[L - 1] = (int32_t)cf;
+    g[L - 1] = (int32_t)cg;
+}
+
+// (d, e) <- ([[u, v], [q, r]] (d, e)) / 2^30 mod m, kept in (-2m, m): a
+// multiple of m chosen from the signs of d, e plus a correction making the sum
+// divisible by 2^30 is added before the shift.
+template <int N, int L>
+VK_HD void update_de30(int32_t *d, int32_t *e, int32_t u, int32_t v, int32_t q, int32_t r) {
+    const int32_t sd = d[L - 1] >> 31, se = e[L - 1] >> 31;  // -1 when negative
+    int32_t md = (u & sd) + (v & se);
+    int32_t me = (q & sd) + (r & se);
+    int64_t cd = (int64_t)u * d[0] + (int64_t)v * e[0];
+    int64_t ce = (int64_t)q * d[0] + (int64_t)r * e[0];
+    md -= (int32_t)((mod_minv30<N>() * (uint32_t)cd + (uint32_t)md) & kMask30);
+    me -= (int32_t)((mod_minv30<N>() * (uint32_t)ce + (uint32_t)me) & kMask30);
+    cd += (int64_t)mod_m30<N>(0) * md;
+    ce += (int64_t)mod_m30<N>(0) * me;
+    cd >>= 30;
+    ce >>= 30;
+    for (int i = 1; i < L; i++) {
+        cd += (int64_t)u * d[i] + (int64_t)v * e[i] + (int64_t)mod_m30<N>(i) * md;
+        ce += (int64_t)q * d[i] + (int64_t)r * e[i] + (int64_t)mod_m30<N>(i) * me;
+        d[i - 1] = (int32_t)((uint32_t)cd & kMask30);
+        e[i - 1] = (int32_t)((uint32_t)ce & kMask30);
+        cd >>= 30;
+        ce >>= 30;
+    }
+    d[L - 1] = (int32_t)cd;
+    e[L - 1] = (int32_t)ce;
+}
+
+// Adds k*m to a signed radix-2^30 number (k small), renormalising limbs.
+template <int N, int L>
+VK_HD void add_m30(int32_t *a, int32_t k) {
+    int64_t c = 0;
+    for (int i = 0; i < L; i++) {
+        c += (int64_t)a[i] + (int64_t)k * mod_m30<N>(i);
+        if (i < L - 1) {
+            a[i] = (int32_t)((uint32_t)c & kMask30);
+            c >>= 30;
+        } else {
+            a[i] = (int32_t)c;
+        }
+    }
+}
+
+// sign of a normalised signed radix-2^30 number compared with m: returns true when a >= m
+template <int N, int L>
+VK_HD bool ge_m30(const int32_t *a) {
+    for (int i = L - 1; i >= 0; i--) {
+        if (a[i] != mod_m30<N>(i)) return a[i] > mod_m30<N>(i);
+    }
+    return true;
+}
+
+// x^-1 mod m for a plain integer x < m given as N 32-bit words (0 -> 0).
+template <int N>
+VK_HD void inverse_words(uint32_t *out, const uint32_t *x) {
+    constexpr int L = N == 12 ? 13 : 9;
+    int32_t f[L], g[L], d[L], e[L];
+    // words -> radix 2^30
+    {
+        int acc_bits = 0, w = 0;
+        uint64_t acc = 0;
+        for (int i = 0; i < L; i++) {
+            while (acc_bits < 30 && w < N) {
+                acc |= (uint64_t)x[w++] << acc_bits;
+                acc_bits += 32;
+            }
+            g[i] = (int32_t)((uint32_t)acc & kMask30);
+            acc >>= 30;
+            acc_bits -= 30;
+            if (acc_bits < 0) acc_bits = 0;
+            f[i] = mod_m30<N>(i);
+            d[i] = 0;
+            e[i] = 0;
+        }
+    }
+    e[0] = 1;
+    int32_t delta = 1;
+    bool g_zero = true;
+    for (int i = 0; i < L; i++) g_zero &= g[i] == 0;
+    if (g_zero) {
+        for (int i = 0; i < N; i++) out[i] = 0;
+        return;
+    }
+    // 64 batches = 1920 divsteps, beyond the worst case for a 381-bit modulus
+    for (int it = 0; it < 64 && !g_zero; it++) {
+        int32_t u, v, q, r;
+        divsteps30(delta, (uint32_t)f[0], (uint32_t)g[0], u, v, q, r);
+        update_de30<N, L>(d, e, u, v, q, r);
+        update_fg30<L>(f, g, u, v, q, r);
+        g_zero = true;
+        for (int i = 0; i < L; i++) g_zero &= g[i] == 0;
+    }
+    // f = +-1: x^-1 = f * d, then into [0, m)
+    if (f[L - 1] < 0) {
+        for (int i = 0; i < L; i++) d[i] = -d[i];
+        add_m30<N, L>(d, 0); // renormalise limbs after negation
+    }
+    while (d[L - 1] < 0) add_m30<N, L>(d, 1);
+    while (ge_m30<N, L>(d)) add_m30<N, L>(d, -1);
+    // radix 2^30 -> words
+    {
+        uint64_t acc = 0;
+        int acc_bits = 0, i = 0;
+        for (int w = 0; w < N; w++) {
+            while (acc_bits < 32 && i < L) {
+                acc |= (uint64_t)(uint32_t)d[i++] << acc_bits;
+                acc_bits += 30;
+            }
+            out[w] = (uint32_t)acc;
+            acc >>= 32;
+            acc_bits -= 32;
+        }
+    }
+}
+
+// Montgomery-form inverses: for a = x R, inverse_words gives (x R)^-1; one
+// Montgomery product with R^3 gives x^-1 R.
+VK_HD Fp fp_inv_fast(const Fp &a) {
+    Fp raw;
+    inverse_words<12>(raw.v, a.v);
+    const Fp r3 = Fp{{0xd94ca1e0u, 0xed48ac6bu, 0x03a7adf8u, 0x315f831eu, 0x615e29ddu, 0x9a53352au, 0x921e1761u,
+                      0x34c04e5eu, 0x65724728u, 0x2512d435u, 0x91755d4du, 0x0aa63460u}};
+    return fp_mul(r3, raw);
+}
+VK_HD Fr fr_inv_fast(const Fr &a) {
+    Fr raw;
+    inverse_words<8>(raw.v, a.v);
+    const Fr r3 = Fr{{0x439b73afu, 0xc62c1807u, 0x8cf06990u, 0x1b3e0d18u, 0xc7b5f418u, 0x73d13c71u, 0xc8db33e9u,
+                      0x6e2a5bb9u}};
+    return fr_mul(r3, raw);
+}
+
+} // namespace vkzg

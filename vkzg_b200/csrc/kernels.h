@@ -49,7 +49,16 @@ struct ProofWork {
     G1A *ladder_aff = nullptr;  // [cap][128][32]
     uint8_t *proofs = nullptr;  // [cap][128][48]
     uint32_t *err = nullptr;    // [cap]
+    // batch-affine accumulation (accum_mode 1)
+    G1A *bucket_aff = nullptr;  // [cap][128][128] affine bucket sums
+    G1A *ba_scratch = nullptr;  // [ba_blocks][kBAScratchPoints]
+    int ba_blocks = 0;          // persistent grid size of the batch-affine kernels
+    int accum_mode = 1;         // 0: serial Jacobian buckets, 1: batch-affine rounds
 };
+// MSM outputs per batch-affine block, and its scratch: round-1 and round-2 outputs
+// of 2048 points in 128 buckets per output
+constexpr int kBAOutputs = 8;
+constexpr int kBAScratchPoints = kBAOutputs * (1088 + 608);
 
 struct RecoverWork {
     uint8_t *cells = nullptr;     // [cap][8192*32]

@@ -15,8 +15,11 @@
 //   4'k_reduce
 //   9 k_finish           combine C+ +- C-, normalise, compress, write slot brev7(a)
 //                                                           (k_combine_split, k_normalize, k_compress_proofs)
+#include "bucket_sum.cuh"
 #include "device_util.cuh"
 #include "kernels.h"
+
+#include <algorithm>
 
 namespace vkzg {
 
@@ -300,6 +303,175 @@ __global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, ui
     dst[2] = e4[2];
 }
 
+// ------------------------------------------- batch-affine phase A / phase B
+// Persistent blocks: block x owns scratch slot x and walks work items of
+// kBAOutputs consecutive outputs of one blob with stride gridDim.x.  Output:
+// affine bucket sums bucket_aff[blob][output][k], infinity for empty buckets.
+constexpr int kBANB = kBAOutputs * kBuckets;
+constexpr int kBAMaxPairs = kBAOutputs * kCellElems * kDigits / 2 / kBAThreads;
+constexpr size_t kPhaseADynSmem = (2 * kBANB + 4) * sizeof(uint32_t) + kBAOutputs * kCellElems * kDigits * 2;
+
+// Block-wide exclusive scan of cnt[0..NB) into start[0..NB] (partials per thread).
+template <int NB>
+__device__ void block_exclusive_scan(const uint32_t *cnt, uint32_t *start, uint32_t *part) {
+    constexpr int per = (NB + kBAThreads - 1) / kBAThreads;
+    const int t = threadIdx.x, lo = t * per;
+    uint32_t p = 0;
+    for (int k = lo; k < lo + per && k < NB; k++) p += cnt[k];
+    part[t] = p;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t a = 0;
+        for (int q = 0; q < kBAThreads; q++) {
+            const uint32_t x = part[q];
+            part[q] = a;
+            a += x;
+        }
+        start[NB] = a;
+    }
+    __syncthreads();
+    p = part[t];
+    for (int k = lo; k < lo + per && k < NB; k++) {
+        start[k] = p;
+        p += cnt[k];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB> &sh, const G1A *res, int slot,
+                                                  G1A *out /* [kBANB] */) {
+    for (int k = threadIdx.x; k < kBANB; k += kBAThreads) {
+        G1A v;
+        if (sh.cnt[k]) {
+            v = ld_vec(&res[sh.base[slot][k]]);
+        } else {
+            v.x = fp_zero();
+            v.y = fp_zero();
+        }
+        st_vec(&out[k], v);
+    }
+}
+
+__global__ void __launch_bounds__(kBAThreads, 2) k_phase_a_affine(const Fr *__restrict__ scalars,
+                                                                 const G1A *__restrict__ pos, G1A *bucket_aff,
+                                                                 G1A *scratch, int n_work) {
+    __shared__ BucketSumShared<kBANB> sh;
+    // dynamic: start[kBANB + 1], cursor[kBANB], items[kBAOutputs * 2048] (kPhaseADynSmem bytes)
+    extern __shared__ uint4 dyn_smem[];
+    uint32_t *start = reinterpret_cast<uint32_t *>(dyn_smem);
+    uint32_t *cursor = start + kBANB + 4;
+    uint16_t *items = reinterpret_cast<uint16_t *>(cursor + kBANB);
+    G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
+    const int tid = threadIdx.x;
+    constexpr int kScalarsPerThread = kBAOutputs * kCellElems / kBAThreads;
+    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const int o0 = w * kBAOutputs; // first output (blob * 128 + j0)
+        for (int k = tid; k < kBANB; k += kBAThreads) sh.cnt[k] = 0;
+        __syncthreads();
+        Fr sc[kScalarsPerThread];
+        for (int r = 0; r < kScalarsPerThread; r++) {
+            const int q = tid + r * kBAThreads, g = q / kCellElems, i = q % kCellElems;
+            sc[r] = ld_vec(&scalars[((size_t)o0 + g) * kCellElems + i]);
+            int carry = 0;
+            for (int dd = 0; dd < kDigits; dd++) {
+                const int v = recode_digit(sc[r], dd, carry);
+                if (v) atomicAdd(&sh.cnt[g * kBuckets + abs(v) - 1], 1u);
+            }
+        }
+        __syncthreads();
+        block_exclusive_scan<kBANB>(sh.cnt, start, sh.part[0]);
+        for (int k = tid; k < kBANB; k += kBAThreads) cursor[k] = start[k];
+        __syncthreads();
+        for (int r = 0; r < kScalarsPerThread; r++) {
+            const int q = tid + r * kBAThreads, g = q / kCellElems, i = q % kCellElems;
+            int carry = 0;
+            for (int dd = 0; dd < kDigits; dd++) {
+                const int v = recode_digit(sc[r], dd, carry);
+                if (v) {
+                    const uint32_t slot = atomicAdd(&cursor[g * kBuckets + abs(v) - 1], 1u);
+                    items[slot] = (uint16_t)((i << 6) | (dd << 1) | (v < 0 ? 1 : 0));
+                }
+            }
+        }
+        __syncthreads();
+        const G1A *t0 = pos + (size_t)(o0 % kCells) * kCellElems * kDigits;
+        auto src0 = [t0, items, start](int k, uint32_t e) {
+            const uint32_t packed = items[start[k] + e];
+            const G1A *tj = t0 + (size_t)(k >> 7) * kCellElems * kDigits;
+            G1A pt = ldg_vec(&tj[(packed >> 6) * kDigits + ((packed >> 1) & 31u)]);
+            if (packed & 1u) pt.y = fp_neg(pt.y);
+            return pt;
+        };
+        int slot = 0;
+        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs>(sh, src0, buf0, buf1, slot);
+        store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kBAThreads, 2) k_phase_b_affine(const G1A *__restrict__ ladder_aff,
+                                                                 const uint32_t *__restrict__ items_p,
+                                                                 const uint32_t *__restrict__ off_p,
+                                                                 const uint32_t *__restrict__ items_m,
+                                                                 const uint32_t *__restrict__ off_m, G1A *bucket_aff,
+                                                                 G1A *scratch, int n_work) {
+    __shared__ BucketSumShared<kBANB> sh;
+    G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
+    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const int o0 = w * kBAOutputs, b = o0 / kCells, a0 = o0 % kCells;
+        const bool minus = a0 >= kHalf; // the kBAOutputs outputs share a half
+        const uint32_t *items = minus ? items_m : items_p;
+        const uint32_t *off = minus ? off_m : off_p;
+        for (int k = threadIdx.x; k < kBANB; k += kBAThreads) {
+            const int kk = k & (kBuckets - 1);
+            sh.cnt[k] = __ldg(&off[kk + 1]) - __ldg(&off[kk]);
+        }
+        __syncthreads();
+        const G1A *lad = ladder_aff + ((size_t)b * kCells + (minus ? kHalf : 0)) * kDigits;
+        auto src0 = [=](int k, uint32_t e) {
+            const int aa = (a0 + (k >> 7)) & (kHalf - 1);
+            const uint32_t packed = __ldg(&items[__ldg(&off[k & (kBuckets - 1)]) + e]);
+            const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
+            G1A pt = ld_vec(&lad[((aa - tap) & (kHalf - 1)) * kDigits + d]);
+            if (((packed >> 16) & 1u) != (minus && tap > aa)) pt.y = fp_neg(pt.y);
+            return pt;
+        };
+        int slot = 0;
+        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs>(sh, src0, buf0, buf1, slot);
+        store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
+        __syncthreads();
+    }
+}
+
+// k_reduce over affine bucket sums: s += B_k is a mixed addition.
+__global__ void __launch_bounds__(kReduceThreads) k_reduce_affine(const G1A *__restrict__ buckets, G1J *out,
+                                                                 int n_outputs) {
+    __shared__ G1J sh_s[kReduceThreads], sh_w[kReduceThreads];
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = gid / kReduceLanes, lane = gid % kReduceLanes;
+    constexpr int per = kBuckets / kReduceLanes;
+    G1J s = g1_identity(), w = g1_identity();
+    if (o < n_outputs) {
+        const G1A *bk = buckets + (size_t)o * kBuckets + lane * per;
+        for (int k = per - 1; k >= 0; k--) {
+            s = g1_madd(s, ld_vec(&bk[k]));
+            w = g1_add(w, s);
+        }
+    }
+    st_vec(&sh_s[threadIdx.x], s);
+    st_vec(&sh_w[threadIdx.x], w);
+    __syncthreads();
+    if (lane != 0 || o >= n_outputs) return;
+    G1J run = g1_identity(), acc = g1_identity();
+    for (int l = kReduceLanes - 1; l >= 1; l--) {
+        run = g1_add(run, ld_vec(&sh_s[threadIdx.x + l]));
+        acc = g1_add(acc, run);
+        w = g1_add(w, ld_vec(&sh_w[threadIdx.x + l]));
+    }
+    for (int q = 0; q < 4; q++) acc = g1_dbl(acc);
+    st_vec(&out[o], g1_add(w, acc));
+}
+
 // ---------------------------------------------------------------- launcher
 // ev (nullable): kProofStages + 1 events recorded around the stages.
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev) {
@@ -317,9 +489,19 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
     mark();
-    k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
-    mark();
-    k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    const bool affine = w.accum_mode == 1 && w.ba_blocks > 0;
+    const int ba_work = n_out / kBAOutputs;
+    const int ba_grid = std::min(w.ba_blocks, ba_work);
+    if (affine) {
+        k_phase_a_affine<<<ba_grid, kBAThreads, kPhaseADynSmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
+                                                                      ba_work);
+        mark();
+        k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
+    } else {
+        k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
+        mark();
+        k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    }
     mark();
     k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
     mark();
@@ -327,10 +509,19 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     mark();
-    k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0], t.tap_perm[0],
-                                                   t.tap_items[1], t.tap_offsets[1], t.tap_perm[1], w.buckets);
-    mark();
-    k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    if (affine) {
+        k_phase_b_affine<<<ba_grid, kBAThreads, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
+                                                        t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
+                                                        w.ba_scratch, ba_work);
+        mark();
+        k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
+    } else {
+        k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
+                                                       t.tap_perm[0], t.tap_items[1], t.tap_offsets[1],
+                                                       t.tap_perm[1], w.buckets);
+        mark();
+        k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+    }
     mark();
     k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
     mark();
@@ -341,9 +532,19 @@ cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cuda
     return launch_proofs_timed(t, w, n, s, nullptr);
 }
 
+// Resident blocks per SM of the batch-affine kernels (sizes their persistent grid).
+int batch_affine_blocks_per_sm() {
+    int a = 0, b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_phase_a_affine, kBAThreads, kPhaseADynSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_phase_b_affine, kBAThreads, 0);
+    return std::max(1, std::min(a, b));
+}
+
 cudaError_t configure_proof_kernels() {
-    return cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kBlobElems * sizeof(Fr)));
+    cudaError_t e = cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kBlobElems * sizeof(Fr)));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseADynSmem);
 }
 
 } // namespace vkzg

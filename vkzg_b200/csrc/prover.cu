@@ -26,6 +26,7 @@ using namespace vkzg;
 namespace vkzg {
 cudaError_t configure_proof_kernels();
 cudaError_t configure_recover_kernels();
+int batch_affine_blocks_per_sm();
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s,
                                 cudaEvent_t *ev);
 cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
@@ -336,6 +337,13 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
               p->alloc(r.zv, B * kCells) && p->alloc(r.inv_zc, B * kCells) && p->alloc(r.err, B);
     if (!ok) return VKZG_ERR_MALLOC;
     if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
+    // batch-affine bucket accumulation: one scratch slot per resident block
+    const char *mode = getenv("VKZG_ACCUM");
+    w.accum_mode = (mode && strcmp(mode, "jacobian") == 0) ? 0 : 1;
+    w.ba_blocks = (int)p->sm_count * batch_affine_blocks_per_sm();
+    if (!p->alloc(w.bucket_aff, B * kCells * kBuckets) ||
+        !p->alloc(w.ba_scratch, (size_t)w.ba_blocks * kBAScratchPoints))
+        return VKZG_ERR_MALLOC;
     return VKZG_OK;
 }
 
@@ -651,4 +659,63 @@ vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_ce
                                (cudaStream_t)stream) != cudaSuccess)
         return VKZG_ERR_GPU;
     return VKZG_OK;
+}
+
+// ------------------------------------------------- cells (2x RS extension)
+
+namespace vkzg {
+cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, Fr *scratch, uint32_t *err,
+                         int n, cudaStream_t s);
+cudaError_t configure_cells_kernels();
+} // namespace vkzg
+
+namespace {
+
+// One chunk of compute_cells / compute_cells_and_kzg_proofs: one upload, both
+// pipelines on the same device copy of the blobs, outputs written only when
+// every blob of the chunk is canonical (the proofs path's rule).
+vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
+    static const cudaError_t configured = configure_cells_kernels();
+    if (configured != cudaSuccess) return VKZG_ERR_GPU;
+    cudaStream_t s = p->stream;
+    CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+    CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->rw.scratch, p->pw.err, (int)n, s));
+    if (proofs) CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
+    CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (uint32_t b = 0; b < n; b++)
+        if (p->h_err[b]) return VKZG_ERR_INVALID_BLOB;
+    CK(cudaMemcpyAsync(cells, p->rw.out, (size_t)n * kExtElems * 32, cudaMemcpyDeviceToHost, s));
+    if (proofs) CK(cudaMemcpyAsync(proofs, p->pw.proofs, (size_t)n * kCells * kProofBytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return VKZG_OK;
+}
+
+vkzg_result cells_batch(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const uint8_t *blobs, size_t num_blobs) {
+    if (!p || !cells || !blobs) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        const vkzg_result rc = cells_chunk(p, cells + done * (size_t)kExtElems * 32,
+                                           proofs ? proofs + done * kCells * kProofBytes : nullptr,
+                                           blobs + done * kBlobBytes, n);
+        if (rc != VKZG_OK) return rc;
+        done += n;
+    }
+    return VKZG_OK;
+}
+
+} // namespace
+
+vkzg_result vkzg_b200_compute_cells_batch(vkzg_prover *p, uint8_t *cells, const uint8_t *blobs, size_t num_blobs) {
+    return cells_batch(p, cells, nullptr, blobs, num_blobs);
+}
+
+vkzg_result vkzg_b200_compute_cells_and_proofs_batch(vkzg_prover *p, uint8_t *cells, uint8_t *proofs,
+                                                     const uint8_t *blobs, size_t num_blobs) {
+    if (!proofs) return VKZG_ERR_BADARGS;
+    return cells_batch(p, cells, proofs, blobs, num_blobs);
 }
