@@ -93,6 +93,32 @@ vkzg_result vkzg_b200_compute_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
                                                      const uint8_t *blobs, size_t num_blobs);
 
 /*
+ * Recovered cells and the proofs of the recovered blob in one call (the
+ * consensus specs' recover_cells_and_kzg_proofs; the reference recovers cells
+ * only, include/vkzg.h:106-121).  Same inputs and error rules as
+ * vkzg_recover_cells_batch; proofs_out receives num_blobs x 128 x 48 bytes.
+ */
+vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *cells_out, uint8_t *proofs_out,
+                                                     const uint8_t *cells, const uint8_t *cell_present,
+                                                     size_t num_blobs);
+
+/*
+ * Autotuner.  Proof chunks run under one of three plans that compute identical
+ * bytes: 0 = serial Jacobian bucket accumulation and reduction (one output per
+ * block, the reference's scheme, k_phase_a.comp / k_bucket_reduce.comp);
+ * 1 = batch-affine bucket accumulation and a binary-split batch-affine
+ * reduction; 2 = batch-affine accumulation with the serial reduction.  The
+ * first chunk of each power-of-two size class is timed under all plans and the
+ * fastest is kept (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
+ * vkzg_b200_autotune tunes every size class up to max_blobs (0 = the prover's
+ * max_batch_size) on seeded synthetic blobs; vkzg_b200_tuning_table reports the
+ * decisions (size class, plan, and the three plans' times in ms, -1 if loaded
+ * from the cache) and returns how many classes are tuned.
+ */
+vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
+int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms3, int cap);
+
+/*
  * Throughput probes on the current device, for roofline denominators (the
  * reference has none).  which = 0: 32-bit integer multiply-add issue rate in
  * tera-ops/s; 1: this library's Fp (381-bit) Montgomery multiplies in giga-ops/s;

@@ -171,3 +171,16 @@ def test_cells_then_recover_roundtrip(prover, golden_proofs):
     erased[present == 0] = 0x5A
     out = prover.recover_cells_batch(erased.tobytes(), present.tobytes(), 3)
     assert out == cells.tobytes()
+
+
+def test_recovery_vectors_with_proofs(prover, golden_recover):
+    """recover_cells_and_kzg_proofs: cells and the recovered blob's proofs (output[1] of the
+    recovery vectors, which tests/vectors.h:8-10 leaves unchecked)."""
+    names = [n for n in golden_recover["names"] if n + "__expected" in golden_recover.files]
+    ins = [recover_inputs(golden_recover, n) for n in names]
+    cells = np.concatenate([c for c, _ in ins])
+    present = np.concatenate([p for _, p in ins])
+    out, proofs = prover.recover_cells_and_kzg_proofs_batch(cells.tobytes(), present.tobytes(), len(names))
+    for k, n in enumerate(names):
+        assert out[k * 262144:(k + 1) * 262144] == golden_recover[n + "__expected"].tobytes(), n
+        assert proofs[k * 6144:(k + 1) * 6144] == golden_recover[n + "__proofs"].tobytes(), n

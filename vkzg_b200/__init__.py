@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_last_stage_times", "vkzg_b200_stage_name", "vkzg_b200_compute_proofs_device",
     "vkzg_b200_recover_cells_device", "vkzg_b200_microbench", "vkzg_b200_recover_cells_device_noalloc",
     "vkzg_b200_bucket_sums_selftest", "vkzg_b200_compute_cells_batch", "vkzg_b200_compute_cells_and_proofs_batch",
+    "vkzg_b200_autotune", "vkzg_b200_tuning_table", "vkzg_b200_recover_cells_and_proofs_batch",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -104,6 +105,12 @@ def library():
             L.vkzg_b200_compute_cells_batch.restype = ctypes.c_int
             L.vkzg_b200_compute_cells_and_proofs_batch.argtypes = [vp, vp, vp, vp, ctypes.c_size_t]
             L.vkzg_b200_compute_cells_and_proofs_batch.restype = ctypes.c_int
+            L.vkzg_b200_autotune.argtypes = [vp, ctypes.c_uint32]
+            L.vkzg_b200_autotune.restype = ctypes.c_int
+            L.vkzg_b200_tuning_table.argtypes = [vp, vp, vp, vp, ctypes.c_int]
+            L.vkzg_b200_tuning_table.restype = ctypes.c_int
+            L.vkzg_b200_recover_cells_and_proofs_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t]
+            L.vkzg_b200_recover_cells_and_proofs_batch.restype = ctypes.c_int
             _lib = L
     return _lib
 
@@ -237,6 +244,31 @@ class Prover:
                                                                   blob_count))
         return (bytes(cells[:blob_count * BYTES_PER_EXT_BLOB]),
                 bytes(proofs[:blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF]))
+
+    def recover_cells_and_kzg_proofs_batch(self, cells, cell_present, blob_count):
+        """(cells, proofs): recovery, then the proofs of the recovered blob (recover_cells_and_kzg_proofs)."""
+        if len(cells) != blob_count * BYTES_PER_EXT_BLOB or len(cell_present) != blob_count * CELL_PROOFS_PER_BLOB:
+            raise ValueError("cells / cell_present length")
+        out = bytearray(max(1, len(cells)))
+        proofs = bytearray(max(1, blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF))
+        c, pr = bytes(cells) or b"\0", bytes(cell_present) or b"\0"
+        _check(self._lib.vkzg_b200_recover_cells_and_proofs_batch(self._h, _ptr(out), _ptr(proofs), _ptr(c), _ptr(pr),
+                                                                  blob_count))
+        return bytes(out[:len(cells)]), bytes(proofs[:blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF])
+
+    def autotune(self, max_blobs=0):
+        """Times the three proof plans for every power-of-two size class up to max_blobs."""
+        _check(self._lib.vkzg_b200_autotune(self._h, int(max_blobs)))
+        return self.tuning_table()
+
+    def tuning_table(self):
+        """{size_class: (plan, (ms_plan0, ms_plan1, ms_plan2))}"""
+        cap = 32
+        sc = (ctypes.c_uint32 * cap)()
+        pl = (ctypes.c_int * cap)()
+        ms = (ctypes.c_double * (3 * cap))()
+        n = self._lib.vkzg_b200_tuning_table(self._h, sc, pl, ms, cap)
+        return {int(sc[i]): (int(pl[i]), tuple(ms[3 * i:3 * i + 3])) for i in range(min(n, cap))}
 
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)

@@ -25,16 +25,19 @@
 
 namespace vkzg {
 
-constexpr int kBAThreads = 256;
+#ifndef VKZG_BA_THREADS
+#define VKZG_BA_THREADS 256
+#endif
+constexpr int kBAThreads = VKZG_BA_THREADS; // threads of the batch-affine phase kernels
 constexpr int kBABuckets = 128; // buckets per MSM output
 
-template <int NB>
+template <int NB, int NT = kBAThreads>
 struct BucketSumShared {
     uint32_t cnt[NB];
     uint32_t pscan[NB + 1];   // exclusive scan of pairs per bucket
     uint32_t base[2][NB + 1]; // element offsets of the current / next list
-    uint32_t part[2][kBAThreads];
-    Fp tree[2 * kBAThreads];
+    uint32_t part[2][NT];
+    Fp tree[2 * NT];
 };
 
 // kind: 0 general, 1 doubling, 2 result = a, 3 result = b, 4 result = infinity
@@ -76,9 +79,9 @@ __device__ __forceinline__ G1A pair_result(const G1A &a, const G1A &b, int kind,
 
 // Exclusive scans of pair counts and of next-round element counts over the NB
 // buckets: each thread sums a contiguous run, one thread scans the partials.
-template <int NB>
-__device__ void ba_plan_round(BucketSumShared<NB> &sh, int next) {
-    constexpr int per = (NB + kBAThreads - 1) / kBAThreads;
+template <int NB, int NT>
+__device__ void ba_plan_round(BucketSumShared<NB, NT> &sh, int next) {
+    constexpr int per = (NB + NT - 1) / NT;
     const int t = threadIdx.x, lo = t * per;
     uint32_t p = 0, e = 0;
     for (int k = lo; k < lo + per && k < NB; k++) {
@@ -90,7 +93,7 @@ __device__ void ba_plan_round(BucketSumShared<NB> &sh, int next) {
     __syncthreads();
     if (t == 0) {
         uint32_t ap = 0, ae = 0;
-        for (int q = 0; q < kBAThreads; q++) {
+        for (int q = 0; q < NT; q++) {
             const uint32_t xp = sh.part[0][q], xe = sh.part[1][q];
             sh.part[0][q] = ap;
             sh.part[1][q] = ae;
@@ -126,22 +129,22 @@ __device__ __forceinline__ int ba_bucket_of(const uint32_t *pscan, uint32_t q) {
 
 // One round: pairs of the current list (loaded by `src(k, i)`) into `dst`.
 // MAXP bounds the pairs per thread (P <= MAXP * kBAThreads).
-template <int NB, int MAXP, typename Src>
-__device__ void ba_round(BucketSumShared<NB> &sh, int next, const Src &src, G1A *dst) {
+template <int NB, int NT, int MAXP, typename Src>
+__device__ void ba_round(BucketSumShared<NB, NT> &sh, int next, const Src &src, G1A *dst) {
     const uint32_t P = sh.pscan[NB];
     Fp pre[MAXP];
     Fp acc = fp_one();
     int s = 0;
-    for (uint32_t q = threadIdx.x; q < P; q += kBAThreads, s++) {
+    for (uint32_t q = threadIdx.x; q < P; q += NT, s++) {
         const int k = ba_bucket_of<NB>(sh.pscan, q);
         const uint32_t i = q - sh.pscan[k];
         const G1A a = src(k, 2 * i), b = src(k, 2 * i + 1);
         pre[s] = acc;
         acc = fp_mul(acc, pair_denominator(a, b, pair_kind(a, b)));
     }
-    Fp inv = block_batch_inverse_fp<kBAThreads>(acc, sh.tree);
+    Fp inv = block_batch_inverse_fp<NT>(acc, sh.tree);
     for (int t = s - 1; t >= 0; t--) {
-        const uint32_t q = threadIdx.x + (uint32_t)t * kBAThreads;
+        const uint32_t q = threadIdx.x + (uint32_t)t * NT;
         const int k = ba_bucket_of<NB>(sh.pscan, q);
         const uint32_t i = q - sh.pscan[k];
         const G1A a = src(k, 2 * i), b = src(k, 2 * i + 1);
@@ -152,24 +155,24 @@ __device__ void ba_round(BucketSumShared<NB> &sh, int next, const Src &src, G1A 
         st_vec(&dst[sh.base[next][k] + i], pair_result(a, b, kind, inv_den));
     }
     // odd leftovers move to the end of their bucket's next list
-    for (int k = threadIdx.x; k < NB; k += kBAThreads) {
+    for (int k = threadIdx.x; k < NB; k += NT) {
         const uint32_t c = sh.cnt[k];
         if (c & 1u) st_vec(&dst[sh.base[next][k] + (c >> 1)], src(k, c - 1));
     }
 }
 
-template <int NB>
-__device__ __forceinline__ void ba_halve_counts(BucketSumShared<NB> &sh) {
+template <int NB, int NT>
+__device__ __forceinline__ void ba_halve_counts(BucketSumShared<NB, NT> &sh) {
     __syncthreads();
-    for (int k = threadIdx.x; k < NB; k += kBAThreads) sh.cnt[k] = (sh.cnt[k] + 1) >> 1;
+    for (int k = threadIdx.x; k < NB; k += NT) sh.cnt[k] = (sh.cnt[k] + 1) >> 1;
     __syncthreads();
 }
 
-template <int NB>
-__device__ bool ba_any_pair(const BucketSumShared<NB> &sh) {
+template <int NB, int NT>
+__device__ bool ba_any_pair(const BucketSumShared<NB, NT> &sh) {
     return __syncthreads_or(([&] {
         bool m = false;
-        for (int k = threadIdx.x; k < NB; k += kBAThreads) m |= sh.cnt[k] > 1;
+        for (int k = threadIdx.x; k < NB; k += NT) m |= sh.cnt[k] > 1;
         return m;
     })());
 }
@@ -178,11 +181,12 @@ __device__ bool ba_any_pair(const BucketSumShared<NB> &sh) {
 // round-1 pairs per thread.  buf0 holds the round-1 output (<= (n + NB) / 2
 // points), buf1 the round-2 output.  Returns the buffer holding the sums; their
 // offsets are in sh.base[result_slot].
-template <int NB, int MAXP0, typename Src0>
-__device__ G1A *ba_bucket_sums(BucketSumShared<NB> &sh, const Src0 &src0, G1A *buf0, G1A *buf1, int &result_slot) {
+template <int NB, int MAXP0, int NT, typename Src0>
+__device__ G1A *ba_bucket_sums(BucketSumShared<NB, NT> &sh, const Src0 &src0, G1A *buf0, G1A *buf1,
+                               int &result_slot) {
     // round 1 always runs, so singletons are materialised in buf0 too
     ba_plan_round(sh, 0);
-    ba_round<NB, MAXP0>(sh, 0, src0, buf0);
+    ba_round<NB, NT, MAXP0>(sh, 0, src0, buf0);
     ba_halve_counts(sh);
     G1A *cur = buf0, *other = buf1;
     int slot = 0;
@@ -192,7 +196,7 @@ __device__ G1A *ba_bucket_sums(BucketSumShared<NB> &sh, const Src0 &src0, G1A *b
         const G1A *from = cur;
         const uint32_t *fb = sh.base[slot];
         auto src = [from, fb](int k, uint32_t i) { return ld_vec(&from[fb[k] + i]); };
-        ba_round<NB, MAXP0>(sh, slot ^ 1, src, other);
+        ba_round<NB, NT, MAXP0>(sh, slot ^ 1, src, other);
         ba_halve_counts(sh);
         slot ^= 1;
         G1A *t = cur;

@@ -49,15 +49,19 @@ struct ProofWork {
     G1A *ladder_aff = nullptr;  // [cap][128][32]
     uint8_t *proofs = nullptr;  // [cap][128][48]
     uint32_t *err = nullptr;    // [cap]
-    // batch-affine accumulation (accum_mode 1)
+    // batch-affine accumulation (plans 1, 2)
     G1A *bucket_aff = nullptr;  // [cap][128][128] affine bucket sums
     G1A *ba_scratch = nullptr;  // [ba_blocks][kBAScratchPoints]
     int ba_blocks = 0;          // persistent grid size of the batch-affine kernels
-    int accum_mode = 1;         // 0: serial Jacobian buckets, 1: batch-affine rounds
+    int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
+    G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
 };
 // MSM outputs per batch-affine block, and its scratch: round-1 and round-2 outputs
 // of 2048 points in 128 buckets per output
-constexpr int kBAOutputs = 8;
+#ifndef VKZG_BA_OUTPUTS
+#define VKZG_BA_OUTPUTS 8
+#endif
+constexpr int kBAOutputs = VKZG_BA_OUTPUTS;
 constexpr int kBAScratchPoints = kBAOutputs * (1088 + 608);
 
 struct RecoverWork {

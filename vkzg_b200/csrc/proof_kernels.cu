@@ -20,6 +20,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <vector>
 
 namespace vkzg {
 
@@ -309,6 +310,7 @@ __global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, ui
 // affine bucket sums bucket_aff[blob][output][k], infinity for empty buckets.
 constexpr int kBANB = kBAOutputs * kBuckets;
 constexpr int kBAMaxPairs = kBAOutputs * kCellElems * kDigits / 2 / kBAThreads;
+constexpr int kBAMinBlocks = 65536 / (kBAThreads * 128); // at most 128 registers per thread
 constexpr size_t kPhaseADynSmem = (2 * kBANB + 4) * sizeof(uint32_t) + kBAOutputs * kCellElems * kDigits * 2;
 
 // Block-wide exclusive scan of cnt[0..NB) into start[0..NB] (partials per thread).
@@ -338,7 +340,7 @@ __device__ void block_exclusive_scan(const uint32_t *cnt, uint32_t *start, uint3
     __syncthreads();
 }
 
-__device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB> &sh, const G1A *res, int slot,
+__device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB, kBAThreads> &sh, const G1A *res, int slot,
                                                   G1A *out /* [kBANB] */) {
     for (int k = threadIdx.x; k < kBANB; k += kBAThreads) {
         G1A v;
@@ -352,10 +354,10 @@ __device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB> &
     }
 }
 
-__global__ void __launch_bounds__(kBAThreads, 2) k_phase_a_affine(const Fr *__restrict__ scalars,
+__global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_a_affine(const Fr *__restrict__ scalars,
                                                                  const G1A *__restrict__ pos, G1A *bucket_aff,
                                                                  G1A *scratch, int n_work) {
-    __shared__ BucketSumShared<kBANB> sh;
+    __shared__ BucketSumShared<kBANB, kBAThreads> sh;
     // dynamic: start[kBANB + 1], cursor[kBANB], items[kBAOutputs * 2048] (kPhaseADynSmem bytes)
     extern __shared__ uint4 dyn_smem[];
     uint32_t *start = reinterpret_cast<uint32_t *>(dyn_smem);
@@ -364,6 +366,7 @@ __global__ void __launch_bounds__(kBAThreads, 2) k_phase_a_affine(const Fr *__re
     G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
     const int tid = threadIdx.x;
     constexpr int kScalarsPerThread = kBAOutputs * kCellElems / kBAThreads;
+    static_assert(kScalarsPerThread * kBAThreads == kBAOutputs * kCellElems, "whole scalars per thread");
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const int o0 = w * kBAOutputs; // first output (blob * 128 + j0)
         for (int k = tid; k < kBANB; k += kBAThreads) sh.cnt[k] = 0;
@@ -403,19 +406,19 @@ __global__ void __launch_bounds__(kBAThreads, 2) k_phase_a_affine(const Fr *__re
             return pt;
         };
         int slot = 0;
-        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs>(sh, src0, buf0, buf1, slot);
+        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs, kBAThreads>(sh, src0, buf0, buf1, slot);
         store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
         __syncthreads();
     }
 }
 
-__global__ void __launch_bounds__(kBAThreads, 2) k_phase_b_affine(const G1A *__restrict__ ladder_aff,
+__global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(const G1A *__restrict__ ladder_aff,
                                                                  const uint32_t *__restrict__ items_p,
                                                                  const uint32_t *__restrict__ off_p,
                                                                  const uint32_t *__restrict__ items_m,
                                                                  const uint32_t *__restrict__ off_m, G1A *bucket_aff,
                                                                  G1A *scratch, int n_work) {
-    __shared__ BucketSumShared<kBANB> sh;
+    __shared__ BucketSumShared<kBANB, kBAThreads> sh;
     G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const int o0 = w * kBAOutputs, b = o0 / kCells, a0 = o0 % kCells;
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kBAThreads, 2) k_phase_b_affine(const G1A *__r
             return pt;
         };
         int slot = 0;
-        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs>(sh, src0, buf0, buf1, slot);
+        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs, kBAThreads>(sh, src0, buf0, buf1, slot);
         store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
         __syncthreads();
     }
@@ -472,6 +475,136 @@ __global__ void __launch_bounds__(kReduceThreads) k_reduce_affine(const G1A *__r
     st_vec(&out[o], g1_add(w, acc));
 }
 
+// ------------------------------------------- batch-affine bucket reduction
+// sum_{k=1..128} k B_k = S + sum_{b=0..6} 2^b T_b with A_i = B_{i+1},
+// S = sum_i A_i and T_b = sum of A_i over the i with bit b set.  All eight
+// sums come out of one halving hierarchy, C^(j+1)_m = C^(j)_2m + C^(j)_2m+1
+// (C^(0) = A, C^(7)_0 = S), because T_j = sum of the odd-indexed C^(j)_m:
+// 127 additions for the hierarchy plus 120 to add up the odd lists, 247 in all,
+// against 256 serial Jacobian additions for the running sum
+// (field.glsl.inc:485-489).  Every addition is affine and the schedule is the
+// same for every output, so rounds of it run as batch-affine rounds across
+// kRedOutputs outputs; a 13-operation Horner step in Jacobian coordinates
+// (6 doublings, 7 mixed additions) finishes each output.
+constexpr int kRedOps = 247;
+constexpr int kRedSlots = kBuckets + kRedOps;   // slots < 128 are the bucket sums themselves
+constexpr int kRedMaxRounds = 8;
+constexpr int kRedOutputs = 128;                 // outputs per block (one blob)
+constexpr int kRedThreads = 256;
+constexpr int kRedMaxPairs = 96 * kRedOutputs / kRedThreads; // round 1 has the most operations (96)
+
+struct ReduceSchedule {
+    uint16_t dst[kRedOps], a[kRedOps], b[kRedOps];
+    uint16_t round_start[kRedMaxRounds + 1];
+    uint16_t t_slot[7];
+    uint16_t all_slot;
+    int n_rounds;
+};
+__constant__ ReduceSchedule c_red;
+
+static bool build_reduce_schedule(ReduceSchedule &s) {
+    struct Op { int dst, a, b, round; };
+    std::vector<Op> ops;
+    std::vector<int> ready(kRedSlots, 0);
+    int next = kBuckets;
+    auto add = [&](int a, int b) {
+        const int d = next++;
+        const int r = std::max(ready[a], ready[b]) + 1;
+        ready[d] = r;
+        ops.push_back({d, a, b, r});
+        return d;
+    };
+    std::vector<int> cur(kBuckets);
+    for (int i = 0; i < kBuckets; i++) cur[i] = i;
+    for (int j = 0; j < 7; j++) {
+        std::vector<int> odd;
+        for (size_t m = 1; m < cur.size(); m += 2) odd.push_back(cur[m]);
+        std::vector<int> nxt;
+        for (size_t m = 0; m + 1 < cur.size(); m += 2) nxt.push_back(add(cur[m], cur[m + 1]));
+        while (odd.size() > 1) {
+            std::vector<int> nl;
+            for (size_t q = 0; q + 1 < odd.size(); q += 2) nl.push_back(add(odd[q], odd[q + 1]));
+            if (odd.size() & 1) nl.push_back(odd.back());
+            odd.swap(nl);
+        }
+        s.t_slot[j] = (uint16_t)odd[0];
+        cur.swap(nxt);
+    }
+    s.all_slot = (uint16_t)cur[0];
+    if ((int)ops.size() != kRedOps) return false;
+    std::stable_sort(ops.begin(), ops.end(), [](const Op &x, const Op &y) { return x.round < y.round; });
+    int nr = 0;
+    for (int q = 0; q < kRedOps; q++) {
+        s.dst[q] = (uint16_t)ops[q].dst;
+        s.a[q] = (uint16_t)ops[q].a;
+        s.b[q] = (uint16_t)ops[q].b;
+        nr = std::max(nr, ops[q].round);
+    }
+    if (nr > kRedMaxRounds) return false;
+    s.n_rounds = nr;
+    int q = 0;
+    for (int r = 1; r <= nr; r++) {
+        s.round_start[r - 1] = (uint16_t)q;
+        while (q < kRedOps && ops[q].round == r) q++;
+    }
+    s.round_start[nr] = (uint16_t)q;
+    for (int r = 0; r < nr; r++)
+        if ((s.round_start[r + 1] - s.round_start[r]) * kRedOutputs > kRedMaxPairs * kRedThreads) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(kRedThreads, 2) k_reduce_hier(const G1A *__restrict__ bucket_aff, G1J *out,
+                                                              G1A *scratch, int n_outputs) {
+    __shared__ Fp tree[2 * kRedThreads];
+    const int o0 = blockIdx.x * kRedOutputs;
+    const int go = min(kRedOutputs, n_outputs - o0);
+    G1A *slots = scratch + (size_t)blockIdx.x * kRedOutputs * kRedOps;
+    auto slot = [&](int g, int s) -> G1A * {
+        return s < kBuckets ? const_cast<G1A *>(&bucket_aff[((size_t)o0 + g) * kBuckets + s])
+                            : &slots[(size_t)g * kRedOps + (s - kBuckets)];
+    };
+    for (int r = 0; r < c_red.n_rounds; r++) {
+        const int q0 = c_red.round_start[r], nops = c_red.round_start[r + 1] - q0;
+        const int items = nops * go;
+        Fp pre[kRedMaxPairs];
+        Fp acc = fp_one();
+        int s = 0;
+        for (int it = threadIdx.x; it < items; it += kRedThreads, s++) {
+            const int g = it / nops, op = q0 + it % nops;
+            const G1A a = ld_vec(slot(g, c_red.a[op])), b = ld_vec(slot(g, c_red.b[op]));
+            pre[s] = acc;
+            acc = fp_mul(acc, pair_denominator(a, b, pair_kind(a, b)));
+        }
+        Fp inv = block_batch_inverse_fp<kRedThreads>(acc, tree);
+        for (int t = s - 1; t >= 0; t--) {
+            const int it = threadIdx.x + t * kRedThreads;
+            const int g = it / nops, op = q0 + it % nops;
+            const G1A a = ld_vec(slot(g, c_red.a[op])), b = ld_vec(slot(g, c_red.b[op]));
+            const int kind = pair_kind(a, b);
+            const Fp den = pair_denominator(a, b, kind);
+            const Fp inv_den = fp_mul(inv, pre[t]);
+            inv = fp_mul(inv, den);
+            st_vec(slot(g, c_red.dst[op]), pair_result(a, b, kind, inv_den));
+        }
+        __syncthreads();
+    }
+    // Horner: H = sum_b 2^b T_b, then + S
+    for (int g = threadIdx.x; g < go; g += kRedThreads) {
+        G1J h = g1_from_affine(ld_vec(slot(g, c_red.t_slot[6])));
+        for (int j = 5; j >= 0; j--) {
+            h = g1_dbl(h);
+            h = g1_madd(h, ld_vec(slot(g, c_red.t_slot[j])));
+        }
+        st_vec(&out[o0 + g], g1_madd(h, ld_vec(slot(g, c_red.all_slot))));
+    }
+}
+
+cudaError_t configure_reduce_schedule() {
+    ReduceSchedule s;
+    if (!build_reduce_schedule(s)) return cudaErrorInvalidValue;
+    return cudaMemcpyToSymbol(c_red, &s, sizeof(s));
+}
+
 // ---------------------------------------------------------------- launcher
 // ev (nullable): kProofStages + 1 events recorded around the stages.
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev) {
@@ -489,19 +622,27 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
     mark();
-    const bool affine = w.accum_mode == 1 && w.ba_blocks > 0;
+    // plan: 0 serial Jacobian buckets + serial reduction; 1 batch-affine buckets +
+    // binary-split reduction; 2 batch-affine buckets + serial reduction
+    const bool affine = w.plan != 0 && w.ba_blocks > 0;
+    const bool hier = w.plan == 1;
     const int ba_work = n_out / kBAOutputs;
     const int ba_grid = std::min(w.ba_blocks, ba_work);
+    auto reduce = [&]() {
+        if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+        else if (hier)
+            k_reduce_hier<<<(n_out + kRedOutputs - 1) / kRedOutputs, kRedThreads, 0, s>>>(w.bucket_aff, w.points,
+                                                                                       w.red_scratch, n_out);
+        else k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
+    };
     if (affine) {
         k_phase_a_affine<<<ba_grid, kBAThreads, kPhaseADynSmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
                                                                       ba_work);
-        mark();
-        k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     } else {
         k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
-        mark();
-        k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
     }
+    mark();
+    reduce();
     mark();
     k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
     mark();
@@ -513,15 +654,13 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         k_phase_b_affine<<<ba_grid, kBAThreads, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                         t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
                                                         w.ba_scratch, ba_work);
-        mark();
-        k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     } else {
         k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                        t.tap_perm[0], t.tap_items[1], t.tap_offsets[1],
                                                        t.tap_perm[1], w.buckets);
-        mark();
-        k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
     }
+    mark();
+    reduce();
     mark();
     k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
     mark();
@@ -540,8 +679,12 @@ int batch_affine_blocks_per_sm() {
     return std::max(1, std::min(a, b));
 }
 
+size_t reduce_scratch_points(int cap_blobs) { return (size_t)cap_blobs * kCells * kRedOps; }
+
 cudaError_t configure_proof_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = configure_reduce_schedule();
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kBlobElems * sizeof(Fr)));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseADynSmem);

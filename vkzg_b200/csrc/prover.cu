@@ -17,6 +17,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -27,6 +29,7 @@ namespace vkzg {
 cudaError_t configure_proof_kernels();
 cudaError_t configure_recover_kernels();
 int batch_affine_blocks_per_sm();
+size_t reduce_scratch_points(int cap_blobs);
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s,
                                 cudaEvent_t *ev);
 cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
@@ -62,6 +65,12 @@ struct vkzg_prover {
     mutable double last_proof_ms[kProofStages] = {};
     mutable double last_recover_ms[kRecoverStages] = {};
     mutable bool pending_proof = false, pending_recover = false;
+    // autotuner: plan per power-of-two chunk size (see choose_plan)
+    int plan_forced = -1;
+    std::map<uint32_t, int> plan_of;
+    std::map<uint32_t, std::array<double, 3>> plan_ms;
+    std::string tune_cache;
+    cudaEvent_t ev_tune[2] = {nullptr, nullptr};
 
     ~vkzg_prover() {
         if (stream) cudaStreamSynchronize(stream);
@@ -72,6 +81,8 @@ struct vkzg_prover {
         for (auto &e : ev_rec)
             if (e) cudaEventDestroy(e);
         if (ev_in) cudaEventDestroy(ev_in);
+        for (auto &e : ev_tune)
+            if (e) cudaEventDestroy(e);
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -322,6 +333,8 @@ void computed_small_tables(HostTables &h) {
     h.inv_blob = fr_inv(fr_from_u32(kBlobElems));
 }
 
+void load_tune_cache(vkzg_prover *p);
+
 vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     p->cap = cap;
     ProofWork &w = p->pw;
@@ -338,11 +351,17 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     if (!ok) return VKZG_ERR_MALLOC;
     if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
     // batch-affine bucket accumulation: one scratch slot per resident block
-    const char *mode = getenv("VKZG_ACCUM");
-    w.accum_mode = (mode && strcmp(mode, "jacobian") == 0) ? 0 : 1;
+    // plan override (0 serial Jacobian, 1 batch-affine + binary split, 2 batch-affine + serial)
+    if (const char *plan = getenv("VKZG_PLAN")) {
+        const int v = atoi(plan);
+        if (v >= 0 && v < 3) p->plan_forced = v;
+    }
+    if (const char *cache = getenv("VKZG_TUNE_CACHE")) p->tune_cache = cache;
+    load_tune_cache(p);
     w.ba_blocks = (int)p->sm_count * batch_affine_blocks_per_sm();
     if (!p->alloc(w.bucket_aff, B * kCells * kBuckets) ||
-        !p->alloc(w.ba_scratch, (size_t)w.ba_blocks * kBAScratchPoints))
+        !p->alloc(w.ba_scratch, (size_t)w.ba_blocks * kBAScratchPoints) ||
+        !p->alloc(w.red_scratch, reduce_scratch_points((int)B)))
         return VKZG_ERR_MALLOC;
     return VKZG_OK;
 }
@@ -380,7 +399,8 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
             return VKZG_ERR_GPU;
         }
     if (cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&p->ev_tune[0]) != cudaSuccess || cudaEventCreate(&p->ev_tune[1]) != cudaSuccess) {
         delete p;
         return VKZG_ERR_GPU;
     }
@@ -444,10 +464,93 @@ void collect_times(const cudaEvent_t *ev, int stages, double *dst) {
     }
 }
 
+// ---------------------------------------------------------------- autotuner
+// Three plans compute identical bytes (section "plan" in launch_proofs_timed):
+// serial Jacobian buckets win for a handful of blobs (more, smaller blocks),
+// batch-affine rounds win once a chunk fills the GPU, and which reduction is
+// faster depends on the chunk size.  The first chunk of each power-of-two size
+// class is timed under every plan on the stream and the fastest is kept.
+
+constexpr int kPlans = 3;
+
+uint32_t size_class(uint32_t n) {
+    uint32_t c = 1;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+void save_tune_cache(const vkzg_prover *p) {
+    if (p->tune_cache.empty()) return;
+    FILE *f = fopen(p->tune_cache.c_str(), "w");
+    if (!f) return;
+    for (const auto &kv : p->plan_of) fprintf(f, "%s|%u|%u %d\n", p->name.c_str(), p->sm_count, kv.first, kv.second);
+    fclose(f);
+}
+
+void load_tune_cache(vkzg_prover *p) {
+    if (p->tune_cache.empty()) return;
+    FILE *f = fopen(p->tune_cache.c_str(), "r");
+    if (!f) return;
+    char line[512];
+    const std::string key = p->name + "|" + std::to_string(p->sm_count) + "|";
+    while (fgets(line, sizeof line, f)) {
+        std::string l(line);
+        if (l.compare(0, key.size(), key) != 0) continue;
+        unsigned c = 0;
+        int plan = -1;
+        if (sscanf(l.c_str() + key.size(), "%u %d", &c, &plan) == 2 && plan >= 0 && plan < kPlans) p->plan_of[c] = plan;
+    }
+    fclose(f);
+}
+
+// Runs every plan on w (already holding n blobs), keeps the fastest; the
+// outputs left in w are those of the last run (identical for all plans).
+vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
+    cudaStream_t s = p->stream;
+    std::array<double, 3> ms{};
+    for (int plan = 0; plan < kPlans; plan++) {
+        w.plan = plan;
+        double best = 1e30;
+        for (int rep = 0; rep < 2; rep++) { // the first run of a plan also pays its first-launch costs
+            CK(cudaEventRecord(p->ev_tune[0], s));
+            CK(launch_proofs_timed(p->t, w, (int)n, s, nullptr));
+            CK(cudaEventRecord(p->ev_tune[1], s));
+            CK(cudaEventSynchronize(p->ev_tune[1]));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, p->ev_tune[0], p->ev_tune[1]));
+            best = std::min(best, (double)t);
+        }
+        ms[plan] = best;
+    }
+    const uint32_t c = size_class(n);
+    p->plan_ms[c] = ms;
+    p->plan_of[c] = (int)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+    save_tune_cache(p);
+    return VKZG_OK;
+}
+
+// Plan for a chunk of n blobs: forced, tuned, or (device-pointer calls that
+// cannot stop to measure) a size rule fitted to the B200 measurements.
+int planned(const vkzg_prover *p, uint32_t n) {
+    if (p->plan_forced >= 0) return p->plan_forced;
+    auto it = p->plan_of.find(size_class(n));
+    if (it != p->plan_of.end()) return it->second;
+    return n >= 128 ? 1 : (n >= 8 ? 2 : 0);
+}
+
+bool tuned(const vkzg_prover *p, uint32_t n) {
+    return p->plan_forced >= 0 || p->plan_of.count(size_class(n)) != 0;
+}
+
 vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+    if (!tuned(p, n)) {
+        const vkzg_result rc = tune_chunk(p, p->pw, n);
+        if (rc != VKZG_OK) return rc;
+    }
+    p->pw.plan = planned(p, n);
     CK(launch_proofs_timed(p->t, p->pw, (int)n, s, p->timing ? p->ev : nullptr));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -606,6 +709,7 @@ vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, c
         w.proofs = d_proofs + done * kCells * kProofBytes;
         w.err = d_err + done;
         CK(cudaMemsetAsync(w.err, 0, n * sizeof(uint32_t), p->stream));
+        w.plan = planned(p, n);
         CK(launch_proofs_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev : nullptr));
         done += n;
     }
@@ -681,6 +785,7 @@ vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const u
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
     CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->rw.scratch, p->pw.err, (int)n, s));
+    p->pw.plan = planned(p, n);
     if (proofs) CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -718,4 +823,88 @@ vkzg_result vkzg_b200_compute_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
                                                      const uint8_t *blobs, size_t num_blobs) {
     if (!proofs) return VKZG_ERR_BADARGS;
     return cells_batch(p, cells, proofs, blobs, num_blobs);
+}
+
+// ------------------------------------------------------------ autotuner API
+
+vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
+    if (!p) return VKZG_ERR_BADARGS;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    const uint32_t top = std::min<uint32_t>(max_blobs ? max_blobs : p->cap, p->cap);
+    // seeded canonical blobs (top byte below r's 0x73)
+    std::vector<uint8_t> blobs((size_t)top * kBlobBytes);
+    uint64_t x = 0x7594ull;
+    for (size_t i = 0; i < blobs.size(); i++) {
+        x ^= x << 13;
+        x ^= x >> 7;
+        x ^= x << 17;
+        blobs[i] = (uint8_t)(x >> 24);
+        if (i % 32 == 0) blobs[i] &= 0x3f;
+    }
+    CK(cudaMemcpyAsync(p->pw.blobs, blobs.data(), blobs.size(), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemsetAsync(p->pw.err, 0, top * sizeof(uint32_t), p->stream));
+    for (uint32_t n = 1; n <= top; n <<= 1) {
+        if (p->plan_forced >= 0) break;
+        const vkzg_result rc = tune_chunk(p, p->pw, n);
+        if (rc != VKZG_OK) return rc;
+        if (n < top && (n << 1) > top) n = top >> 1; // finish with the capacity itself
+    }
+    return VKZG_OK;
+}
+
+int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class_out, int *plan_out, double *ms_out, int cap) {
+    if (!p) return 0;
+    int i = 0;
+    for (const auto &kv : p->plan_of) {
+        if (i < cap) {
+            if (size_class_out) size_class_out[i] = kv.first;
+            if (plan_out) plan_out[i] = kv.second;
+            auto it = p->plan_ms.find(kv.first);
+            if (ms_out)
+                for (int q = 0; q < 3; q++) ms_out[3 * i + q] = it != p->plan_ms.end() ? it->second[q] : -1.0;
+        }
+        i++;
+    }
+    return i;
+}
+
+// --------------------------------------- recovered cells and their proofs
+
+// recover_cells_and_kzg_proofs: the extension is systematic, so the first 64
+// cells of the recovered wire-order array are the blob itself (element i of
+// that half sits at domain point w_8192^brev13(i) = w_4096^brev12(i)); proofs
+// are computed from them after a device-to-device copy.  Pinned by the
+// recovery vectors' proofs (output[1], which tests/vectors.h:8-10 skips).
+vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *cells_out, uint8_t *proofs_out,
+                                                     const uint8_t *cells, const uint8_t *cell_present,
+                                                     size_t num_blobs) {
+    if (!p || !cells_out || !proofs_out || !cells || !cell_present) return VKZG_ERR_BADARGS;
+    if (num_blobs == 0) return VKZG_OK;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+    const size_t ext_bytes = (size_t)kExtElems * 32;
+    for (size_t done = 0; done < num_blobs;) {
+        const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
+        const uint8_t *pr = cell_present + done * kCells;
+        for (uint32_t b = 0; b < n; b++) {
+            int miss = 0;
+            for (int i = 0; i < kCells; i++) miss += pr[(size_t)b * kCells + i] == 0;
+            if (miss > kCellElems) return VKZG_ERR_BADARGS;
+        }
+        cudaStream_t s = p->stream;
+        CK(cudaMemcpyAsync(p->rw.cells, cells + done * ext_bytes, (size_t)n * ext_bytes, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(p->rw.present, pr, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
+        CK(launch_recover_timed(p->t, p->rw, (int)n, s, nullptr));
+        CK(cudaMemcpy2DAsync(p->pw.blobs, kBlobBytes, p->rw.out, ext_bytes, kBlobBytes, n, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+        p->pw.plan = planned(p, n);
+        CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
+        CK(cudaMemcpyAsync(cells_out + done * ext_bytes, p->rw.out, (size_t)n * ext_bytes, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(proofs_out + done * kCells * kProofBytes, p->pw.proofs, (size_t)n * kCells * kProofBytes,
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        done += n;
+    }
+    return VKZG_OK;
 }
