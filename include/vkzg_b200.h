@@ -119,6 +119,45 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms3, int cap);
 
 /*
+ * Serving loop with continuous batching (the reference has none: one blocking
+ * batch call per caller, serialised per prover, src/vkzg.cpp:1183-1218).
+ *
+ * Requests of any blob count are submitted without blocking and identified by
+ * a ticket; their buffers must stay valid until vkzg_b200_server_wait returns
+ * for the ticket.  A dispatcher cuts pending requests into batches (one kind
+ * per batch, first come first served, at most max_blobs_per_batch blobs;
+ * larger requests are split) and hands each batch to a free lane: a prover with
+ * its own CUDA stream and buffers, so batches on different lanes run
+ * concurrently on the GPU and requests that arrive while lanes are busy join
+ * the next batch.  A batch is admitted only while the device working set of
+ * all batches in flight stays within hbm_budget_bytes.  Each blob is computed
+ * independently, so a request's output is the same alone and in any mix.
+ * vkzg_b200_server_wait returns the request's status (VKZG_ERR_INVALID_BLOB /
+ * VKZG_ERR_BADARGS as the batch calls would; VKZG_ERR_GPU on timeout, with the
+ * ticket still valid).  Stats cover requests completed since the last reset:
+ * latency from submit to completion.
+ */
+typedef struct vkzg_server vkzg_server;
+typedef struct {
+    uint32_t max_blobs_per_batch; /* 0 = 128 */
+    uint32_t lanes;               /* concurrent device batches; 0 = 3 */
+    uint64_t hbm_budget_bytes;    /* admission cap on the in-flight working set; 0 = 8 GiB */
+} vkzg_server_options;
+typedef struct {
+    uint64_t requests, blobs;
+    double p50_ms, p99_ms, p999_ms, mean_ms, max_ms, seconds;
+} vkzg_server_stats;
+void vkzg_b200_server_options_default(vkzg_server_options *opts);
+vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *opts);
+void vkzg_b200_server_free(vkzg_server *s);
+vkzg_result vkzg_b200_server_submit_proofs(vkzg_server *s, uint8_t *proofs, const uint8_t *blobs, size_t num_blobs,
+                                           uint64_t *ticket);
+vkzg_result vkzg_b200_server_submit_recovery(vkzg_server *s, uint8_t *cells_out, const uint8_t *cells,
+                                             const uint8_t *cell_present, size_t num_blobs, uint64_t *ticket);
+vkzg_result vkzg_b200_server_wait(vkzg_server *s, uint64_t ticket, int64_t timeout_ms);
+vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int reset);
+
+/*
  * Throughput probes on the current device, for roofline denominators (the
  * reference has none).  which = 0: 32-bit integer multiply-add issue rate in
  * tera-ops/s; 1: this library's Fp (381-bit) Montgomery multiplies in giga-ops/s;

@@ -21,14 +21,27 @@ def oracle():
     return Oracle()
 
 
+class Golden(dict):
+    """Every array of an .npz fixture, read once (an NpzFile decompresses on each
+    access and must not be shared between threads)."""
+
+    def __init__(self, path):
+        with np.load(path) as z:
+            super().__init__({k: z[k] for k in z.files})
+
+    @property
+    def files(self):
+        return list(self.keys())
+
+
 @pytest.fixture(scope="session")
 def golden_proofs():
-    return np.load(os.path.join(GOLDEN, "compute_cells_and_kzg_proofs.npz"))
+    return Golden(os.path.join(GOLDEN, "compute_cells_and_kzg_proofs.npz"))
 
 
 @pytest.fixture(scope="session")
 def golden_recover():
-    return np.load(os.path.join(GOLDEN, "recover_cells_and_kzg_proofs.npz"))
+    return Golden(os.path.join(GOLDEN, "recover_cells_and_kzg_proofs.npz"))
 
 
 @pytest.fixture(scope="session")

@@ -38,6 +38,9 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_recover_cells_device", "vkzg_b200_microbench", "vkzg_b200_recover_cells_device_noalloc",
     "vkzg_b200_bucket_sums_selftest", "vkzg_b200_compute_cells_batch", "vkzg_b200_compute_cells_and_proofs_batch",
     "vkzg_b200_autotune", "vkzg_b200_tuning_table", "vkzg_b200_recover_cells_and_proofs_batch",
+    "vkzg_b200_server_options_default", "vkzg_b200_server_new", "vkzg_b200_server_free",
+    "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
+    "vkzg_b200_server_stats",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -50,6 +53,20 @@ class VkzgException(RuntimeError):
 
 class _Options(ctypes.Structure):
     _fields_ = [("max_batch_size", ctypes.c_uint32)]
+
+
+class _ServerOptions(ctypes.Structure):
+    _fields_ = [("max_blobs_per_batch", ctypes.c_uint32), ("lanes", ctypes.c_uint32),
+                ("hbm_budget_bytes", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("blobs", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -111,6 +128,21 @@ def library():
             L.vkzg_b200_tuning_table.restype = ctypes.c_int
             L.vkzg_b200_recover_cells_and_proofs_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t]
             L.vkzg_b200_recover_cells_and_proofs_batch.restype = ctypes.c_int
+            L.vkzg_b200_server_options_default.argtypes = [ctypes.POINTER(_ServerOptions)]
+            L.vkzg_b200_server_options_default.restype = None
+            L.vkzg_b200_server_new.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_ServerOptions)]
+            L.vkzg_b200_server_new.restype = ctypes.c_int
+            L.vkzg_b200_server_free.argtypes = [vp]
+            L.vkzg_b200_server_free.restype = None
+            L.vkzg_b200_server_submit_proofs.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
+            L.vkzg_b200_server_submit_proofs.restype = ctypes.c_int
+            L.vkzg_b200_server_submit_recovery.argtypes = [vp, vp, vp, vp, ctypes.c_size_t,
+                                                           ctypes.POINTER(ctypes.c_uint64)]
+            L.vkzg_b200_server_submit_recovery.restype = ctypes.c_int
+            L.vkzg_b200_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int64]
+            L.vkzg_b200_server_wait.restype = ctypes.c_int
+            L.vkzg_b200_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats), ctypes.c_int]
+            L.vkzg_b200_server_stats.restype = ctypes.c_int
             _lib = L
     return _lib
 
@@ -277,6 +309,61 @@ class Prover:
         buf = (ctypes.c_double * 32)()
         n = self._lib.vkzg_b200_last_stage_times(self._h, 1 if recovery else 0, buf, 32)
         return {self._lib.vkzg_b200_stage_name(1 if recovery else 0, i).decode(): buf[i] for i in range(n)}
+
+
+class Server:
+    """Continuous-batching request loop (include/vkzg_b200.h).  Buffers passed to
+    submit_* must stay alive until wait() returns for their ticket; numpy arrays
+    or raw addresses are accepted."""
+
+    def __init__(self, max_blobs_per_batch=0, lanes=0, hbm_budget_bytes=0):
+        L = library()
+        o = _ServerOptions()
+        L.vkzg_b200_server_options_default(ctypes.byref(o))
+        o.max_blobs_per_batch, o.lanes, o.hbm_budget_bytes = max_blobs_per_batch, lanes, hbm_budget_bytes
+        h = ctypes.c_void_p()
+        _check(L.vkzg_b200_server_new(ctypes.byref(h), ctypes.byref(o)))
+        self._h, self._lib = h, L
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.vkzg_b200_server_free(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit_proofs(self, proofs_out, blobs, n):
+        t = ctypes.c_uint64()
+        _check(self._lib.vkzg_b200_server_submit_proofs(self._h, _ptr(proofs_out), _ptr(blobs), n, ctypes.byref(t)))
+        self._keep[t.value] = (proofs_out, blobs)
+        return t.value
+
+    def submit_recovery(self, cells_out, cells, present, n):
+        t = ctypes.c_uint64()
+        _check(self._lib.vkzg_b200_server_submit_recovery(self._h, _ptr(cells_out), _ptr(cells), _ptr(present), n,
+                                                          ctypes.byref(t)))
+        self._keep[t.value] = (cells_out, cells, present)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        """Returns the request's status code (0 = ok)."""
+        rc = self._lib.vkzg_b200_server_wait(self._h, ticket, int(timeout_ms))
+        self._keep.pop(ticket, None)
+        return rc
+
+    def stats(self, reset=False):
+        st = ServerStats()
+        _check(self._lib.vkzg_b200_server_stats(self._h, ctypes.byref(st), 1 if reset else 0))
+        return st.as_dict()
 
 
 def microbench(which):

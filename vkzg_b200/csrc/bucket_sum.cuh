@@ -2,20 +2,18 @@
 //
 // The reference accumulates each bucket serially in Jacobian coordinates
 // (k_phase_a.comp:37-42, k_phase_b_split.comp:43-55: madd-2007-bl, 11 Fp
-// multiplies per point).  Here the points of NB buckets (G MSM outputs x 128
-// buckets) are summed in pairwise rounds: round r adds element pairs
+// multiplies per point).  Here the points of the 128 buckets of one MSM output
+// are summed in pairwise rounds: round r adds element pairs
 // (2i, 2i+1) of every bucket, so a round is a batch of independent affine
 // additions
 //   lambda = (y2 - y1) / (x2 - x1),  x3 = lambda^2 - x1 - x2,  y3 = lambda (x1 - x3) - y1
-// whose denominators share one inversion (Montgomery's trick across the block:
-// per-thread prefix products, a block product tree, one divstep inversion).
-// That is 6 multiplies per addition plus the amortised inversion; the more
-// outputs a block carries, the more additions share each round's inversion
-// and product-tree latency.  Doubling (equal points), cancellation (P + -P)
-// and the point at infinity ((0,0)) are handled per pair, so any input is
-// summed exactly.
+// whose denominators share one inversion (Montgomery's trick across a warp:
+// per-lane prefix products, shuffle scans, one divstep inversion).  That is 6
+// multiplies per addition plus the amortised inversion.  Doubling (equal
+// points), cancellation (P + -P) and the point at infinity ((0,0)) are handled
+// per pair, so any input is summed exactly.
 //
-// Layout: the block owns two global scratch buffers.  Round 1 reads the source
+// Layout: each warp owns two global scratch buffers.  Round 1 reads the source
 // points through a loader, later rounds ping-pong between the buffers.  After
 // the last round, bucket k's sum is at buf[base[k]] when cnt[k] == 1 (cnt[k] == 0:
 // empty bucket, infinity).
@@ -30,15 +28,6 @@ namespace vkzg {
 #endif
 constexpr int kBAThreads = VKZG_BA_THREADS; // threads of the batch-affine phase kernels
 constexpr int kBABuckets = 128; // buckets per MSM output
-
-template <int NB, int NT = kBAThreads>
-struct BucketSumShared {
-    uint32_t cnt[NB];
-    uint32_t pscan[NB + 1];   // exclusive scan of pairs per bucket
-    uint32_t base[2][NB + 1]; // element offsets of the current / next list
-    uint32_t part[2][NT];
-    Fp tree[2 * NT];
-};
 
 // kind: 0 general, 1 doubling, 2 result = a, 3 result = b, 4 result = infinity
 __device__ __forceinline__ int pair_kind(const G1A &a, const G1A &b) {
@@ -77,44 +66,6 @@ __device__ __forceinline__ G1A pair_result(const G1A &a, const G1A &b, int kind,
     return r;
 }
 
-// Exclusive scans of pair counts and of next-round element counts over the NB
-// buckets: each thread sums a contiguous run, one thread scans the partials.
-template <int NB, int NT>
-__device__ void ba_plan_round(BucketSumShared<NB, NT> &sh, int next) {
-    constexpr int per = (NB + NT - 1) / NT;
-    const int t = threadIdx.x, lo = t * per;
-    uint32_t p = 0, e = 0;
-    for (int k = lo; k < lo + per && k < NB; k++) {
-        p += sh.cnt[k] >> 1;
-        e += (sh.cnt[k] + 1) >> 1;
-    }
-    sh.part[0][t] = p;
-    sh.part[1][t] = e;
-    __syncthreads();
-    if (t == 0) {
-        uint32_t ap = 0, ae = 0;
-        for (int q = 0; q < NT; q++) {
-            const uint32_t xp = sh.part[0][q], xe = sh.part[1][q];
-            sh.part[0][q] = ap;
-            sh.part[1][q] = ae;
-            ap += xp;
-            ae += xe;
-        }
-        sh.pscan[NB] = ap;
-        sh.base[next][NB] = ae;
-    }
-    __syncthreads();
-    p = sh.part[0][t];
-    e = sh.part[1][t];
-    for (int k = lo; k < lo + per && k < NB; k++) {
-        sh.pscan[k] = p;
-        sh.base[next][k] = e;
-        p += sh.cnt[k] >> 1;
-        e += (sh.cnt[k] + 1) >> 1;
-    }
-    __syncthreads();
-}
-
 // bucket containing pair q: largest k with pscan[k] <= q
 template <int NB>
 __device__ __forceinline__ int ba_bucket_of(const uint32_t *pscan, uint32_t q) {
@@ -127,77 +78,168 @@ __device__ __forceinline__ int ba_bucket_of(const uint32_t *pscan, uint32_t q) {
     return lo;
 }
 
-// One round: pairs of the current list (loaded by `src(k, i)`) into `dst`.
-// MAXP bounds the pairs per thread (P <= MAXP * kBAThreads).
-template <int NB, int NT, int MAXP, typename Src>
-__device__ void ba_round(BucketSumShared<NB, NT> &sh, int next, const Src &src, G1A *dst) {
-    const uint32_t P = sh.pscan[NB];
-    Fp pre[MAXP];
+// ------------------------------------------------------------ warp-level form
+// One warp sums a bucket space of NB buckets on its own (the 128 buckets of
+// NB / 128 MSM outputs side by side): pairwise rounds as above, and each
+// round's denominators share one inversion per warp (prefix and suffix products
+// by shuffles, one divstep inversion on one lane), so warps never wait on each
+// other.  The inversion runs on one lane but costs a whole warp's issue slots,
+// which is why several outputs share a bucket space: the more pairs a round
+// holds, the smaller that fixed share.  The per-pair prefix products go to the
+// warp's global scratch in word-major order (word w of element s of lane l at
+// [(s * 12 + w) * 32 + l]), which keeps every access a full 128-byte line.
+
+template <int NB>
+struct WarpBuckets {
+    uint32_t cnt[NB];
+    uint32_t pscan[NB + 1];
+    uint32_t base[2][NB + 1];
+};
+
+__device__ __forceinline__ Fp fp_shfl_up(const Fp &a, int d) {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) r.v[i] = __shfl_up_sync(0xffffffffu, a.v[i], d);
+    return r;
+}
+__device__ __forceinline__ Fp fp_shfl_down(const Fp &a, int d) {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) r.v[i] = __shfl_down_sync(0xffffffffu, a.v[i], d);
+    return r;
+}
+__device__ __forceinline__ Fp fp_shfl(const Fp &a, int src) {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) r.v[i] = __shfl_sync(0xffffffffu, a.v[i], src);
+    return r;
+}
+
+// 1 / a for one value per lane (none zero).
+__device__ inline Fp warp_batch_inverse_fp(const Fp &a) {
+    const int lane = threadIdx.x & 31;
+    Fp pre = a, suf = a;
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fp o = fp_shfl_up(pre, d);
+        if (lane >= d) pre = fp_mul(pre, o);
+        const Fp u = fp_shfl_down(suf, d);
+        if (lane + d < 32) suf = fp_mul(suf, u);
+    }
+    Fp tot = fp_shfl(pre, 31);
+    if (lane == 0) tot = fp_inv_fast(tot);
+    tot = fp_shfl(tot, 0);
+    Fp pre_x = fp_shfl_up(pre, 1), suf_x = fp_shfl_down(suf, 1);
+    if (lane == 0) pre_x = fp_one();
+    if (lane == 31) suf_x = fp_one();
+    return fp_mul(fp_mul(tot, pre_x), suf_x);
+}
+
+__device__ __forceinline__ void wb_store_pre(uint32_t *pre, int s, const Fp &v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int w = 0; w < 12; w++) pre[(s * 12 + w) * 32 + lane] = v.v[w];
+}
+__device__ __forceinline__ Fp wb_load_pre(const uint32_t *pre, int s) {
+    const int lane = threadIdx.x & 31;
+    Fp v;
+#pragma unroll
+    for (int w = 0; w < 12; w++) v.v[w] = pre[(s * 12 + w) * 32 + lane];
+    return v;
+}
+
+// pair and next-element scans over the NB buckets: NB / 32 buckets per lane
+template <int NB>
+__device__ inline void wb_plan_round(WarpBuckets<NB> &wb, int next) {
+    static_assert(NB % 32 == 0, "whole buckets per lane");
+    constexpr int per = NB / 32;
+    const int lane = threadIdx.x & 31;
+    uint32_t p = 0, e = 0;
+#pragma unroll
+    for (int k = lane * per; k < lane * per + per; k++) {
+        p += wb.cnt[k] >> 1;
+        e += (wb.cnt[k] + 1) >> 1;
+    }
+    uint32_t ip = p, ie = e;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t op = __shfl_up_sync(0xffffffffu, ip, d), oe = __shfl_up_sync(0xffffffffu, ie, d);
+        if (lane >= d) {
+            ip += op;
+            ie += oe;
+        }
+    }
+    p = ip - p;
+    e = ie - e;
+#pragma unroll
+    for (int k = lane * per; k < lane * per + per; k++) {
+        wb.pscan[k] = p;
+        wb.base[next][k] = e;
+        p += wb.cnt[k] >> 1;
+        e += (wb.cnt[k] + 1) >> 1;
+    }
+    if (lane == 31) {
+        wb.pscan[NB] = ip;
+        wb.base[next][NB] = ie;
+    }
+    __syncwarp();
+}
+
+template <int NB, typename Src>
+__device__ void wb_round(WarpBuckets<NB> &wb, int next, const Src &src, G1A *dst, uint32_t *pre) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t P = wb.pscan[NB];
     Fp acc = fp_one();
     int s = 0;
-    for (uint32_t q = threadIdx.x; q < P; q += NT, s++) {
-        const int k = ba_bucket_of<NB>(sh.pscan, q);
-        const uint32_t i = q - sh.pscan[k];
+    for (uint32_t q = lane; q < P; q += 32, s++) {
+        const int k = ba_bucket_of<NB>(wb.pscan, q);
+        const uint32_t i = q - wb.pscan[k];
         const G1A a = src(k, 2 * i), b = src(k, 2 * i + 1);
-        pre[s] = acc;
+        wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(a, b, pair_kind(a, b)));
     }
-    Fp inv = block_batch_inverse_fp<NT>(acc, sh.tree);
+    Fp inv = warp_batch_inverse_fp(acc);
     for (int t = s - 1; t >= 0; t--) {
-        const uint32_t q = threadIdx.x + (uint32_t)t * NT;
-        const int k = ba_bucket_of<NB>(sh.pscan, q);
-        const uint32_t i = q - sh.pscan[k];
+        const uint32_t q = lane + (uint32_t)t * 32;
+        const int k = ba_bucket_of<NB>(wb.pscan, q);
+        const uint32_t i = q - wb.pscan[k];
         const G1A a = src(k, 2 * i), b = src(k, 2 * i + 1);
         const int kind = pair_kind(a, b);
         const Fp den = pair_denominator(a, b, kind);
-        const Fp inv_den = fp_mul(inv, pre[t]);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
         inv = fp_mul(inv, den);
-        st_vec(&dst[sh.base[next][k] + i], pair_result(a, b, kind, inv_den));
+        st_vec(&dst[wb.base[next][k] + i], pair_result(a, b, kind, inv_den));
     }
-    // odd leftovers move to the end of their bucket's next list
-    for (int k = threadIdx.x; k < NB; k += NT) {
-        const uint32_t c = sh.cnt[k];
-        if (c & 1u) st_vec(&dst[sh.base[next][k] + (c >> 1)], src(k, c - 1));
+    for (int k = lane; k < NB; k += 32) {
+        const uint32_t c = wb.cnt[k];
+        if (c & 1u) st_vec(&dst[wb.base[next][k] + (c >> 1)], src(k, c - 1));
     }
+    __syncwarp();
+    for (int k = lane; k < NB; k += 32) wb.cnt[k] = (wb.cnt[k] + 1) >> 1;
+    __syncwarp();
 }
 
-template <int NB, int NT>
-__device__ __forceinline__ void ba_halve_counts(BucketSumShared<NB, NT> &sh) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < NB; k += NT) sh.cnt[k] = (sh.cnt[k] + 1) >> 1;
-    __syncthreads();
-}
-
-template <int NB, int NT>
-__device__ bool ba_any_pair(const BucketSumShared<NB, NT> &sh) {
-    return __syncthreads_or(([&] {
-        bool m = false;
-        for (int k = threadIdx.x; k < NB; k += NT) m |= sh.cnt[k] > 1;
-        return m;
-    })());
-}
-
-// Sums every bucket.  sh.cnt must hold the initial counts; MAXP0 bounds the
-// round-1 pairs per thread.  buf0 holds the round-1 output (<= (n + NB) / 2
-// points), buf1 the round-2 output.  Returns the buffer holding the sums; their
-// offsets are in sh.base[result_slot].
-template <int NB, int MAXP0, int NT, typename Src0>
-__device__ G1A *ba_bucket_sums(BucketSumShared<NB, NT> &sh, const Src0 &src0, G1A *buf0, G1A *buf1,
+// Sums the warp's NB buckets (wb.cnt = initial counts, at most 16 * NB points).
+// buf0 >= NB / 128 * 1088 points, buf1 >= NB / 128 * 608, pre >= NB * 3 * 32
+// words (NB / 4 pairs per lane).  Round 1 reads src0 only, so wb.base[1] may
+// hold src0's own offsets.  Returns the buffer of sums, offsets in
+// wb.base[result_slot].
+template <int NB, typename Src0>
+__device__ G1A *wb_bucket_sums(WarpBuckets<NB> &wb, const Src0 &src0, G1A *buf0, G1A *buf1, uint32_t *pre,
                                int &result_slot) {
-    // round 1 always runs, so singletons are materialised in buf0 too
-    ba_plan_round(sh, 0);
-    ba_round<NB, NT, MAXP0>(sh, 0, src0, buf0);
-    ba_halve_counts(sh);
+    wb_plan_round(wb, 0);
+    wb_round(wb, 0, src0, buf0, pre);
     G1A *cur = buf0, *other = buf1;
     int slot = 0;
     for (int round = 0; round < 16; round++) {
-        if (!ba_any_pair(sh)) break;
-        ba_plan_round(sh, slot ^ 1);
+        bool more = false;
+        for (int k = threadIdx.x & 31; k < NB; k += 32) more |= wb.cnt[k] > 1;
+        if (!__any_sync(0xffffffffu, more)) break;
+        wb_plan_round(wb, slot ^ 1);
         const G1A *from = cur;
-        const uint32_t *fb = sh.base[slot];
+        const uint32_t *fb = wb.base[slot];
         auto src = [from, fb](int k, uint32_t i) { return ld_vec(&from[fb[k] + i]); };
-        ba_round<NB, NT, MAXP0>(sh, slot ^ 1, src, other);
-        ba_halve_counts(sh);
+        wb_round(wb, slot ^ 1, src, other, pre);
         slot ^= 1;
         G1A *t = cur;
         cur = other;

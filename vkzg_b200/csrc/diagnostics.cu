@@ -56,23 +56,24 @@ __global__ void __launch_bounds__(256) k_probe_fr(uint32_t seed, int iters, uint
 // Sums caller-chosen points into 128 buckets with the batch-affine routine of
 // the proof kernels (one block), so tests can drive its special cases: repeated
 // points (doubling), P + -P, the point at infinity.
-__global__ void __launch_bounds__(256) k_bucket_sums_selftest(const G1A *points, const uint32_t *start,
-                                                                     G1A *sums, G1A *scratch) {
-    __shared__ BucketSumShared<kBABuckets, 256> sh;
-    if (threadIdx.x < kBABuckets) sh.cnt[threadIdx.x] = start[threadIdx.x + 1] - start[threadIdx.x];
-    __syncthreads();
+__global__ void __launch_bounds__(32) k_bucket_sums_selftest(const G1A *points, const uint32_t *start, G1A *sums,
+                                                            G1A *scratch) {
+    __shared__ WarpBuckets<kBABuckets> wb;
+    for (int k = threadIdx.x; k < kBABuckets; k += 32) wb.cnt[k] = start[k + 1] - start[k];
+    __syncwarp();
     auto src0 = [points, start](int k, uint32_t i) { return ld_vec(&points[start[k] + i]); };
     int slot = 0;
-    const G1A *res = ba_bucket_sums<kBABuckets, 4, 256>(sh, src0, scratch, scratch + 1088, slot);
-    if (threadIdx.x < kBABuckets) {
+    const G1A *res = wb_bucket_sums(wb, src0, scratch, scratch + 1088, reinterpret_cast<uint32_t *>(scratch + 1696),
+                                    slot);
+    for (int k = threadIdx.x; k < kBABuckets; k += 32) {
         G1A v;
-        if (sh.cnt[threadIdx.x]) {
-            v = ld_vec(&res[sh.base[slot][threadIdx.x]]);
+        if (wb.cnt[k]) {
+            v = ld_vec(&res[wb.base[slot][k]]);
         } else {
             v.x = fp_zero();
             v.y = fp_zero();
         }
-        st_vec(&sums[threadIdx.x], v);
+        st_vec(&sums[k], v);
     }
 }
 
@@ -114,7 +115,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
     vkzg_result rc = VKZG_OK;
     if (cudaMalloc(&d_pts, pts.size() * sizeof(G1A)) != cudaSuccess ||
         cudaMalloc(&d_sums, kBABuckets * sizeof(G1A)) != cudaSuccess ||
-        cudaMalloc(&d_scratch, (1088 + 608) * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&d_scratch, (1088 + 608 + 512) * sizeof(G1A)) != cudaSuccess ||
         cudaMalloc(&d_start, start.size() * 4) != cudaSuccess) {
         rc = VKZG_ERR_MALLOC;
     } else {
@@ -123,7 +124,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
             cudaMemcpy(d_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
             rc = VKZG_ERR_GPU;
         } else {
-            k_bucket_sums_selftest<<<1, 256>>>(d_pts, d_start, d_sums, d_scratch);
+            k_bucket_sums_selftest<<<1, 32>>>(d_pts, d_start, d_sums, d_scratch);
             if (cudaDeviceSynchronize() != cudaSuccess ||
                 cudaMemcpy(sums.data(), d_sums, kBABuckets * sizeof(G1A), cudaMemcpyDeviceToHost) != cudaSuccess)
                 rc = VKZG_ERR_GPU;

@@ -56,13 +56,21 @@ struct ProofWork {
     int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
     G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
 };
-// MSM outputs per batch-affine block, and its scratch: round-1 and round-2 outputs
-// of 2048 points in 128 buckets per output
-#ifndef VKZG_BA_OUTPUTS
-#define VKZG_BA_OUTPUTS 8
+// Batch-affine kernels: VKZG_BA_THREADS threads per block, one warp sums the
+// buckets of kWarpOutputs MSM outputs at a time.  Per-warp scratch: round-1 and
+// round-2 outputs (at most 1088 and 608 points per output of 2048 points in 128
+// buckets), prefix products (32 pairs x 12 words per lane per output = 512
+// points), and phase A's sorted bucket items (2048 x 2 bytes per output, 43
+// points).
+#ifndef VKZG_BA_THREADS
+#define VKZG_BA_THREADS 256
 #endif
-constexpr int kBAOutputs = VKZG_BA_OUTPUTS;
-constexpr int kBAScratchPoints = kBAOutputs * (1088 + 608);
+#ifndef VKZG_WARP_OUTPUTS
+#define VKZG_WARP_OUTPUTS 4
+#endif
+constexpr int kWarpOutputs = VKZG_WARP_OUTPUTS;
+constexpr int kBAWarpScratchPoints = kWarpOutputs * (1088 + 608 + 512 + 43);
+constexpr int kBAScratchPoints = (VKZG_BA_THREADS / 32) * kBAWarpScratchPoints; // per block
 
 struct RecoverWork {
     uint8_t *cells = nullptr;     // [cap][8192*32]

@@ -305,47 +305,40 @@ __global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, ui
 }
 
 // ------------------------------------------- batch-affine phase A / phase B
-// Persistent blocks: block x owns scratch slot x and walks work items of
-// kBAOutputs consecutive outputs of one blob with stride gridDim.x.  Output:
-// affine bucket sums bucket_aff[blob][output][k], infinity for empty buckets.
-constexpr int kBANB = kBAOutputs * kBuckets;
-constexpr int kBAMaxPairs = kBAOutputs * kCellElems * kDigits / 2 / kBAThreads;
+// Persistent blocks of kBAWarps independent warps.  A warp's task is
+// kWarpOutputs consecutive MSM outputs, whose 128 buckets each it sums as one
+// bucket space (wb_bucket_sums), tasks strided over all warps of the grid.
+// Output: affine bucket sums bucket_aff[output][k], infinity for empty buckets.
+constexpr int kBAWarps = kBAThreads / 32;
+constexpr int kWarpNB = kWarpOutputs * kBuckets;
 constexpr int kBAMinBlocks = 65536 / (kBAThreads * 128); // at most 128 registers per thread
-constexpr size_t kPhaseADynSmem = (2 * kBANB + 4) * sizeof(uint32_t) + kBAOutputs * kCellElems * kDigits * 2;
+constexpr size_t kBASmem = kBAWarps * sizeof(WarpBuckets<kWarpNB>);
+static_assert(kCells % kWarpOutputs == 0, "a task stays within one blob");
+static_assert(kBAThreads == VKZG_BA_THREADS, "scratch sized for this block");
 
-// Block-wide exclusive scan of cnt[0..NB) into start[0..NB] (partials per thread).
-template <int NB>
-__device__ void block_exclusive_scan(const uint32_t *cnt, uint32_t *start, uint32_t *part) {
-    constexpr int per = (NB + kBAThreads - 1) / kBAThreads;
-    const int t = threadIdx.x, lo = t * per;
-    uint32_t p = 0;
-    for (int k = lo; k < lo + per && k < NB; k++) p += cnt[k];
-    part[t] = p;
-    __syncthreads();
-    if (t == 0) {
-        uint32_t a = 0;
-        for (int q = 0; q < kBAThreads; q++) {
-            const uint32_t x = part[q];
-            part[q] = a;
-            a += x;
-        }
-        start[NB] = a;
-    }
-    __syncthreads();
-    p = part[t];
-    for (int k = lo; k < lo + per && k < NB; k++) {
-        start[k] = p;
-        p += cnt[k];
-    }
-    __syncthreads();
+struct WarpScratch {
+    G1A *buf0, *buf1;
+    uint32_t *pre;
+    uint16_t *items;
+};
+
+__device__ __forceinline__ WarpScratch warp_scratch(G1A *scratch) {
+    const size_t wid = (size_t)blockIdx.x * kBAWarps + (threadIdx.x >> 5);
+    WarpScratch ws;
+    ws.buf0 = scratch + wid * kBAWarpScratchPoints;
+    ws.buf1 = ws.buf0 + kWarpOutputs * 1088;
+    ws.pre = reinterpret_cast<uint32_t *>(ws.buf1 + kWarpOutputs * 608);
+    ws.items = reinterpret_cast<uint16_t *>(ws.buf1 + kWarpOutputs * (608 + 512));
+    return ws;
 }
 
-__device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB, kBAThreads> &sh, const G1A *res, int slot,
-                                                  G1A *out /* [kBANB] */) {
-    for (int k = threadIdx.x; k < kBANB; k += kBAThreads) {
+// bucket v of the task's space is bucket v % 128 of output o0 + v / 128, which
+// sits at out[v] with out = bucket_aff + o0 * 128
+__device__ __forceinline__ void store_warp_sums(const WarpBuckets<kWarpNB> &wb, const G1A *res, int slot, G1A *out) {
+    for (int k = threadIdx.x & 31; k < kWarpNB; k += 32) {
         G1A v;
-        if (sh.cnt[k]) {
-            v = ld_vec(&res[sh.base[slot][k]]);
+        if (wb.cnt[k]) {
+            v = ld_vec(&res[wb.base[slot][k]]);
         } else {
             v.x = fp_zero();
             v.y = fp_zero();
@@ -354,95 +347,130 @@ __device__ __forceinline__ void store_bucket_sums(const BucketSumShared<kBANB, k
     }
 }
 
+// Exclusive scan of cnt[0..NB) into a[0..NB] and b[0..NB) (two copies).
+template <int NB>
+__device__ __forceinline__ void warp_exclusive_scan(const uint32_t *cnt, uint32_t *a, uint32_t *b) {
+    constexpr int per = NB / 32;
+    const int lane = threadIdx.x & 31;
+    uint32_t p = 0;
+#pragma unroll
+    for (int k = lane * per; k < lane * per + per; k++) p += cnt[k];
+    uint32_t ip = p;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, ip, d);
+        if (lane >= d) ip += o;
+    }
+    p = ip - p;
+#pragma unroll
+    for (int k = lane * per; k < lane * per + per; k++) {
+        a[k] = p;
+        b[k] = p;
+        p += cnt[k];
+    }
+    if (lane == 31) a[NB] = ip;
+    __syncwarp();
+}
+
+// Phase A: output o = blob * 128 + j is sum_i sum_d digit_d(s_j[i]) * pos[j][i][d].
+// The warp sorts its outputs' (position, digit) items by bucket (counts by
+// shared atomics, a scan, a scatter into its scratch) and sums the buckets.
 __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_a_affine(const Fr *__restrict__ scalars,
-                                                                 const G1A *__restrict__ pos, G1A *bucket_aff,
-                                                                 G1A *scratch, int n_work) {
-    __shared__ BucketSumShared<kBANB, kBAThreads> sh;
-    // dynamic: start[kBANB + 1], cursor[kBANB], items[kBAOutputs * 2048] (kPhaseADynSmem bytes)
+                                                                          const G1A *__restrict__ pos,
+                                                                          G1A *bucket_aff, G1A *scratch, int n_out) {
     extern __shared__ uint4 dyn_smem[];
-    uint32_t *start = reinterpret_cast<uint32_t *>(dyn_smem);
-    uint32_t *cursor = start + kBANB + 4;
-    uint16_t *items = reinterpret_cast<uint16_t *>(cursor + kBANB);
-    G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
-    const int tid = threadIdx.x;
-    constexpr int kScalarsPerThread = kBAOutputs * kCellElems / kBAThreads;
-    static_assert(kScalarsPerThread * kBAThreads == kBAOutputs * kCellElems, "whole scalars per thread");
-    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
-        const int o0 = w * kBAOutputs; // first output (blob * 128 + j0)
-        for (int k = tid; k < kBANB; k += kBAThreads) sh.cnt[k] = 0;
-        __syncthreads();
-        Fr sc[kScalarsPerThread];
-        for (int r = 0; r < kScalarsPerThread; r++) {
-            const int q = tid + r * kBAThreads, g = q / kCellElems, i = q % kCellElems;
-            sc[r] = ld_vec(&scalars[((size_t)o0 + g) * kCellElems + i]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpBuckets<kWarpNB> &wb = reinterpret_cast<WarpBuckets<kWarpNB> *>(dyn_smem)[warp];
+    const WarpScratch ws = warp_scratch(scratch);
+    constexpr int kScalars = kWarpOutputs * kCellElems;
+    const int n_tasks = n_out / kWarpOutputs;
+    for (int task = blockIdx.x * kBAWarps + warp; task < n_tasks; task += gridDim.x * kBAWarps) {
+        const int o0 = task * kWarpOutputs;
+        const Fr *sc_base = scalars + (size_t)o0 * kCellElems;
+        for (int k = lane; k < kWarpNB; k += 32) wb.cnt[k] = 0;
+        __syncwarp();
+        for (int q = lane; q < kScalars; q += 32) {
+            const Fr sc = ld_vec(&sc_base[q]);
+            const int g = q / kCellElems;
             int carry = 0;
             for (int dd = 0; dd < kDigits; dd++) {
-                const int v = recode_digit(sc[r], dd, carry);
-                if (v) atomicAdd(&sh.cnt[g * kBuckets + abs(v) - 1], 1u);
+                const int v = recode_digit(sc, dd, carry);
+                if (v) atomicAdd(&wb.cnt[g * kBuckets + abs(v) - 1], 1u);
             }
         }
-        __syncthreads();
-        block_exclusive_scan<kBANB>(sh.cnt, start, sh.part[0]);
-        for (int k = tid; k < kBANB; k += kBAThreads) cursor[k] = start[k];
-        __syncthreads();
-        for (int r = 0; r < kScalarsPerThread; r++) {
-            const int q = tid + r * kBAThreads, g = q / kCellElems, i = q % kCellElems;
+        __syncwarp();
+        // item offsets in wb.base[1] (read by round 1 only), cursors in wb.pscan
+        warp_exclusive_scan<kWarpNB>(wb.cnt, wb.base[1], wb.pscan);
+        for (int q = lane; q < kScalars; q += 32) {
+            const Fr sc = ld_vec(&sc_base[q]);
+            const int g = q / kCellElems, i = q % kCellElems;
             int carry = 0;
             for (int dd = 0; dd < kDigits; dd++) {
-                const int v = recode_digit(sc[r], dd, carry);
+                const int v = recode_digit(sc, dd, carry);
                 if (v) {
-                    const uint32_t slot = atomicAdd(&cursor[g * kBuckets + abs(v) - 1], 1u);
-                    items[slot] = (uint16_t)((i << 6) | (dd << 1) | (v < 0 ? 1 : 0));
+                    const uint32_t slot = atomicAdd(&wb.pscan[g * kBuckets + abs(v) - 1], 1u);
+                    ws.items[slot] = (uint16_t)((i << 6) | (dd << 1) | (v < 0 ? 1 : 0));
                 }
             }
         }
-        __syncthreads();
-        const G1A *t0 = pos + (size_t)(o0 % kCells) * kCellElems * kDigits;
-        auto src0 = [t0, items, start](int k, uint32_t e) {
-            const uint32_t packed = items[start[k] + e];
-            const G1A *tj = t0 + (size_t)(k >> 7) * kCellElems * kDigits;
+        __syncwarp();
+        const uint32_t *st = wb.base[1];
+        const uint16_t *items = ws.items;
+        auto src0 = [=](int k, uint32_t e) {
+            const uint32_t packed = items[st[k] + e];
+            const G1A *tj = pos + (size_t)((o0 + (k >> 7)) % kCells) * kCellElems * kDigits;
             G1A pt = ldg_vec(&tj[(packed >> 6) * kDigits + ((packed >> 1) & 31u)]);
             if (packed & 1u) pt.y = fp_neg(pt.y);
             return pt;
         };
         int slot = 0;
-        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs, kBAThreads>(sh, src0, buf0, buf1, slot);
-        store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
-        __syncthreads();
+        const G1A *res = wb_bucket_sums(wb, src0, ws.buf0, ws.buf1, ws.pre, slot);
+        store_warp_sums(wb, res, slot, bucket_aff + (size_t)o0 * kBuckets);
+        __syncwarp();
     }
 }
 
+// Phase B: output (blob b, a) with a < 64 sums the plus-half taps, a >= 64 the
+// minus-half taps (negacyclic: tap e > a - 64 flips sign), over the blob's
+// normalised ladder points.
 __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(const G1A *__restrict__ ladder_aff,
-                                                                 const uint32_t *__restrict__ items_p,
-                                                                 const uint32_t *__restrict__ off_p,
-                                                                 const uint32_t *__restrict__ items_m,
-                                                                 const uint32_t *__restrict__ off_m, G1A *bucket_aff,
-                                                                 G1A *scratch, int n_work) {
-    __shared__ BucketSumShared<kBANB, kBAThreads> sh;
-    G1A *buf0 = scratch + (size_t)blockIdx.x * kBAScratchPoints, *buf1 = buf0 + kBAOutputs * 1088;
-    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
-        const int o0 = w * kBAOutputs, b = o0 / kCells, a0 = o0 % kCells;
-        const bool minus = a0 >= kHalf; // the kBAOutputs outputs share a half
-        const uint32_t *items = minus ? items_m : items_p;
-        const uint32_t *off = minus ? off_m : off_p;
-        for (int k = threadIdx.x; k < kBANB; k += kBAThreads) {
+                                                                          const uint32_t *__restrict__ items_p,
+                                                                          const uint32_t *__restrict__ off_p,
+                                                                          const uint32_t *__restrict__ items_m,
+                                                                          const uint32_t *__restrict__ off_m,
+                                                                          G1A *bucket_aff, G1A *scratch,
+                                                                          int n_out) {
+    extern __shared__ uint4 dyn_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpBuckets<kWarpNB> &wb = reinterpret_cast<WarpBuckets<kWarpNB> *>(dyn_smem)[warp];
+    const WarpScratch ws = warp_scratch(scratch);
+    const int n_tasks = n_out / kWarpOutputs;
+    for (int task = blockIdx.x * kBAWarps + warp; task < n_tasks; task += gridDim.x * kBAWarps) {
+        const int o0 = task * kWarpOutputs;
+        for (int k = lane; k < kWarpNB; k += 32) {
             const int kk = k & (kBuckets - 1);
-            sh.cnt[k] = __ldg(&off[kk + 1]) - __ldg(&off[kk]);
+            const uint32_t *off = (o0 + (k >> 7)) % kCells >= kHalf ? off_m : off_p;
+            wb.cnt[k] = __ldg(&off[kk + 1]) - __ldg(&off[kk]);
         }
-        __syncthreads();
-        const G1A *lad = ladder_aff + ((size_t)b * kCells + (minus ? kHalf : 0)) * kDigits;
+        __syncwarp();
         auto src0 = [=](int k, uint32_t e) {
-            const int aa = (a0 + (k >> 7)) & (kHalf - 1);
-            const uint32_t packed = __ldg(&items[__ldg(&off[k & (kBuckets - 1)]) + e]);
+            const int o = o0 + (k >> 7), kk = k & (kBuckets - 1);
+            const int b = o / kCells, a = o % kCells;
+            const bool minus = a >= kHalf;
+            const int aa = a & (kHalf - 1);
+            const uint32_t *items = minus ? items_m : items_p;
+            const uint32_t *off = minus ? off_m : off_p;
+            const uint32_t packed = __ldg(&items[__ldg(&off[kk]) + e]);
             const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
+            const G1A *lad = ladder_aff + ((size_t)b * kCells + (minus ? kHalf : 0)) * kDigits;
             G1A pt = ld_vec(&lad[((aa - tap) & (kHalf - 1)) * kDigits + d]);
             if (((packed >> 16) & 1u) != (minus && tap > aa)) pt.y = fp_neg(pt.y);
             return pt;
         };
         int slot = 0;
-        const G1A *res = ba_bucket_sums<kBANB, kBAMaxPairs, kBAThreads>(sh, src0, buf0, buf1, slot);
-        store_bucket_sums(sh, res, slot, bucket_aff + (size_t)o0 * kBuckets);
-        __syncthreads();
+        const G1A *res = wb_bucket_sums(wb, src0, ws.buf0, ws.buf1, ws.pre, slot);
+        store_warp_sums(wb, res, slot, bucket_aff + (size_t)o0 * kBuckets);
+        __syncwarp();
     }
 }
 
@@ -626,8 +654,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     // binary-split reduction; 2 batch-affine buckets + serial reduction
     const bool affine = w.plan != 0 && w.ba_blocks > 0;
     const bool hier = w.plan == 1;
-    const int ba_work = n_out / kBAOutputs;
-    const int ba_grid = std::min(w.ba_blocks, ba_work);
+    const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
     auto reduce = [&]() {
         if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
         else if (hier)
@@ -636,8 +663,8 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         else k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     };
     if (affine) {
-        k_phase_a_affine<<<ba_grid, kBAThreads, kPhaseADynSmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
-                                                                      ba_work);
+        k_phase_a_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
+                                                               n_out);
     } else {
         k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
     }
@@ -651,9 +678,9 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     mark();
     if (affine) {
-        k_phase_b_affine<<<ba_grid, kBAThreads, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
-                                                        t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
-                                                        w.ba_scratch, ba_work);
+        k_phase_b_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
+                                                              t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
+                                                              w.ba_scratch, n_out);
     } else {
         k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                        t.tap_perm[0], t.tap_items[1], t.tap_offsets[1],
@@ -674,8 +701,8 @@ cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cuda
 // Resident blocks per SM of the batch-affine kernels (sizes their persistent grid).
 int batch_affine_blocks_per_sm() {
     int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_phase_a_affine, kBAThreads, kPhaseADynSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_phase_b_affine, kBAThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_phase_a_affine, kBAThreads, kBASmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_phase_b_affine, kBAThreads, kBASmem);
     return std::max(1, std::min(a, b));
 }
 
@@ -687,7 +714,9 @@ cudaError_t configure_proof_kernels() {
     e = cudaFuncSetAttribute(k_blob_to_coeffs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kBlobElems * sizeof(Fr)));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseADynSmem);
+    e = cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBASmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_phase_b_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBASmem);
 }
 
 } // namespace vkzg
