@@ -33,7 +33,7 @@ R_MOD = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
 BLOB = 131072
 EXT = 262144
 PROOFS = 6144
-METRIC = "proof & recovery blobs/s at 256 blobs, bit-exact"
+METRIC = "proof & recovery blobs/s at 256 blobs, bit-exact; served p50/p99 latency"
 
 # Algorithmic work per blob of the reference algorithm (frozen per-unit figures):
 # 1 Fp multiply = 4*12^2 = 576 32-bit IMAD, 1 Fr multiply = 4*8^2 = 256.
@@ -202,14 +202,109 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------- GPU arm
-def run_ours(args, rank, world, local_rank):
+def plain_rates(prover, h_blobs, h_cells, h_present, sample):
+    """The plain form: one blocking C-ABI call per blob (pinned host buffers)."""
     import torch
-    import torch.distributed as dist
+    out_p = torch.empty(PROOFS, dtype=torch.uint8).pin_memory()
+    out_c = torch.empty(EXT, dtype=torch.uint8).pin_memory()
+    for k in range(2):  # warm the size-1 class
+        prover.compute_proofs_raw(out_p.data_ptr(), h_blobs.data_ptr() + k * BLOB, 1)
+        prover.recover_cells_raw(out_c.data_ptr(), h_cells.data_ptr() + k * EXT, h_present.data_ptr() + k * 128, 1)
+    t0 = time.perf_counter()
+    for k in range(sample):
+        assert prover.compute_proofs_raw(out_p.data_ptr(), h_blobs.data_ptr() + k * BLOB, 1) == 0
+    tp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for k in range(sample):
+        assert prover.recover_cells_raw(out_c.data_ptr(), h_cells.data_ptr() + k * EXT,
+                                        h_present.data_ptr() + k * 128, 1) == 0
+    tr = time.perf_counter() - t0
+    rp, rr = sample / tp, sample / tr
+    return {"value": 1.0 / (1.0 / rp + 1.0 / rr), "unit": "blobs/s", "proof_blobs_per_s": rp,
+            "recovery_blobs_per_s": rr, "sample": f"{sample} proof + {sample} recovery calls of 1 blob"}
+
+
+def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions, seconds, seed=99):
+    """Served mixed stream (continuous batching, vkzg_b200_server_*): Poisson arrivals,
+    request sizes geometric with mean 6 in 1..64 blobs, 70% proof requests and 30%
+    recovery requests (64..127 cells present).  One segment per offered load
+    (fraction x capacity blobs/s); latency is submit-to-completion inside the server."""
+    import queue
     import vkzg_b200
+    rng = np.random.default_rng(seed)
+    results, checks = [], []
+    with vkzg_b200.Server(max_blobs_per_batch=128, lanes=3, hbm_budget_bytes=8 << 30) as srv:
+        for frac in fractions:
+            offered = frac * capacity
+            req_rate = offered / 6.0
+            tickets = queue.Queue()
+            statuses = []
+
+            def waiter():
+                while True:
+                    item = tickets.get()
+                    if item is None:
+                        return
+                    statuses.append(srv.wait(item[0]))
+                    if len(checks) < 24 and item[1] is not None:
+                        checks.append(item[1])
+
+            th = threading.Thread(target=waiter, daemon=True)
+            th.start()
+            srv.stats(reset=True)
+            t_start = time.perf_counter()
+            t_next = t_start
+            while True:
+                t_next += rng.exponential(1.0 / req_rate)
+                if t_next - t_start > seconds:
+                    break
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                n = int(min(64, rng.geometric(1.0 / 6.0)))
+                first = int(rng.integers(0, n_pool - n + 1))
+                if rng.random() < 0.7:
+                    out = np.empty(n * PROOFS, np.uint8)
+                    t = srv.submit_proofs(out, h_blobs.data_ptr() + first * BLOB, n)
+                    tickets.put((t, ("proofs", first, n, out)))
+                else:
+                    out = np.empty(n * EXT, np.uint8)
+                    t = srv.submit_recovery(out, h_cells.data_ptr() + first * EXT,
+                                            h_present.data_ptr() + first * 128, n)
+                    tickets.put((t, ("recovery", first, n, out)))
+            tickets.put(None)
+            th.join()
+            st = srv.stats()
+            assert all(x == 0 for x in statuses), "served request failed"
+            results.append({"offered_blobs_per_s": round(offered, 1),
+                            "served_blobs_per_s": round(st["blobs"] / st["seconds"], 1),
+                            "requests": int(st["requests"]), "blobs": int(st["blobs"]),
+                            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                            "p999_ms": round(st["p999_ms"], 3), "max_ms": round(st["max_ms"], 3)})
+    # bit-exactness in the mix: the first requests against direct calls on the same inputs
+    for kind, first, n, out in checks:
+        ref = np.empty_like(out)
+        if kind == "proofs":
+            assert prover.compute_proofs_raw(ref, h_blobs.data_ptr() + first * BLOB, n) == 0
+        else:
+            assert prover.recover_cells_raw(ref, h_cells.data_ptr() + first * EXT,
+                                            h_present.data_ptr() + first * 128, n) == 0
+        assert np.array_equal(ref, out), f"served {kind} request differs from a direct call"
+    return results, len(checks)
+
+
+def run_ours(args, rank, world, local_rank):
+    import tempfile
+    import torch
+    import vkzg_b200
+    from vkzg_b200 import replicas
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     n = args.blobs
+    # the autotuner's decisions are shared with the serving lanes' provers through this file
+    tune_dir = tempfile.mkdtemp(prefix="vkzg_tune_")
+    os.environ["VKZG_TUNE_CACHE"] = os.path.join(tune_dir, "plans.txt")
     prover = vkzg_b200.Prover(max_batch_size=n)
 
     blobs_np = make_blobs(n, 1234 + rank)
@@ -230,16 +325,19 @@ def run_ours(args, rank, world, local_rank):
                                           d_err.data_ptr() + 4 * n, n, sp)
         assert rc == 0
 
-    # ---- device-resident arm: inputs in HBM, CUDA events on the launching stream
+    # ---- warm-up: the autotuner times the proof plans of every size class up to n
+    tuning = prover.autotune(n)
     for _ in range(args.warmup):
         device_step()
     torch.cuda.synchronize()
-    assert int(d_err[:n - 4].count_nonzero()) == 0
+    assert int(d_err.count_nonzero()) == 0
+
+    # ---- device-resident arm: inputs in HBM, CUDA events on the launching stream
     prover.set_stage_timing(True)
     step_ms, phase_a_ms, stages_acc = [], [], {}
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(dev)
     torch.cuda.synchronize()
+    launches0 = vkzg_b200.kernel_launches()
     with ClockSampler(local_rank) as clocks:
         for _ in range(args.steps):
             flush.fill_(1)
@@ -257,12 +355,9 @@ def run_ours(args, rank, world, local_rank):
             phase_a_ms.append(st["phase_a"])
             step_ms.append(e0.elapsed_time(e2))
         torch.cuda.synchronize()
+    launches = vkzg_b200.kernel_launches() - launches0
     prover.set_stage_timing(False)
-    total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(sum(step_ms), dev)
     value = world * n * args.steps / (total_ms / 1e3)
 
     # ---- end-to-end arm: public C ABI with pinned host buffers, copies in the timed region
@@ -273,28 +368,38 @@ def run_ours(args, rank, world, local_rank):
     h_out = torch.empty(n * EXT, dtype=torch.uint8).pin_memory()
 
     def e2e_step():
+        t0 = time.perf_counter()
         rc = prover.compute_proofs_raw(h_proofs.data_ptr(), h_blobs.data_ptr(), n)
+        t1 = time.perf_counter()
         rc2 = prover.recover_cells_raw(h_out.data_ptr(), h_cells.data_ptr(), h_present.data_ptr(), n)
         assert rc == 0 and rc2 == 0
+        return t1 - t0, time.perf_counter() - t1
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(dev)
     torch.cuda.synchronize()
-    e2e_s = []
+    e2e_p, e2e_r = [], []
     for _ in range(args.steps):
         flush.fill_(1)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2e_step()
-        torch.cuda.synchronize()
-        e2e_s.append(time.perf_counter() - t0)
-    te = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * args.steps / float(te.item())
+        tp, tr = e2e_step()
+        e2e_p.append(tp)
+        e2e_r.append(tr)
+    e2e_total = replicas.max_over_ranks(sum(e2e_p) + sum(e2e_r), dev)
+    e2e_value = world * n * args.steps / e2e_total
+    e2e_proof_rate = n * args.steps / sum(e2e_p)
+    e2e_rec_rate = n * args.steps / sum(e2e_r)
 
+    # ---- the plain form (one call per blob) and the served form, one replica each
+    plain = plain_rates(prover, h_blobs, h_cells, h_present, args.plain_sample) if not args.no_plain else None
+    serving, checked = None, 0
+    if args.serve_seconds > 0:
+        capacity = 1.0 / (0.7 / e2e_proof_rate + 0.3 / e2e_rec_rate)
+        fractions = [float(x) for x in args.serve_loads.split(",")]
+        serving, checked = serve_sweep(prover, h_blobs, h_cells, h_present, n, capacity, fractions,
+                                       args.serve_seconds)
+    replicas.barrier(dev)
     if rank != 0:
         return
 
@@ -316,7 +421,6 @@ def run_ours(args, rank, world, local_rank):
                          f"on {c['threads']} host threads ({c['seconds']:.1f} s)",
                "proof_blobs_per_s": c["proof_blobs_per_s"], "recovery_blobs_per_s": c["recovery_blobs_per_s"]}
 
-    launches_per_step = 10 * ((n + prover_cap(n) - 1) // prover_cap(n)) + 2 * ((n + prover_cap(n) - 1) // prover_cap(n))
     line = {
         "metric": METRIC, "value": value, "unit": "blobs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
@@ -324,28 +428,33 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded uniform Fr blobs + 4 adversarial; seeded uneven survivor sets)",
         "config": {"workload": "proofs 256 blobs + uneven recovery 256 blobs per GPU", "blobs": n,
                    "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)",
-                   "setup": "mainnet G1 monomial, FK20 tables generated on the GPU"},
+                   "setup": "mainnet G1 monomial, FK20 tables generated on the GPU",
+                   "tuned_plans": {str(k): v[0] for k, v in tuning.items()}},
         "proof_blobs_per_s": world * n / (proof_ms / 1e3),
         "recovery_blobs_per_s": world * n / (rec_ms / 1e3) if rec_ms > 0 else None,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "e2e": {"value": e2e_value, "unit": "blobs/s",
                 "h2d_bytes_per_step": n * BLOB + n * EXT + n * 128,
-                "d2h_bytes_per_step": n * PROOFS + n * EXT + 4 * n},
-        "roofline": {"kernel": "k_phase_a", "bound": "int", "achieved": achieved, "peak": imad_peak,
+                "d2h_bytes_per_step": n * PROOFS + n * EXT,
+                "proof_blobs_per_s": world * e2e_proof_rate, "recovery_blobs_per_s": world * e2e_rec_rate},
+        "plain_per_blob": plain,
+        "batched_over_plain": (e2e_value / world) / plain["value"] if plain else None,
+        "serving": {"sweep": serving, "lanes": 3, "max_blobs_per_batch": 128, "hbm_budget_bytes": 8 << 30,
+                    "seconds_per_load": args.serve_seconds, "bit_exact_checked_requests": checked,
+                    "mix": "Poisson arrivals; 1-64 blobs per request (geometric, mean 6); 70% proofs, "
+                           "30% recovery with 64-127 cells present"} if serving else None,
+        "roofline": {"kernel": "k_phase_a_affine", "bound": "int", "achieved": achieved, "peak": imad_peak,
                      "unit": "TIMAD/s", "frac": achieved / imad_peak,
                      "peak_source": "measured in-process (vkzg_b200_microbench IMAD probe); "
                                     f"nominal 148 SM x 64/clk x 1.965 GHz = {NOMINAL_IMAD_TPS:.1f}",
-                     "algorithmic": f"{PHASE_A_FP_MUL_PER_BLOB:.3g} Fp mul x 576 IMAD per blob x {n} blobs",
+                     "algorithmic": f"{PHASE_A_FP_MUL_PER_BLOB:.3g} Fp mul x 576 IMAD per blob x {n} blobs "
+                                    "(the reference's madd-2007-bl bucket accumulation)",
                      "traffic": None},
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
-
-
-def prover_cap(n):
-    return n
 
 
 def main():
@@ -358,6 +467,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--ref-sample", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-sample", type=int, default=16)
+    ap.add_argument("--serve-seconds", type=float, default=6.0, help="per offered load; 0 skips serving")
+    ap.add_argument("--serve-loads", default="0.3,0.6,0.9", help="offered loads as fractions of batched capacity")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -119,6 +119,13 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms3, int cap);
 
 /*
+ * Number of CUDA kernels this library has launched in this process (proof,
+ * recovery, cells and table-generation launchers; the diagnostics below are not
+ * counted).  No counterpart in the reference.
+ */
+uint64_t vkzg_b200_kernel_launches(void);
+
+/*
  * Serving loop with continuous batching (the reference has none: one blocking
  * batch call per caller, serialised per prover, src/vkzg.cpp:1183-1218).
  *

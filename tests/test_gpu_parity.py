@@ -22,6 +22,22 @@ def test_device_tables_match_oracle(oracle, mainnet_tables, mainnet_setup, tmp_p
     assert np.array_equal(got, want)
 
 
+def test_tables_cache_file(mainnet_tables, golden_proofs, tmp_path, monkeypatch):
+    """$VKZG_TABLES_CACHE: the first prover generates the tables and writes them
+    there (the oracle's bytes); the next one loads that file and proves the same."""
+    cache = str(tmp_path / "cache.bin")
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.setenv("VKZG_TABLES_CACHE", cache)
+    blob = golden_proofs["valid_blobs"][1].tobytes()
+    with vkzg_b200.Prover(max_batch_size=1) as p1:
+        assert p1.tables_source().startswith("generated:") and cache in p1.tables_source()
+        first = p1.compute_cell_kzg_proofs_batch(blob, 1)
+    assert np.array_equal(np.fromfile(cache, np.uint8), mainnet_tables.serialize())
+    with vkzg_b200.Prover(max_batch_size=1) as p2:
+        assert p2.tables_source() == "file:" + cache
+        assert p2.compute_cell_kzg_proofs_batch(blob, 1) == first == golden_proofs["valid_proofs"][1].tobytes()
+
+
 @pytest.fixture(scope="module")
 def synthetic_prover(synthetic, tmp_path_factory):
     tau, mono, tables = synthetic

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_autotune", "vkzg_b200_tuning_table", "vkzg_b200_recover_cells_and_proofs_batch",
     "vkzg_b200_server_options_default", "vkzg_b200_server_new", "vkzg_b200_server_free",
     "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
-    "vkzg_b200_server_stats",
+    "vkzg_b200_server_stats", "vkzg_b200_kernel_launches",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -143,6 +143,8 @@ def library():
             L.vkzg_b200_server_wait.restype = ctypes.c_int
             L.vkzg_b200_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats), ctypes.c_int]
             L.vkzg_b200_server_stats.restype = ctypes.c_int
+            L.vkzg_b200_kernel_launches.argtypes = []
+            L.vkzg_b200_kernel_launches.restype = ctypes.c_uint64
             _lib = L
     return _lib
 
@@ -364,6 +366,11 @@ class Server:
         st = ServerStats()
         _check(self._lib.vkzg_b200_server_stats(self._h, ctypes.byref(st), 1 if reset else 0))
         return st.as_dict()
+
+
+def kernel_launches():
+    """Kernels the library has launched in this process (vkzg_b200_kernel_launches)."""
+    return int(library().vkzg_b200_kernel_launches())
 
 
 def microbench(which):

@@ -72,6 +72,7 @@ cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *c
     static const Fr scale = fr_to_canonical(fr_inv(fr_from_u32(kBlobElems)));
     k_blob_to_cells<<<n, kCellsThreads, kBlobElems * sizeof(Fr), s>>>(blobs, cells, scratch, t.roots_fwd,
                                                                       t.roots_inv, scale, err);
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -53,6 +53,7 @@ struct ProofWork {
     G1A *bucket_aff = nullptr;  // [cap][128][128] affine bucket sums
     G1A *ba_scratch = nullptr;  // [ba_blocks][kBAScratchPoints]
     int ba_blocks = 0;          // persistent grid size of the batch-affine kernels
+    uint32_t *task_ctr = nullptr; // [2] next task of phase A / phase B (zeroed before phase A)
     int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
     G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
 };
@@ -92,5 +93,8 @@ size_t setup_scratch_bytes();
 cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
                                 uint32_t *d_err, cudaStream_t s);
 cudaError_t configure_kernels();
+// process-wide count of kernels launched by the launchers above
+void count_launches(int k);
+uint64_t launches_total();
 
 } // namespace vkzg

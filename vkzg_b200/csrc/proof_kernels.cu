@@ -347,6 +347,15 @@ __device__ __forceinline__ void store_warp_sums(const WarpBuckets<kWarpNB> &wb, 
     }
 }
 
+// Tasks are handed out by a global counter rather than by a fixed stride: all
+// tasks cost about the same, but warps on an SM that holds fewer of them run
+// faster, so taking the next task when done balances the work per SM.
+__device__ __forceinline__ int next_task(uint32_t *ctr) {
+    uint32_t t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(ctr, 1u);
+    return (int)__shfl_sync(0xffffffffu, t, 0);
+}
+
 // Exclusive scan of cnt[0..NB) into a[0..NB] and b[0..NB) (two copies).
 template <int NB>
 __device__ __forceinline__ void warp_exclusive_scan(const uint32_t *cnt, uint32_t *a, uint32_t *b) {
@@ -377,14 +386,15 @@ __device__ __forceinline__ void warp_exclusive_scan(const uint32_t *cnt, uint32_
 // shared atomics, a scan, a scatter into its scratch) and sums the buckets.
 __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_a_affine(const Fr *__restrict__ scalars,
                                                                           const G1A *__restrict__ pos,
-                                                                          G1A *bucket_aff, G1A *scratch, int n_out) {
+                                                                          G1A *bucket_aff, G1A *scratch, int n_out,
+                                                                          uint32_t *task_ctr) {
     extern __shared__ uint4 dyn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuckets<kWarpNB> &wb = reinterpret_cast<WarpBuckets<kWarpNB> *>(dyn_smem)[warp];
     const WarpScratch ws = warp_scratch(scratch);
     constexpr int kScalars = kWarpOutputs * kCellElems;
     const int n_tasks = n_out / kWarpOutputs;
-    for (int task = blockIdx.x * kBAWarps + warp; task < n_tasks; task += gridDim.x * kBAWarps) {
+    for (int task = next_task(task_ctr); task < n_tasks; task = next_task(task_ctr)) {
         const int o0 = task * kWarpOutputs;
         const Fr *sc_base = scalars + (size_t)o0 * kCellElems;
         for (int k = lane; k < kWarpNB; k += 32) wb.cnt[k] = 0;
@@ -439,13 +449,13 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(con
                                                                           const uint32_t *__restrict__ items_m,
                                                                           const uint32_t *__restrict__ off_m,
                                                                           G1A *bucket_aff, G1A *scratch,
-                                                                          int n_out) {
+                                                                          int n_out, uint32_t *task_ctr) {
     extern __shared__ uint4 dyn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuckets<kWarpNB> &wb = reinterpret_cast<WarpBuckets<kWarpNB> *>(dyn_smem)[warp];
     const WarpScratch ws = warp_scratch(scratch);
     const int n_tasks = n_out / kWarpOutputs;
-    for (int task = blockIdx.x * kBAWarps + warp; task < n_tasks; task += gridDim.x * kBAWarps) {
+    for (int task = next_task(task_ctr); task < n_tasks; task = next_task(task_ctr)) {
         const int o0 = task * kWarpOutputs;
         for (int k = lane; k < kWarpNB; k += 32) {
             const int kk = k & (kBuckets - 1);
@@ -663,8 +673,9 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         else k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     };
     if (affine) {
+        cudaMemsetAsync(w.task_ctr, 0, 2 * sizeof(uint32_t), s);
         k_phase_a_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
-                                                               n_out);
+                                                               n_out, w.task_ctr);
     } else {
         k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
     }
@@ -680,7 +691,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     if (affine) {
         k_phase_b_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                               t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
-                                                              w.ba_scratch, n_out);
+                                                              w.ba_scratch, n_out, w.task_ctr + 1);
     } else {
         k_phase_b<<<dim3(kCells, n), kBuckets, 0, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                        t.tap_perm[0], t.tap_items[1], t.tap_offsets[1],
@@ -691,6 +702,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
     mark();
+    count_launches(10);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -34,6 +35,10 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
                                 cudaEvent_t *ev);
 cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
                                  cudaEvent_t *ev);
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 } // namespace vkzg
 
 static constexpr int kProofStages = 10;
@@ -361,7 +366,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     w.ba_blocks = (int)p->sm_count * batch_affine_blocks_per_sm();
     if (!p->alloc(w.bucket_aff, B * kCells * kBuckets) ||
         !p->alloc(w.ba_scratch, (size_t)w.ba_blocks * kBAScratchPoints) ||
-        !p->alloc(w.red_scratch, reduce_scratch_points((int)B)))
+        !p->alloc(w.red_scratch, reduce_scratch_points((int)B)) || !p->alloc(w.task_ctr, 2))
         return VKZG_ERR_MALLOC;
     return VKZG_OK;
 }
@@ -369,6 +374,8 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
 } // namespace
 
 // -------------------------------------------------------------- lifecycle
+
+static vkzg_result write_tables_file(const char *out_path, const HostTables &h, const G1A *d_pos);
 
 vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
     if (!out) return VKZG_ERR_BADARGS;
@@ -409,6 +416,8 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
     const std::string libdir = library_dir();
     std::vector<std::string> files;
     if (const char *env = getenv("VKZG_TABLES_PATH")) files.push_back(env);
+    const char *cache = getenv("VKZG_TABLES_CACHE");
+    if (cache && *cache) files.push_back(cache);
     files.push_back(libdir + "/precomputed_tables.bin");
     HostTables h;
     vkzg_result rc = VKZG_ERR_IO;
@@ -436,6 +445,10 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
             if (rc == VKZG_OK && !p->alloc(p->t.pos, kPositionPoints)) rc = VKZG_ERR_MALLOC;
             if (rc == VKZG_OK) rc = generate_position_table(p, setup);
             if (rc == VKZG_OK) p->tables_source = "generated:" + setup_path;
+            // setup cache: the next prover loads the file instead of generating
+            if (rc == VKZG_OK && cache && *cache && cudaStreamSynchronize(p->stream) == cudaSuccess &&
+                write_tables_file(cache, h, p->t.pos) == VKZG_OK)
+                p->tables_source += " (cached to " + std::string(cache) + ")";
         } else if (seen_malformed) {
             rc = VKZG_ERR_SETUP;
         }
@@ -643,6 +656,35 @@ const char *vkzg_b200_stage_name(int recovery, int i) {
     return (i >= 0 && i < kProofStages) ? kProofStageNames[i] : "";
 }
 
+// Writes the tables in the reference's file format (src/precomputed_tables.cpp:
+// 16-58): header, position table, roots, phase-B items, offsets, perms,
+// 1/4096.  Written to a temporary name and renamed, so a reader never sees a
+// partial file.
+static vkzg_result write_tables_file(const char *out_path, const HostTables &h, const G1A *d_pos) {
+    std::vector<uint8_t> pos(kPositionPoints * sizeof(G1A));
+    if (cudaMemcpy(pos.data(), d_pos, pos.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return VKZG_ERR_GPU;
+    const std::string tmp_path = std::string(out_path) + ".tmp";
+    FILE *f = fopen(tmp_path.c_str(), "wb");
+    if (!f) return VKZG_ERR_IO;
+    const uint32_t hdr[4] = {0x475A4B56u, 1u, (uint32_t)h.items[0].size(), (uint32_t)h.items[1].size()};
+    bool ok = fwrite(hdr, 1, 16, f) == 16 && fwrite(pos.data(), 1, pos.size(), f) == pos.size() &&
+              fwrite(h.roots_fwd.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
+              fwrite(h.roots_inv.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
+              fwrite(h.items[0].data(), 4, h.items[0].size(), f) == h.items[0].size() &&
+              fwrite(h.items[1].data(), 4, h.items[1].size(), f) == h.items[1].size() &&
+              fwrite(h.offsets[0], 1, sizeof h.offsets[0], f) == sizeof h.offsets[0] &&
+              fwrite(h.offsets[1], 1, sizeof h.offsets[1], f) == sizeof h.offsets[1] &&
+              fwrite(h.perm[0], 1, sizeof h.perm[0], f) == sizeof h.perm[0] &&
+              fwrite(h.perm[1], 1, sizeof h.perm[1], f) == sizeof h.perm[1] &&
+              fwrite(&h.inv_blob, 1, sizeof h.inv_blob, f) == sizeof h.inv_blob;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok || rename(tmp_path.c_str(), out_path) != 0) {
+        remove(tmp_path.c_str());
+        return VKZG_ERR_IO;
+    }
+    return VKZG_OK;
+}
+
 vkzg_result vkzg_b200_write_tables(const uint8_t *g1_monomial_compressed, const char *out_path) {
     if (!g1_monomial_compressed || !out_path) return VKZG_ERR_BADARGS;
     vkzg_prover tmp; // table storage and stream only
@@ -656,23 +698,7 @@ vkzg_result vkzg_b200_write_tables(const uint8_t *g1_monomial_compressed, const 
     std::vector<uint8_t> setup(g1_monomial_compressed, g1_monomial_compressed + (size_t)kBlobElems * 48);
     rc = generate_position_table(&tmp, setup);
     if (rc != VKZG_OK) return rc;
-    std::vector<uint8_t> pos(kPositionPoints * sizeof(G1A));
-    if (cudaMemcpy(pos.data(), tmp.t.pos, pos.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return VKZG_ERR_GPU;
-    FILE *f = fopen(out_path, "wb");
-    if (!f) return VKZG_ERR_IO;
-    const uint32_t hdr[4] = {0x475A4B56u, 1u, (uint32_t)h.items[0].size(), (uint32_t)h.items[1].size()};
-    bool ok = fwrite(hdr, 1, 16, f) == 16 && fwrite(pos.data(), 1, pos.size(), f) == pos.size() &&
-              fwrite(h.roots_fwd.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
-              fwrite(h.roots_inv.data(), sizeof(Fr), kExtElems, f) == (size_t)kExtElems &&
-              fwrite(h.items[0].data(), 4, h.items[0].size(), f) == h.items[0].size() &&
-              fwrite(h.items[1].data(), 4, h.items[1].size(), f) == h.items[1].size() &&
-              fwrite(h.offsets[0], 1, sizeof h.offsets[0], f) == sizeof h.offsets[0] &&
-              fwrite(h.offsets[1], 1, sizeof h.offsets[1], f) == sizeof h.offsets[1] &&
-              fwrite(h.perm[0], 1, sizeof h.perm[0], f) == sizeof h.perm[0] &&
-              fwrite(h.perm[1], 1, sizeof h.perm[1], f) == sizeof h.perm[1] &&
-              fwrite(&h.inv_blob, 1, sizeof h.inv_blob, f) == sizeof h.inv_blob;
-    fclose(f);
-    return ok ? VKZG_OK : VKZG_ERR_IO;
+    return write_tables_file(out_path, h, tmp.t.pos);
 }
 
 // ------------------------------------------------- device-pointer entry points
@@ -852,6 +878,8 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
     }
     return VKZG_OK;
 }
+
+uint64_t vkzg_b200_kernel_launches(void) { return launches_total(); }
 
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class_out, int *plan_out, double *ms_out, int cap) {
     if (!p) return 0;

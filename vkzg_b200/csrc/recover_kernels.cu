@@ -158,6 +158,7 @@ cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, in
                                                                    t.roots_fwd, t.roots_inv, t.shift_fwd,
                                                                    t.shift_inv);
     if (ev) cudaEventRecord(ev[2], s);
+    count_launches(2);
     return cudaGetLastError();
 }
 
@@ -223,6 +224,7 @@ cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, 
     k_recover_prep<<<n, kCells, 0, s>>>(present, t.roots_fwd, seven64, zv, inv_zc, err);
     k_recover_main<<<n, kRecThreads, kBlobElems * sizeof(Fr), s>>>(cells, out, work, zv, inv_zc, t.roots_fwd,
                                                                    t.roots_inv, t.shift_fwd, t.shift_inv);
+    count_launches(2);
     return cudaGetLastError();
 }
 

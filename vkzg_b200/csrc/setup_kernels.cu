@@ -95,6 +95,7 @@ cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr
     k_setup_columns<<<kCellElems, 64, 0, s>>>(mono, x, roots_fwd);
     k_setup_ladder<<<kCells * kCellElems / 128, 128, 0, s>>>(x, lad);
     k_setup_normalize<<<(int)(kPositionPoints / 256), 256, 0, s>>>(lad, pos, (int)kPositionPoints);
+    count_launches(4);
     return cudaGetLastError();
 }
 
