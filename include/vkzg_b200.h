@@ -103,20 +103,29 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
                                                      size_t num_blobs);
 
 /*
- * Autotuner.  Proof chunks run under one of three plans that compute identical
- * bytes: 0 = serial Jacobian bucket accumulation and reduction (one output per
- * block, the reference's scheme, k_phase_a.comp / k_bucket_reduce.comp);
- * 1 = batch-affine bucket accumulation and a binary-split batch-affine
- * reduction; 2 = batch-affine accumulation with the serial reduction.  The
- * first chunk of each power-of-two size class is timed under all plans and the
- * fastest is kept (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
+ * Autotuner.  Proof chunks run under one of VKZG_B200_PLANS plans that compute
+ * identical bytes: 0 = serial Jacobian bucket accumulation and reduction (one
+ * output per block, the reference's scheme, k_phase_a.comp /
+ * k_bucket_reduce.comp); 1 = batch-affine bucket accumulation and a
+ * binary-split batch-affine reduction; 2 = batch-affine accumulation with the
+ * serial reduction; 3 = phase A as plain sums over a precomputed digit table
+ * (every signed c-bit digit multiple of every base, c = 12 by default: 35 GB
+ * of HBM, built on first use and shared by the process's provers with the same
+ * setup; $VKZG_COMB_BITS picks c in 10..14 or 0 to disable it; smaller c is used
+ * when free memory is short), phase B as plan 1.  The first chunk of each
+ * power-of-two size class is timed under all plans and the fastest is kept
+ * (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
  * vkzg_b200_autotune tunes every size class up to max_blobs (0 = the prover's
  * max_batch_size) on seeded synthetic blobs; vkzg_b200_tuning_table reports the
- * decisions (size class, plan, and the three plans' times in ms, -1 if loaded
- * from the cache) and returns how many classes are tuned.
+ * decisions (size class, plan, and VKZG_B200_PLANS times in ms per class, -1
+ * where a plan was not timed) and returns how many classes are tuned.
+ * vkzg_b200_digit_table returns the digit table's window c (0 = none built),
+ * its build time and size.
  */
+#define VKZG_B200_PLANS 4
 vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
-int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms3, int cap);
+int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms, int cap);
+int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes);
 
 /*
  * Number of CUDA kernels this library has launched in this process (proof,

@@ -1,0 +1,71 @@
+"""Plan 3 (phase A as plain sums over the precomputed digit table) against the
+consensus vectors, the oracle and the other plans, for several window widths."""
+import numpy as np
+import pytest
+
+import vkzg_b200
+from conftest import adversarial_blobs, random_blobs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("bits", [10, 11])
+def test_plan3_mainnet_vectors(golden_proofs, monkeypatch, bits):
+    """Every valid vector, batched, with the window forced to `bits`."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.setenv("VKZG_PLAN", "3")
+    monkeypatch.setenv("VKZG_COMB_BITS", str(bits))
+    n = len(golden_proofs["valid_names"])
+    with vkzg_b200.Prover(max_batch_size=n) as p:
+        out = p.compute_cell_kzg_proofs_batch(golden_proofs["valid_blobs"].tobytes(), n)
+        assert p.digit_table()[0] == bits
+    for k in range(n):
+        assert out[k * 6144:(k + 1) * 6144] == golden_proofs["valid_proofs"][k].tobytes(), k
+
+
+def test_plan3_synthetic_vs_oracle(synthetic, oracle, tmp_path, monkeypatch):
+    """Seeded random and the four adversarial blobs under a synthetic setup,
+    default window, against the oracle."""
+    tau, mono, tables = synthetic
+    path = str(tmp_path / "synthetic_tables.bin")
+    vkzg_b200.write_tables(mono, path)
+    monkeypatch.setenv("VKZG_TABLES_PATH", path)
+    monkeypatch.setenv("VKZG_PLAN", "3")
+    monkeypatch.delenv("VKZG_COMB_BITS", raising=False)
+    blobs = np.concatenate([random_blobs(12, 303), adversarial_blobs()])
+    out = np.zeros(len(blobs) * 6144, np.uint8)
+    with vkzg_b200.Prover(max_batch_size=len(blobs)) as p:
+        assert p.compute_proofs_raw(out, blobs, len(blobs)) == 0
+        c, build_ms, nbytes = p.digit_table()
+        assert 10 <= c <= 12 and nbytes > 0
+    rc, want = oracle.compute_proofs(tables, blobs)
+    assert rc == 0
+    for b in range(len(blobs)):
+        assert np.array_equal(out[b * 6144:(b + 1) * 6144], want[b * 6144:(b + 1) * 6144]), b
+
+
+def test_plans_agree_and_tuner_times_plan3(monkeypatch):
+    """All plans give the same bytes at 32 blobs; the tuner times plan 3 for
+    size classes of at least 16 blobs and shares one table between provers."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.delenv("VKZG_PLAN", raising=False)
+    monkeypatch.setenv("VKZG_COMB_BITS", "10")
+    blobs = random_blobs(32, 404)
+    outs = []
+    for plan in range(vkzg_b200.PLANS):
+        monkeypatch.setenv("VKZG_PLAN", str(plan))
+        with vkzg_b200.Prover(max_batch_size=32) as p:
+            out = np.zeros(32 * 6144, np.uint8)
+            assert p.compute_proofs_raw(out, blobs, 32) == 0
+            outs.append(out)
+    for out in outs[1:]:
+        assert np.array_equal(out, outs[0])
+    monkeypatch.delenv("VKZG_PLAN")
+    with vkzg_b200.Prover(max_batch_size=32) as p, vkzg_b200.Prover(max_batch_size=32) as q:
+        table = p.autotune(32)
+        assert table[32][1][3] > 0 and table[16][1][3] > 0 and table[8][1][3] == -1
+        out = np.zeros(32 * 6144, np.uint8)
+        assert p.compute_proofs_raw(out, blobs, 32) == 0
+        assert np.array_equal(out, outs[0])
+        q.autotune(16)
+        assert q.digit_table()[1] == p.digit_table()[1]  # same table object: same build record

@@ -29,6 +29,8 @@ BYTES_PER_EXT_BLOB = CELL_PROOFS_PER_BLOB * BYTES_PER_CELL
 OK, ERR_BADARGS, ERR_MALLOC, ERR_IO, ERR_SETUP, ERR_GPU, ERR_INVALID_BLOB = range(7)
 
 # every symbol declared in include/vkzg.h and include/vkzg_b200.h
+PLANS = 4  # VKZG_B200_PLANS
+
 EXPORTED_SYMBOLS = (
     "vkzg_error_string", "vkzg_options_default", "vkzg_prover_new", "vkzg_prover_free",
     "vkzg_prover_device_name", "vkzg_prover_gpu_core_count", "vkzg_compute_proofs_batch",
@@ -40,7 +42,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_autotune", "vkzg_b200_tuning_table", "vkzg_b200_recover_cells_and_proofs_batch",
     "vkzg_b200_server_options_default", "vkzg_b200_server_new", "vkzg_b200_server_free",
     "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
-    "vkzg_b200_server_stats", "vkzg_b200_kernel_launches",
+    "vkzg_b200_server_stats", "vkzg_b200_kernel_launches", "vkzg_b200_digit_table",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -143,6 +145,8 @@ def library():
             L.vkzg_b200_server_wait.restype = ctypes.c_int
             L.vkzg_b200_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats), ctypes.c_int]
             L.vkzg_b200_server_stats.restype = ctypes.c_int
+            L.vkzg_b200_digit_table.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]
+            L.vkzg_b200_digit_table.restype = ctypes.c_int
             L.vkzg_b200_kernel_launches.argtypes = []
             L.vkzg_b200_kernel_launches.restype = ctypes.c_uint64
             _lib = L
@@ -291,18 +295,25 @@ class Prover:
         return bytes(out[:len(cells)]), bytes(proofs[:blob_count * CELL_PROOFS_PER_BLOB * BYTES_PER_PROOF])
 
     def autotune(self, max_blobs=0):
-        """Times the three proof plans for every power-of-two size class up to max_blobs."""
+        """Times the proof plans for every power-of-two size class up to max_blobs."""
         _check(self._lib.vkzg_b200_autotune(self._h, int(max_blobs)))
         return self.tuning_table()
 
     def tuning_table(self):
-        """{size_class: (plan, (ms_plan0, ms_plan1, ms_plan2))}"""
+        """{size_class: (plan, (ms of plan 0, ..., ms of plan PLANS-1))}, -1 for plans not timed."""
         cap = 32
         sc = (ctypes.c_uint32 * cap)()
         pl = (ctypes.c_int * cap)()
-        ms = (ctypes.c_double * (3 * cap))()
+        ms = (ctypes.c_double * (PLANS * cap))()
         n = self._lib.vkzg_b200_tuning_table(self._h, sc, pl, ms, cap)
-        return {int(sc[i]): (int(pl[i]), tuple(ms[3 * i:3 * i + 3])) for i in range(min(n, cap))}
+        return {int(sc[i]): (int(pl[i]), tuple(ms[PLANS * i:PLANS * i + PLANS])) for i in range(min(n, cap))}
+
+    def digit_table(self):
+        """(window bits c, build ms, bytes) of plan 3's digit table, or None before it is built."""
+        ms = ctypes.c_double()
+        nb = ctypes.c_uint64()
+        c = self._lib.vkzg_b200_digit_table(self._h, ctypes.byref(ms), ctypes.byref(nb))
+        return (c, ms.value, nb.value) if c else None
 
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)

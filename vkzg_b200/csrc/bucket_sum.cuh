@@ -249,4 +249,5 @@ __device__ G1A *wb_bucket_sums(WarpBuckets<NB> &wb, const Src0 &src0, G1A *buf0,
     return cur;
 }
 
+
 } // namespace vkzg

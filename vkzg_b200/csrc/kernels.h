@@ -54,6 +54,15 @@ struct ProofWork {
     G1A *ba_scratch = nullptr;  // [ba_blocks][kBAScratchPoints]
     int ba_blocks = 0;          // persistent grid size of the batch-affine kernels
     uint32_t *task_ctr = nullptr; // [2] next task of phase A / phase B (zeroed before phase A)
+    const G1A *comb = nullptr;    // plan 3: digit table [128 j][64 i][D][2^(c-1)], shared by provers
+    int comb_c = 0;               // its window width
+    // plan 3's grid-wide tree rounds (flat_sizes gives the sizes)
+    int16_t *flat_dig = nullptr;  // [cap * 128][64 D] digits
+    G1A *flat_buf[2] = {nullptr, nullptr};
+    uint32_t *flat_pre = nullptr;
+    Fp *flat_others = nullptr, *flat_tot = nullptr, *flat_totinv = nullptr;
+    size_t flat_slots = 0;
+    int flat_blocks = 0;
     int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
     G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
 };
@@ -90,6 +99,13 @@ cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, c
 // Table generation from 4096 compressed monomial points already on the device.
 // Writes t.pos; needs `scratch` of at least setup_scratch_bytes().
 size_t setup_scratch_bytes();
+size_t comb_build_scratch_bytes(int c);
+struct FlatSizes {
+    int blocks = 0;
+    size_t lanes = 0, dig = 0, buf0 = 0, buf1 = 0, slots = 0, pre_words = 0;
+};
+FlatSizes flat_sizes(int cap, int c);
+cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int c, cudaStream_t s);
 cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
                                 uint32_t *d_err, cudaStream_t s);
 cudaError_t configure_kernels();

@@ -314,6 +314,10 @@ constexpr int kWarpNB = kWarpOutputs * kBuckets;
 constexpr int kBAMinBlocks = 65536 / (kBAThreads * 128); // at most 128 registers per thread
 constexpr size_t kBASmem = kBAWarps * sizeof(WarpBuckets<kWarpNB>);
 static_assert(kCells % kWarpOutputs == 0, "a task stays within one blob");
+// phase B also stages the tap items (at most one per tap and digit) and their
+// bucket offsets of both halves in shared memory
+constexpr int kTapItemsMax = kHalf * kDigits;
+constexpr size_t kPhaseBSmem = kBASmem + (2 * kTapItemsMax + 2 * (kBuckets + 1)) * sizeof(uint32_t);
 static_assert(kBAThreads == VKZG_BA_THREADS, "scratch sized for this block");
 
 struct WarpScratch {
@@ -444,15 +448,27 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_a_affine(con
 // minus-half taps (negacyclic: tap e > a - 64 flips sign), over the blob's
 // normalised ladder points.
 __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(const G1A *__restrict__ ladder_aff,
-                                                                          const uint32_t *__restrict__ items_p,
-                                                                          const uint32_t *__restrict__ off_p,
-                                                                          const uint32_t *__restrict__ items_m,
-                                                                          const uint32_t *__restrict__ off_m,
+                                                                          const uint32_t *__restrict__ g_items_p,
+                                                                          const uint32_t *__restrict__ g_off_p,
+                                                                          const uint32_t *__restrict__ g_items_m,
+                                                                          const uint32_t *__restrict__ g_off_m,
                                                                           G1A *bucket_aff, G1A *scratch,
                                                                           int n_out, uint32_t *task_ctr) {
     extern __shared__ uint4 dyn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuckets<kWarpNB> &wb = reinterpret_cast<WarpBuckets<kWarpNB> *>(dyn_smem)[warp];
+    uint32_t *items_p = reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(dyn_smem) + kBASmem);
+    uint32_t *items_m = items_p + kTapItemsMax;
+    uint32_t *off_p = items_m + kTapItemsMax;
+    uint32_t *off_m = off_p + kBuckets + 1;
+    for (int k = threadIdx.x; k <= kBuckets; k += kBAThreads) {
+        off_p[k] = __ldg(&g_off_p[k]);
+        off_m[k] = __ldg(&g_off_m[k]);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < off_p[kBuckets]; k += kBAThreads) items_p[k] = __ldg(&g_items_p[k]);
+    for (uint32_t k = threadIdx.x; k < off_m[kBuckets]; k += kBAThreads) items_m[k] = __ldg(&g_items_m[k]);
+    __syncthreads();
     const WarpScratch ws = warp_scratch(scratch);
     const int n_tasks = n_out / kWarpOutputs;
     for (int task = next_task(task_ctr); task < n_tasks; task = next_task(task_ctr)) {
@@ -460,7 +476,7 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(con
         for (int k = lane; k < kWarpNB; k += 32) {
             const int kk = k & (kBuckets - 1);
             const uint32_t *off = (o0 + (k >> 7)) % kCells >= kHalf ? off_m : off_p;
-            wb.cnt[k] = __ldg(&off[kk + 1]) - __ldg(&off[kk]);
+            wb.cnt[k] = off[kk + 1] - off[kk];
         }
         __syncwarp();
         auto src0 = [=](int k, uint32_t e) {
@@ -470,7 +486,7 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(con
             const int aa = a & (kHalf - 1);
             const uint32_t *items = minus ? items_m : items_p;
             const uint32_t *off = minus ? off_m : off_p;
-            const uint32_t packed = __ldg(&items[__ldg(&off[kk]) + e]);
+            const uint32_t packed = items[off[kk] + e];
             const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
             const G1A *lad = ladder_aff + ((size_t)b * kCells + (minus ? kHalf : 0)) * kDigits;
             G1A pt = ld_vec(&lad[((aa - tap) & (kHalf - 1)) * kDigits + d]);
@@ -482,6 +498,312 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(con
         store_warp_sums(wb, res, slot, bucket_aff + (size_t)o0 * kBuckets);
         __syncwarp();
     }
+}
+
+// ------------------------------------------------ phase A over a digit table
+// Fixed-base comb: the bases X[j][i] of phase A are setup constants, so with
+// c-bit signed windows every digit value has its own precomputed point,
+//   comb[j][i][k][m - 1] = m 2^(c k) X[j][i],   m = 1..2^(c-1), k < D = ceil(256 / c),
+// and output o = (blob, j) is a plain sum of 64 * D table points (one per
+// nonzero digit, negated for negative digits): no buckets, no bucket
+// reduction.  c = 12 takes 1408 additions per output against the reference
+// form's 2048 bucket additions plus the 128-bucket reduction, for a 35.4 GB
+// table (HBM holds it; the reads are 96-byte gathers, ~4 GB per 256 blobs).
+
+// Bits [off, off + c) of a canonical 256-bit scalar.
+__device__ __forceinline__ uint32_t scalar_window(const Fr &s, int off, int c) {
+    const int w = off >> 5, sh = off & 31;
+    const uint64_t lo = w < 8 ? s.v[w] : 0u, hi = w + 1 < 8 ? s.v[w + 1] : 0u;
+    return (uint32_t)((((hi << 32) | lo) >> sh) & ((1ull << c) - 1));
+}
+
+// Plan 3's phase A as grid-wide tree rounds.  The 64 D digit-table points of
+// every output form a list; round r adds elements (2i, 2i+1) of every list of
+// the chunk at once, with the pairs of all lists dealt to all lanes of the grid
+// (pair p to lane p mod lanes).  A round is three launches: pass 1 (each lane's
+// running product of its denominators, then the warp's product), one launch
+// that inverts every warp's product (32 per warp, one inversion per warp), and
+// pass 2 (the lane's inverses and the additions).  No warp waits on a
+// one-lane inversion of its own, and every lane has pairs until the lists are
+// short.
+constexpr int kFlatThreads = 256;
+
+struct FlatArgs {
+    const int16_t *dig;  // [list][64 D] signed digits
+    const G1A *comb;     // digit table
+    size_t per_j;        // points per column j of the table
+    int H, L;            // 2^(c-1), 64 D
+    const G1A *src;      // round input lists (round 1: the table)
+    G1A *dst;            // round output lists
+    uint32_t *pre;       // per warp: slots x 12 x 32 words of prefix products
+    Fp *others;          // per lane: product of the other lanes' running products
+    Fp *tot, *totinv;    // per warp: product of all, and its inverse
+    size_t slots;
+    int n_lists;
+};
+
+template <bool FIRST>
+__device__ __forceinline__ G1A flat_load(const FlatArgs &a, uint32_t o, uint32_t t, uint32_t m) {
+    if (FIRST) {
+        const int v = a.dig[(size_t)o * a.L + t];
+        G1A pt;
+        if (v == 0) {
+            pt.x = fp_zero();
+            pt.y = fp_zero();
+            return pt;
+        }
+        pt = ldg_vec(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)]);
+        if (v < 0) pt.y = fp_neg(pt.y);
+        return pt;
+    }
+    return ld_vec(&a.src[(size_t)o * m + t]);
+}
+
+// Signed c-bit digits of every scalar: scalar q = o 64 + i fills dig[q D ..].
+__global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, int c, int D,
+                                                    int n_scalars) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_scalars) return;
+    const Fr sc = ld_vec(&scalars[q]);
+    int16_t *d = dig + (size_t)q * D;
+    const int H = 1 << (c - 1);
+    int carry = 0;
+    for (int k = 0; k < D; k++) {
+        const int v = (int)scalar_window(sc, k * c, c) + carry;
+        carry = v > H ? 1 : 0;
+        d[k] = (int16_t)(v - (carry << c));
+    }
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t h = m >> 1;
+    const size_t P = (size_t)a.n_lists * h;
+    uint32_t *pre = a.pre + wg * a.slots * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (size_t p = gl; p < P; p += NL, s++) {
+        const uint32_t o = (uint32_t)(p / h), i = (uint32_t)(p - (size_t)o * h);
+        const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+    }
+    // products of the other lanes' values (prefix x suffix) and of all of them
+    Fp pr = acc, sf = acc;
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fp u = fp_shfl_up(pr, d);
+        if (lane >= d) pr = fp_mul(pr, u);
+        const Fp w = fp_shfl_down(sf, d);
+        if (lane + d < 32) sf = fp_mul(sf, w);
+    }
+    const Fp total = fp_shfl(pr, 31);
+    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
+    if (lane == 0) pre_x = fp_one();
+    if (lane == 31) suf_x = fp_one();
+    st_vec(&a.others[gl], fp_mul(pre_x, suf_x));
+    if (lane == 0) st_vec(&a.tot[wg], total);
+}
+
+// Inverts n warp products, 32 per warp with one inversion.
+__global__ void __launch_bounds__(128) k_flat_invert(const Fp *__restrict__ tot, Fp *totinv, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const Fp r = warp_batch_inverse_fp(t < n ? ld_vec(&tot[t]) : fp_one());
+    if (t < n) st_vec(&totinv[t], r);
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint32_t m) {
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const uint32_t h = m >> 1, m_next = (m + 1) >> 1;
+    const size_t P = (size_t)a.n_lists * h;
+    const uint32_t *pre = a.pre + wg * a.slots * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        const size_t p = gl + (size_t)t * NL;
+        const uint32_t o = (uint32_t)(p / h), i = (uint32_t)(p - (size_t)o * h);
+        const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, den);
+        st_vec(&a.dst[(size_t)o * m_next + i], pair_result(x, y, kind, inv_den));
+    }
+    if (m & 1u)
+        for (size_t o = gl; o < (size_t)a.n_lists; o += NL)
+            st_vec(&a.dst[o * m_next + h], flat_load<FIRST>(a, (uint32_t)o, m - 1, m));
+}
+
+__global__ void __launch_bounds__(128) k_flat_finish(const G1A *__restrict__ sums, G1J *points, int n) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o < n) st_vec(&points[o], g1_from_affine(ld_vec(&sums[o])));
+}
+
+int flat_blocks() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 2;
+}
+
+// Working set of the grid-wide rounds for cap blobs and window c.
+FlatSizes flat_sizes(int cap, int c) {
+    FlatSizes z;
+    const size_t D = (256 + c - 1) / c, L = (size_t)kCellElems * D, lists = (size_t)cap * kCells;
+    z.blocks = flat_blocks();
+    const size_t lanes = (size_t)z.blocks * kFlatThreads;
+    z.dig = lists * L;
+    z.buf0 = lists * ((L + 1) / 2);
+    z.buf1 = lists * ((L + 3) / 4);
+    z.slots = (lists * (L / 2) + lanes - 1) / lanes;
+    z.pre_words = lanes / 32 * z.slots * 384;
+    z.lanes = lanes;
+    return z;
+}
+
+// Phase A of plan 3 for n blobs: digits, tree rounds, Jacobian outputs in
+// w.points.  Returns the number of kernels launched.
+int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
+    const int c = w.comb_c, D = (256 + c - 1) / c, L = kCellElems * D;
+    const int lists = n * kCells;
+    FlatArgs a;
+    a.dig = w.flat_dig;
+    a.comb = w.comb;
+    a.H = 1 << (c - 1);
+    a.L = L;
+    a.per_j = (size_t)L * a.H;
+    a.pre = w.flat_pre;
+    a.others = w.flat_others;
+    a.tot = w.flat_tot;
+    a.totinv = w.flat_totinv;
+    a.slots = w.flat_slots;
+    a.n_lists = lists;
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    int launched = 0;
+    k_flat_digits<<<(lists * kCellElems + 127) / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
+    launched++;
+    uint32_t m = (uint32_t)L;
+    bool first = true;
+    G1A *bufs[2] = {w.flat_buf[0], w.flat_buf[1]};
+    int out = 0;
+    const G1A *cur = nullptr;
+    while (m > 1) {
+        a.src = cur;
+        a.dst = bufs[out];
+        if (first) k_flat_pass1<true><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        if (first) k_flat_pass2<true><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        launched += 3;
+        cur = bufs[out];
+        out ^= 1;
+        m = (m + 1) >> 1;
+        first = false;
+    }
+    k_flat_finish<<<(lists + 127) / 128, 128, 0, s>>>(cur, w.points, lists);
+    return launched + 1;
+}
+
+// Bases of the digit table: B[j][i][k] = 2^(c k) X[j][i], from the position
+// table entry 2^(8 floor(ck / 8)) X[j][i] and (ck mod 8) doublings.
+__global__ void __launch_bounds__(128) k_comb_bases(const G1A *__restrict__ pos, G1A *bases, int c, int D) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= kCells * kCellElems * D) return;
+    const int ji = idx / D, k = idx % D, bit = c * k;
+    G1J p = g1_from_affine(ld_vec(&pos[(size_t)ji * kDigits + (bit >> 3)]));
+    for (int r = 0; r < (bit & 7); r++) p = g1_dbl(p);
+    G1A a;
+    if (fp_is_zero(p.z)) {
+        a.x = fp_zero();
+        a.y = fp_zero();
+    } else {
+        const Fp zi = fp_inv_fast(p.z), z2 = fp_sqr(zi);
+        a.x = fp_mul(p.x, z2);
+        a.y = fp_mul(p.y, fp_mul(z2, zi));
+    }
+    st_vec(&bases[idx], a);
+}
+
+// Rows of the digit table, row[m - 1] = m B for m = 1..H (H a power of two),
+// built level by level: level L (L = 1, 2, 4, ..., H / 2) makes entries
+// L + 1..2L as (L + r) B = r B + L B for r = 1..L (r = L is a doubling).  The
+// additions of a level are independent, so one inversion per level serves all
+// of them for the warp's kCombRows rows: log2(H) inversions per row group
+// instead of one per table entry.
+constexpr int kCombRows = 8;
+constexpr int kCombBuildThreads = 128;
+
+__host__ __device__ inline size_t comb_build_pre_words(int H) { return ((size_t)kCombRows * (H / 2) / 32 + 1) * 384; }
+
+__global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__restrict__ bases, G1A *comb, int H,
+                                                                 int n_bases, uint32_t *pre_all) {
+    const int lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * (kCombBuildThreads / 32) + (threadIdx.x >> 5);
+    const int n_warps = gridDim.x * (kCombBuildThreads / 32);
+    uint32_t *pre = pre_all + (size_t)wid * comb_build_pre_words(H);
+    const int n_tasks = (n_bases + kCombRows - 1) / kCombRows;
+    for (int task = wid; task < n_tasks; task += n_warps) {
+        const int b0 = task * kCombRows;
+        const uint32_t nb = (uint32_t)min(kCombRows, n_bases - b0);
+        G1A *rows = comb + (size_t)b0 * H;
+        for (uint32_t r = lane; r < nb; r += 32) st_vec(&rows[(size_t)r * H], ld_vec(&bases[b0 + r]));
+        __syncwarp();
+        for (uint32_t L = 1; L < (uint32_t)H; L <<= 1) {
+            const uint32_t P = nb * L;
+            Fp acc = fp_one();
+            int s = 0;
+            for (uint32_t q = lane; q < P; q += 32, s++) {
+                const uint32_t rb = q / L, r = q - rb * L + 1;
+                const G1A x = ld_vec(&rows[(size_t)rb * H + r - 1]), y = ld_vec(&rows[(size_t)rb * H + L - 1]);
+                wb_store_pre(pre, s, acc);
+                acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+            }
+            Fp inv = warp_batch_inverse_fp(acc);
+            for (int t = s - 1; t >= 0; t--) {
+                const uint32_t q = lane + (uint32_t)t * 32;
+                const uint32_t rb = q / L, r = q - rb * L + 1;
+                const G1A x = ld_vec(&rows[(size_t)rb * H + r - 1]), y = ld_vec(&rows[(size_t)rb * H + L - 1]);
+                const int kind = pair_kind(x, y);
+                const Fp den = pair_denominator(x, y, kind);
+                const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+                inv = fp_mul(inv, den);
+                st_vec(&rows[(size_t)rb * H + L + r - 1], pair_result(x, y, kind, inv_den));
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Digit table for window c (D = ceil(256 / c) windows) into comb; scratch holds
+// the bases (128 * 64 * D points) followed by the build's prefix products
+// (comb_build_scratch_bytes).
+int comb_build_blocks() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 4;
+}
+
+size_t comb_build_scratch_bytes(int c) {
+    const int D = (256 + c - 1) / c, H = 1 << (c - 1);
+    return (size_t)kCells * kCellElems * D * sizeof(G1A) +
+           (size_t)comb_build_blocks() * (kCombBuildThreads / 32) * comb_build_pre_words(H) * 4;
+}
+
+cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int c, cudaStream_t s) {
+    const int D = (256 + c - 1) / c, n_bases = kCells * kCellElems * D;
+    G1A *bases = reinterpret_cast<G1A *>(scratch);
+    uint32_t *pre = reinterpret_cast<uint32_t *>(bases + n_bases);
+    k_comb_bases<<<(n_bases + 127) / 128, 128, 0, s>>>(t.pos, bases, c, D);
+    k_comb_table<<<comb_build_blocks(), kCombBuildThreads, 0, s>>>(bases, comb, 1 << (c - 1), n_bases, pre);
+    count_launches(2);
+    return cudaGetLastError();
 }
 
 // k_reduce over affine bucket sums: s += B_k is a mixed addition.
@@ -661,9 +983,12 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
     mark();
     // plan: 0 serial Jacobian buckets + serial reduction; 1 batch-affine buckets +
-    // binary-split reduction; 2 batch-affine buckets + serial reduction
+    // binary-split reduction; 2 batch-affine buckets + serial reduction; 3 phase A
+    // over the digit table (no reduction), phase B as plan 1
     const bool affine = w.plan != 0 && w.ba_blocks > 0;
-    const bool hier = w.plan == 1;
+    const bool comb = w.plan == 3 && w.comb != nullptr && w.flat_dig != nullptr && w.ba_blocks > 0;
+    const bool hier = w.plan == 1 || comb;
+    int launched = 10;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
     auto reduce = [&]() {
         if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
@@ -672,7 +997,10 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
                                                                                        w.red_scratch, n_out);
         else k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     };
-    if (affine) {
+    if (comb) {
+        cudaMemsetAsync(w.task_ctr, 0, 2 * sizeof(uint32_t), s);
+        launched += launch_phase_a_flat(w, n, s) - 2; // no phase-A bucket kernel, no reduction
+    } else if (affine) {
         cudaMemsetAsync(w.task_ctr, 0, 2 * sizeof(uint32_t), s);
         k_phase_a_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.scalars, t.pos, w.bucket_aff, w.ba_scratch,
                                                                n_out, w.task_ctr);
@@ -680,7 +1008,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
     }
     mark();
-    reduce();
+    if (!comb) reduce();
     mark();
     k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
     mark();
@@ -689,7 +1017,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     mark();
     if (affine) {
-        k_phase_b_affine<<<ba_grid, kBAThreads, kBASmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
+        k_phase_b_affine<<<ba_grid, kBAThreads, kPhaseBSmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                               t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
                                                               w.ba_scratch, n_out, w.task_ctr + 1);
     } else {
@@ -702,7 +1030,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
     mark();
-    count_launches(10);
+    count_launches(launched);
     return cudaGetLastError();
 }
 
@@ -714,7 +1042,7 @@ cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cuda
 int batch_affine_blocks_per_sm() {
     int a = 0, b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_phase_a_affine, kBAThreads, kBASmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_phase_b_affine, kBAThreads, kBASmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_phase_b_affine, kBAThreads, kPhaseBSmem);
     return std::max(1, std::min(a, b));
 }
 
@@ -728,7 +1056,7 @@ cudaError_t configure_proof_kernels() {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBASmem);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_phase_b_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBASmem);
+    return cudaFuncSetAttribute(k_phase_b_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseBSmem);
 }
 
 } // namespace vkzg

@@ -19,7 +19,9 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -48,6 +50,25 @@ static const char *kProofStageNames[kProofStages] = {"blob_to_coeffs", "circulan
                                                      "reduce_b",       "finish"};
 static const char *kRecoverStageNames[kRecoverStages] = {"recover_prep", "recover_main"};
 
+// Plan 3's digit table (proof_kernels.cu, k_phase_a_comb): tens of GB, built
+// on first use and shared by every prover of the process on the same device
+// with the same setup tables; freed with the last of them.
+struct CombTable {
+    int device = 0;
+    int c = 0;
+    G1A *d = nullptr;
+    size_t bytes = 0;
+    double build_ms = 0.0;
+    ~CombTable() {
+        if (!d) return;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        cudaFree(d);
+        cudaSetDevice(cur);
+    }
+};
+
 struct vkzg_prover {
     int device = 0;
     std::string name;
@@ -73,7 +94,10 @@ struct vkzg_prover {
     // autotuner: plan per power-of-two chunk size (see choose_plan)
     int plan_forced = -1;
     std::map<uint32_t, int> plan_of;
-    std::map<uint32_t, std::array<double, 3>> plan_ms;
+    std::map<uint32_t, std::array<double, 4>> plan_ms;
+    std::string tables_id;            // identity of the setup tables, for sharing the digit table
+    std::shared_ptr<CombTable> comb;  // plan 3's digit table, once built
+    bool comb_failed = false;
     std::string tune_cache;
     cudaEvent_t ev_tune[2] = {nullptr, nullptr};
 
@@ -226,8 +250,10 @@ vkzg_result load_tables_file(const char *path, HostTables &h) {
     if (!f) return VKZG_ERR_IO;
     vkzg_result rc = VKZG_ERR_SETUP;
     uint32_t hdr[4];
-    if (read_exact(f, hdr, 16) && hdr[0] == 0x475A4B56u && hdr[1] == 1u && hdr[2] <= (1u << 20) &&
-        hdr[3] <= (1u << 20)) {
+    // each half holds at most one item per (tap, digit): 64 x 32 (the phase-B
+    // kernels size their shared memory and scratch by that bound)
+    if (read_exact(f, hdr, 16) && hdr[0] == 0x475A4B56u && hdr[1] == 1u && hdr[2] <= (uint32_t)(kHalf * kDigits) &&
+        hdr[3] <= (uint32_t)(kHalf * kDigits)) {
         h.pos.resize(kPositionPoints * sizeof(G1A));
         h.roots_fwd.resize(kExtElems);
         h.roots_inv.resize(kExtElems);
@@ -359,7 +385,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     // plan override (0 serial Jacobian, 1 batch-affine + binary split, 2 batch-affine + serial)
     if (const char *plan = getenv("VKZG_PLAN")) {
         const int v = atoi(plan);
-        if (v >= 0 && v < 3) p->plan_forced = v;
+        if (v >= 0 && v < 4) p->plan_forced = v;
     }
     if (const char *cache = getenv("VKZG_TUNE_CACHE")) p->tune_cache = cache;
     load_tune_cache(p);
@@ -376,6 +402,21 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
 // -------------------------------------------------------------- lifecycle
 
 static vkzg_result write_tables_file(const char *out_path, const HostTables &h, const G1A *d_pos);
+
+// FNV-1a over 8-byte words (plus the tail), as hex: identifies setup tables.
+static std::string hash_hex(const uint8_t *d, size_t n) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        memcpy(&w, d + i, 8);
+        h = (h ^ w) * 0x100000001b3ull;
+    }
+    for (; i < n; i++) h = (h ^ d[i]) * 0x100000001b3ull;
+    char buf[24];
+    snprintf(buf, sizeof buf, "%016llx", (unsigned long long)h);
+    return buf;
+}
 
 vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
     if (!out) return VKZG_ERR_BADARGS;
@@ -426,6 +467,7 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
         rc = load_tables_file(f.c_str(), h);
         if (rc == VKZG_OK) {
             p->tables_source = "file:" + f;
+            p->tables_id = "pos:" + hash_hex(h.pos.data(), h.pos.size());
             break;
         }
         if (rc == VKZG_ERR_SETUP) seen_malformed = true;
@@ -445,6 +487,7 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
             if (rc == VKZG_OK && !p->alloc(p->t.pos, kPositionPoints)) rc = VKZG_ERR_MALLOC;
             if (rc == VKZG_OK) rc = generate_position_table(p, setup);
             if (rc == VKZG_OK) p->tables_source = "generated:" + setup_path;
+            p->tables_id = "setup:" + hash_hex(setup.data(), setup.size());
             // setup cache: the next prover loads the file instead of generating
             if (rc == VKZG_OK && cache && *cache && cudaStreamSynchronize(p->stream) == cudaSuccess &&
                 write_tables_file(cache, h, p->t.pos) == VKZG_OK)
@@ -484,7 +527,106 @@ void collect_times(const cudaEvent_t *ev, int stages, double *dst) {
 // faster depends on the chunk size.  The first chunk of each power-of-two size
 // class is timed under every plan on the stream and the fastest is kept.
 
-constexpr int kPlans = 3;
+constexpr int kPlans = 4;
+
+// plan 3's table and buffers, from the prover's working set into a copy of it
+void take_comb(ProofWork &w, const ProofWork &from) {
+    w.comb = from.comb;
+    w.comb_c = from.comb_c;
+    w.flat_dig = from.flat_dig;
+    w.flat_buf[0] = from.flat_buf[0];
+    w.flat_buf[1] = from.flat_buf[1];
+    w.flat_pre = from.flat_pre;
+    w.flat_others = from.flat_others;
+    w.flat_tot = from.flat_tot;
+    w.flat_totinv = from.flat_totinv;
+    w.flat_slots = from.flat_slots;
+    w.flat_blocks = from.flat_blocks;
+}
+constexpr uint32_t kCombMinBlobs = 16; // smaller chunks never pay for the digit table
+
+// ------------------------------------------------------------ digit table
+std::mutex g_comb_mu;
+std::map<std::string, std::weak_ptr<CombTable>> g_comb;
+
+// Window width of the digit table: $VKZG_COMB_BITS (0 disables it; else 10..14), default 12.
+int comb_bits_wanted() {
+    if (const char *e = getenv("VKZG_COMB_BITS")) {
+        const int c = atoi(e);
+        return c <= 0 ? 0 : std::min(14, std::max(10, c));
+    }
+    return 12;
+}
+
+size_t comb_bytes(int c) {
+    const size_t D = (256 + c - 1) / c;
+    return (size_t)kCells * kCellElems * D * ((size_t)1 << (c - 1)) * sizeof(G1A);
+}
+
+// Builds or shares the digit table; the window shrinks (down to 10 bits) until
+// the table fits in free device memory with 4 GB to spare.
+bool ensure_comb(vkzg_prover *p) {
+    if (p->comb) return true;
+    if (p->comb_failed) return false;
+    int c = comb_bits_wanted();
+    std::lock_guard<std::mutex> lk(g_comb_mu);
+    for (; c >= 10 && !p->comb; c--) {
+        const std::string key = std::to_string(p->device) + "|" + std::to_string(c) + "|" + p->tables_id;
+        auto it = g_comb.find(key);
+        if (it != g_comb.end()) {
+            if (auto sp = it->second.lock()) {
+                p->comb = sp;
+                break;
+            }
+        }
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) break;
+        const size_t bytes = comb_bytes(c);
+        if (free_b < bytes + comb_build_scratch_bytes(c) + (4ull << 30)) continue;
+        auto t = std::make_shared<CombTable>();
+        t->device = p->device;
+        t->c = c;
+        t->bytes = bytes;
+        if (cudaMalloc(&t->d, bytes) != cudaSuccess) {
+            t->d = nullptr;
+            cudaGetLastError();
+            continue;
+        }
+        void *scratch = nullptr;
+        if (cudaMalloc(&scratch, comb_build_scratch_bytes(c)) != cudaSuccess) {
+            cudaGetLastError();
+            break;
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        cudaError_t e = launch_comb_table(p->t, t->d, scratch, c, p->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+        cudaFree(scratch);
+        if (e != cudaSuccess) break;
+        t->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        g_comb[key] = t;
+        p->comb = t;
+    }
+    if (!p->comb) {
+        p->comb_failed = true;
+        return false;
+    }
+    // this prover's working set for the grid-wide rounds
+    const FlatSizes z = flat_sizes((int)p->cap, p->comb->c);
+    ProofWork &w = p->pw;
+    if (!p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) || !p->alloc(w.flat_buf[1], z.buf1) ||
+        !p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
+        !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32)) {
+        cudaGetLastError();
+        p->comb.reset();
+        p->comb_failed = true;
+        return false;
+    }
+    w.flat_slots = z.slots;
+    w.flat_blocks = z.blocks;
+    w.comb = p->comb->d;
+    w.comb_c = p->comb->c;
+    return true;
+}
 
 uint32_t size_class(uint32_t n) {
     uint32_t c = 1;
@@ -520,9 +662,14 @@ void load_tune_cache(vkzg_prover *p) {
 // outputs left in w are those of the last run (identical for all plans).
 vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
     cudaStream_t s = p->stream;
-    std::array<double, 3> ms{};
+    std::array<double, kPlans> ms{};
     for (int plan = 0; plan < kPlans; plan++) {
+        if (plan == 3 && (n < kCombMinBlobs || !ensure_comb(p))) {
+            ms[plan] = 1e30; // not available at this size
+            continue;
+        }
         w.plan = plan;
+        take_comb(w, p->pw);
         double best = 1e30;
         for (int rep = 0; rep < 2; rep++) { // the first run of a plan also pays its first-launch costs
             CK(cudaEventRecord(p->ev_tune[0], s));
@@ -548,7 +695,14 @@ int planned(const vkzg_prover *p, uint32_t n) {
     if (p->plan_forced >= 0) return p->plan_forced;
     auto it = p->plan_of.find(size_class(n));
     if (it != p->plan_of.end()) return it->second;
-    return n >= 128 ? 1 : (n >= 8 ? 2 : 0);
+    if (n >= 128) return p->comb ? 3 : 1;
+    return n >= 8 ? 2 : 0;
+}
+
+// planned(), with the digit table made ready for plan 3 (plan 1 without it)
+int plan_for(vkzg_prover *p, uint32_t n) {
+    const int plan = planned(p, n);
+    return plan == 3 && !ensure_comb(p) ? 1 : plan;
 }
 
 bool tuned(const vkzg_prover *p, uint32_t n) {
@@ -563,7 +717,7 @@ vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, 
         const vkzg_result rc = tune_chunk(p, p->pw, n);
         if (rc != VKZG_OK) return rc;
     }
-    p->pw.plan = planned(p, n);
+    p->pw.plan = plan_for(p, n);
     CK(launch_proofs_timed(p->t, p->pw, (int)n, s, p->timing ? p->ev : nullptr));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -735,7 +889,8 @@ vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, c
         w.proofs = d_proofs + done * kCells * kProofBytes;
         w.err = d_err + done;
         CK(cudaMemsetAsync(w.err, 0, n * sizeof(uint32_t), p->stream));
-        w.plan = planned(p, n);
+        w.plan = plan_for(p, n);
+        take_comb(w, p->pw);
         CK(launch_proofs_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev : nullptr));
         done += n;
     }
@@ -811,7 +966,7 @@ vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const u
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
     CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->rw.scratch, p->pw.err, (int)n, s));
-    p->pw.plan = planned(p, n);
+    p->pw.plan = plan_for(p, n);
     if (proofs) CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -881,6 +1036,13 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
 
 uint64_t vkzg_b200_kernel_launches(void) { return launches_total(); }
 
+int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes) {
+    if (!p || !p->comb) return 0;
+    if (build_ms) *build_ms = p->comb->build_ms;
+    if (bytes) *bytes = p->comb->bytes;
+    return p->comb->c;
+}
+
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class_out, int *plan_out, double *ms_out, int cap) {
     if (!p) return 0;
     int i = 0;
@@ -890,7 +1052,10 @@ int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class_out, int *
             if (plan_out) plan_out[i] = kv.second;
             auto it = p->plan_ms.find(kv.first);
             if (ms_out)
-                for (int q = 0; q < 3; q++) ms_out[3 * i + q] = it != p->plan_ms.end() ? it->second[q] : -1.0;
+                for (int q = 0; q < kPlans; q++) {
+                    const double v = it != p->plan_ms.end() ? it->second[q] : -1.0;
+                    ms_out[kPlans * i + q] = v >= 1e29 ? -1.0 : v;
+                }
         }
         i++;
     }
@@ -926,7 +1091,7 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
         CK(launch_recover_timed(p->t, p->rw, (int)n, s, nullptr));
         CK(cudaMemcpy2DAsync(p->pw.blobs, kBlobBytes, p->rw.out, ext_bytes, kBlobBytes, n, cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
-        p->pw.plan = planned(p, n);
+        p->pw.plan = plan_for(p, n);
         CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
         CK(cudaMemcpyAsync(cells_out + done * ext_bytes, p->rw.out, (size_t)n * ext_bytes, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(proofs_out + done * kCells * kProofBytes, p->pw.proofs, (size_t)n * kCells * kProofBytes,
