@@ -111,3 +111,25 @@ def test_recovery_too_many_missing(synthetic_prover):
     present[1, :65] = 0
     out = np.zeros(2 * 262144, np.uint8)
     assert synthetic_prover.recover_cells_raw(out, cells, present, 2) == vkzg_b200.ERR_BADARGS
+
+
+def test_graph_replay_matches_direct_launches(monkeypatch):
+    """Chunks replayed from the captured CUDA graph give the same bytes as the
+    same pipeline launched kernel by kernel, and count the same launches."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    blobs = np.concatenate([random_blobs(10, 505), adversarial_blobs()])
+    outs, counts = [], []
+    for graphs in ("0", "1"):
+        monkeypatch.setenv("VKZG_GRAPHS", graphs)
+        with vkzg_b200.Prover(max_batch_size=len(blobs)) as p:
+            out = np.zeros(len(blobs) * 6144, np.uint8)
+            assert p.compute_proofs_raw(out, blobs, len(blobs)) == 0  # first call: tuning, capture
+            for _ in range(2):
+                before = vkzg_b200.kernel_launches()
+                out2 = np.zeros_like(out)
+                assert p.compute_proofs_raw(out2, blobs, len(blobs)) == 0
+                counts.append(vkzg_b200.kernel_launches() - before)
+                assert np.array_equal(out, out2)
+            outs.append(out)
+    assert np.array_equal(outs[0], outs[1])
+    assert counts[0] == counts[1] == counts[2] == counts[3] > 0

@@ -24,6 +24,22 @@ constexpr size_t kProofBytes = 48;
 constexpr size_t kCellBytes = 2048;
 constexpr size_t kPositionPoints = (size_t)kCells * kCellElems * kDigits; // 262144
 
+// Round structure of plan 3's phase B (see build_flatb_plan): per round r and
+// half h (0: plus taps, 1: minus taps), each bucket's list length, element
+// offsets, pair offsets and odd buckets, identical for every output of a half.
+constexpr int kFBMaxRounds = 12;
+struct FlatBPlan {
+    int rounds;
+    uint32_t stride[kFBMaxRounds + 1];           // elements per output in round r's buffer
+    uint32_t pairs[kFBMaxRounds][2];             // pairs per output
+    uint32_t n_odd[kFBMaxRounds][2];
+    uint32_t cnt[kFBMaxRounds + 1][2][kBuckets];
+    uint32_t base[kFBMaxRounds + 1][2][kBuckets + 1];
+    uint32_t pscan[kFBMaxRounds][2][kBuckets + 1];
+    uint8_t odd[kFBMaxRounds][2][kBuckets];
+};
+bool build_flatb_plan(const uint32_t offsets[2][kBuckets + 1], FlatBPlan &plan);
+
 // Setup-derived device tables (immutable once built).
 struct DeviceTables {
     G1A *pos = nullptr;             // [128 j][64 i][32 d] affine, 2^(8d) X[j][i]
@@ -35,6 +51,9 @@ struct DeviceTables {
     Fr *shift_fwd = nullptr;        // 7^k / 8192                (recovery)
     Fr *shift_inv = nullptr;        // 7^-k / 8192 / R           (recovery; output lands canonical)
     Fr *inv_blob_r2 = nullptr;      // [1] (1/4096) in Montgomery form
+    FlatBPlan *fb_plan = nullptr;   // plan 3's phase-B rounds
+    int fb_rounds = 0;              // 0: plan 3 uses the per-warp phase B
+    uint32_t fb_stride[2] = {0, 0}; // elements per output after rounds 1 and 2
 };
 
 // Per-batch working set for proofs, capacity `cap` blobs.
@@ -63,6 +82,7 @@ struct ProofWork {
     Fp *flat_others = nullptr, *flat_tot = nullptr, *flat_totinv = nullptr;
     size_t flat_slots = 0;
     int flat_blocks = 0;
+    G1A *flatb_buf[2] = {nullptr, nullptr}; // phase B's round buffers
     int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
     G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
 };

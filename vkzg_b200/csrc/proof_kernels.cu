@@ -20,6 +20,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 namespace vkzg {
@@ -660,7 +661,8 @@ FlatSizes flat_sizes(int cap, int c) {
     z.dig = lists * L;
     z.buf0 = lists * ((L + 1) / 2);
     z.buf1 = lists * ((L + 3) / 4);
-    z.slots = (lists * (L / 2) + lanes - 1) / lanes;
+    // phase A: L / 2 pairs per list; phase B: at most 1024 pairs per output (2048 tap items)
+    z.slots = (lists * std::max<size_t>(L / 2, 1024) + lanes - 1) / lanes;
     z.pre_words = lanes / 32 * z.slots * 384;
     z.lanes = lanes;
     return z;
@@ -707,6 +709,263 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
         first = false;
     }
     k_flat_finish<<<(lists + 127) / 128, 128, 0, s>>>(cur, w.points, lists);
+    return launched + 1;
+}
+
+// Plan 3's phase B as grid-wide rounds.  The bucket lists of an output are the
+// tap items of its half (plus: a < 64, minus: a >= 64), so every output of a
+// half has the same bucket lengths in every round: the round structure is a
+// setup constant (FlatBPlan, built on the host) and the pairs of all outputs
+// are dealt to all lanes as in phase A.  Round r keeps bucket k of output o at
+// buf[o * stride[r] + base[r][half][k] ..]; the last round leaves one point or
+// none per bucket, scattered into bucket_aff for the reduction.
+bool build_flatb_plan(const uint32_t offsets[2][kBuckets + 1], FlatBPlan &pl) {
+    memset(&pl, 0, sizeof pl);
+    uint32_t cnt[2][kBuckets];
+    for (int h = 0; h < 2; h++)
+        for (int k = 0; k < kBuckets; k++) cnt[h][k] = offsets[h][k + 1] - offsets[h][k];
+    int r = 0;
+    for (;; r++) {
+        if (r > kFBMaxRounds) return false;
+        bool more = false;
+        uint32_t stride = 0;
+        for (int h = 0; h < 2; h++) {
+            uint32_t b = 0, ps = 0, no = 0;
+            for (int k = 0; k < kBuckets; k++) {
+                pl.cnt[r][h][k] = cnt[h][k];
+                pl.base[r][h][k] = b;
+                b += cnt[h][k];
+                more |= cnt[h][k] > 1;
+                if (r < kFBMaxRounds) {
+                    pl.pscan[r][h][k] = ps;
+                    ps += cnt[h][k] >> 1;
+                    if (cnt[h][k] & 1u) pl.odd[r][h][no++] = (uint8_t)k;
+                }
+            }
+            pl.base[r][h][kBuckets] = b;
+            stride = std::max(stride, b);
+            if (r < kFBMaxRounds) {
+                pl.pscan[r][h][kBuckets] = ps;
+                pl.pairs[r][h] = ps;
+                pl.n_odd[r][h] = no;
+            }
+        }
+        pl.stride[r] = stride;
+        if (!more) break;
+        for (int h = 0; h < 2; h++)
+            for (int k = 0; k < kBuckets; k++) cnt[h][k] = (cnt[h][k] + 1) >> 1;
+    }
+    pl.rounds = r;
+    return true;
+}
+
+struct FlatBArgs {
+    const FlatBPlan *plan;
+    const G1A *ladder_aff;
+    const uint32_t *items[2];
+    const uint32_t *offsets[2];
+    const G1A *src;
+    G1A *dst;
+    uint32_t *pre;
+    Fp *others, *tot, *totinv;
+    size_t slots;
+    int n_blobs;
+};
+
+// shared copy of one round's plan (and, in round 0, the tap items)
+struct FlatBRound {
+    uint32_t pscan[2][kBuckets + 1];
+    uint32_t base[2][kBuckets + 1];
+    uint32_t base_next[2][kBuckets + 1];
+    uint32_t cnt[2][kBuckets];
+    uint32_t stride, stride_next, pairs[2];
+};
+constexpr size_t kFlatBSmem = sizeof(FlatBRound) + (2 * kTapItemsMax + 2 * (kBuckets + 1)) * sizeof(uint32_t);
+
+template <bool FIRST>
+__device__ void flatb_stage(const FlatBArgs &a, int r, FlatBRound &sr, uint32_t *items, uint32_t *offs) {
+    const FlatBPlan &pl = *a.plan;
+    for (int x = threadIdx.x; x < 2 * (kBuckets + 1); x += blockDim.x) {
+        const int h = x / (kBuckets + 1), k = x % (kBuckets + 1);
+        sr.pscan[h][k] = pl.pscan[r][h][k];
+        sr.base[h][k] = pl.base[r][h][k];
+        sr.base_next[h][k] = pl.base[r + 1][h][k];
+        if (k < kBuckets) sr.cnt[h][k] = pl.cnt[r][h][k];
+        if (FIRST) offs[x] = __ldg(&a.offsets[h][k]);
+    }
+    if (threadIdx.x == 0) {
+        sr.stride = pl.stride[r];
+        sr.stride_next = pl.stride[r + 1];
+        sr.pairs[0] = pl.pairs[r][0];
+        sr.pairs[1] = pl.pairs[r][1];
+    }
+    if (FIRST) {
+        __syncthreads();
+        for (int h = 0; h < 2; h++)
+            for (uint32_t k = threadIdx.x; k < offs[h * (kBuckets + 1) + kBuckets]; k += blockDim.x)
+                items[h * kTapItemsMax + k] = __ldg(&a.items[h][k]);
+    }
+    __syncthreads();
+}
+
+// element e of bucket k of output o (half h)
+template <bool FIRST>
+__device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
+                                          const uint32_t *offs, uint32_t o, int h, int k, uint32_t e) {
+    if (FIRST) {
+        const uint32_t packed = items[h * kTapItemsMax + offs[h * (kBuckets + 1) + k] + e];
+        const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
+        const uint32_t b = o / kCells, aa = o % kHalf;
+        G1A pt = ld_vec(&a.ladder_aff[((size_t)b * kCells + h * kHalf + ((aa - tap) & (kHalf - 1))) * kDigits + d]);
+        if (((packed >> 16) & 1u) != (h == 1 && tap > (int)aa)) pt.y = fp_neg(pt.y);
+        return pt;
+    }
+    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[h][k] + e]);
+}
+
+// pair p of the round -> output, half, bucket, index
+__device__ __forceinline__ void flatb_pair(const FlatBRound &sr, int n_blobs, size_t p, uint32_t &o, int &h, int &k,
+                                           uint32_t &i) {
+    const size_t p_plus = (size_t)n_blobs * kHalf * sr.pairs[0];
+    h = p < p_plus ? 0 : 1;
+    const size_t pp = h ? p - p_plus : p;
+    const uint32_t per = sr.pairs[h];
+    const uint32_t ol = (uint32_t)(pp / per), q = (uint32_t)(pp - (size_t)ol * per);
+    o = (ol / kHalf) * kCells + h * kHalf + ol % kHalf;
+    k = ba_bucket_of<kBuckets>(sr.pscan[h], q);
+    i = q - sr.pscan[h][k];
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, int r) {
+    extern __shared__ uint4 dyn_smem[];
+    FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
+    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
+    flatb_stage<FIRST>(a, r, sr, items, offs);
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const int lane = threadIdx.x & 31;
+    const size_t P = (size_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    uint32_t *pre = a.pre + wg * a.slots * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (size_t p = gl; p < P; p += NL, s++) {
+        uint32_t o, i;
+        int h, k;
+        flatb_pair(sr, a.n_blobs, p, o, h, k, i);
+        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i);
+        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i + 1);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+    }
+    Fp pr = acc, sf = acc;
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fp u = fp_shfl_up(pr, d);
+        if (lane >= d) pr = fp_mul(pr, u);
+        const Fp w = fp_shfl_down(sf, d);
+        if (lane + d < 32) sf = fp_mul(sf, w);
+    }
+    const Fp total = fp_shfl(pr, 31);
+    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
+    if (lane == 0) pre_x = fp_one();
+    if (lane == 31) suf_x = fp_one();
+    st_vec(&a.others[gl], fp_mul(pre_x, suf_x));
+    if (lane == 0) st_vec(&a.tot[wg], total);
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, int r) {
+    extern __shared__ uint4 dyn_smem[];
+    FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
+    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
+    flatb_stage<FIRST>(a, r, sr, items, offs);
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const size_t P = (size_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    const uint32_t *pre = a.pre + wg * a.slots * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        const size_t p = gl + (size_t)t * NL;
+        uint32_t o, i;
+        int h, k;
+        flatb_pair(sr, a.n_blobs, p, o, h, k, i);
+        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i);
+        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i + 1);
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, den);
+        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[h][k] + i], pair_result(x, y, kind, inv_den));
+    }
+    // odd last elements move up unchanged
+    const FlatBPlan &pl = *a.plan;
+    const size_t n_half = (size_t)a.n_blobs * kHalf;
+    const size_t odd_all = n_half * (pl.n_odd[r][0] + pl.n_odd[r][1]);
+    for (size_t x = gl; x < odd_all; x += NL) {
+        const size_t x_plus = n_half * pl.n_odd[r][0];
+        const int h = x < x_plus ? 0 : 1;
+        const size_t xx = h ? x - x_plus : x;
+        const uint32_t no = pl.n_odd[r][h];
+        const uint32_t ol = (uint32_t)(xx / no), j = (uint32_t)(xx - (size_t)ol * no);
+        const int k = pl.odd[r][h][j];
+        const uint32_t o = (ol / kHalf) * kCells + h * kHalf + ol % kHalf;
+        const uint32_t c = sr.cnt[h][k];
+        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[h][k] + (c >> 1)],
+               flatb_load<FIRST>(a, sr, items, offs, o, h, k, c - 1));
+    }
+}
+
+// bucket_aff[o][k] from the last round (infinity for empty buckets)
+__global__ void __launch_bounds__(128) k_flatb_finish(const FlatBPlan *__restrict__ plan, const G1A *__restrict__ last,
+                                                     G1A *bucket_aff, int n_out) {
+    const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= (size_t)n_out * kBuckets) return;
+    const uint32_t o = (uint32_t)(x / kBuckets), k = (uint32_t)(x % kBuckets);
+    const int h = (o % kCells) >= kHalf ? 1 : 0, R = plan->rounds;
+    G1A v;
+    if (plan->cnt[R][h][k]) {
+        v = ld_vec(&last[(size_t)o * plan->stride[R] + plan->base[R][h][k]]);
+    } else {
+        v.x = fp_zero();
+        v.y = fp_zero();
+    }
+    st_vec(&bucket_aff[x], v);
+}
+
+// Phase B of plan 3 into w.bucket_aff; returns the number of kernels launched.
+int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    FlatBArgs a;
+    a.plan = t.fb_plan;
+    a.ladder_aff = w.ladder_aff;
+    for (int h = 0; h < 2; h++) {
+        a.items[h] = t.tap_items[h];
+        a.offsets[h] = t.tap_offsets[h];
+    }
+    a.pre = w.flat_pre;
+    a.others = w.flat_others;
+    a.tot = w.flat_tot;
+    a.totinv = w.flat_totinv;
+    a.slots = w.flat_slots;
+    a.n_blobs = n;
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    G1A *bufs[2] = {w.flatb_buf[0], w.flatb_buf[1]};
+    const G1A *cur = nullptr;
+    int out = 0, launched = 0;
+    for (int r = 0; r < t.fb_rounds; r++) {
+        a.src = cur;
+        a.dst = bufs[out];
+        if (r == 0) k_flatb_pass1<true><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
+        else k_flatb_pass1<false><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
+        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        if (r == 0) k_flatb_pass2<true><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
+        else k_flatb_pass2<false><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
+        launched += 3;
+        cur = bufs[out];
+        out ^= 1;
+    }
+    k_flatb_finish<<<(n * kCells * kBuckets + 127) / 128, 128, 0, s>>>(t.fb_plan, cur, w.bucket_aff, n * kCells);
     return launched + 1;
 }
 
@@ -1016,7 +1275,9 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     mark();
-    if (affine) {
+    if (comb && t.fb_rounds > 0) {
+        launched += launch_phase_b_flat(t, w, n, s) - 1;
+    } else if (affine) {
         k_phase_b_affine<<<ba_grid, kBAThreads, kPhaseBSmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],
                                                               t.tap_items[1], t.tap_offsets[1], w.bucket_aff,
                                                               w.ba_scratch, n_out, w.task_ctr + 1);

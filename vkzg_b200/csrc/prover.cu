@@ -39,7 +39,11 @@ cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, in
                                  cudaEvent_t *ev);
 
 static std::atomic<uint64_t> g_launches{0};
-void count_launches(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+static thread_local uint64_t t_launches = 0; // this thread's share (graph captures count their launches by it)
+void count_launches(int k) {
+    g_launches.fetch_add((uint64_t)(int64_t)k, std::memory_order_relaxed);
+    t_launches += (uint64_t)(int64_t)k;
+}
 uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 } // namespace vkzg
 
@@ -98,11 +102,28 @@ struct vkzg_prover {
     std::string tables_id;            // identity of the setup tables, for sharing the digit table
     std::shared_ptr<CombTable> comb;  // plan 3's digit table, once built
     bool comb_failed = false;
+    // CUDA graphs of the proof pipeline per (chunk size, plan), see run_proofs
+    struct GraphRec {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    };
+    std::map<uint64_t, GraphRec> graphs;
+    bool use_graphs = true;
+    // recovery from host buffers runs in parts on these streams so that copies
+    // in, transforms and copies out of different parts overlap
+    static constexpr int kSides = 4;
+    cudaStream_t side[kSides] = {};
+    cudaEvent_t side_ev[kSides + 1] = {};
     std::string tune_cache;
     cudaEvent_t ev_tune[2] = {nullptr, nullptr};
 
     ~vkzg_prover() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+        for (auto &x : side)
+            if (x) cudaStreamDestroy(x);
+        for (auto &e : side_ev)
+            if (e) cudaEventDestroy(e);
         for (void *a : allocs) cudaFree(a);
         if (h_err) cudaFreeHost(h_err);
         for (auto &e : ev)
@@ -314,6 +335,17 @@ vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
     CK(cudaMemcpy(t.roots_fwd, h.roots_fwd.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(t.roots_inv, h.roots_inv.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(t.inv_blob_r2, &h.inv_blob, sizeof(Fr), cudaMemcpyHostToDevice));
+    // plan 3's phase-B round structure, from the tap offsets
+    {
+        std::unique_ptr<FlatBPlan> pl(new FlatBPlan);
+        if (build_flatb_plan(h.offsets, *pl) && pl->rounds > 0) {
+            if (!p->alloc(t.fb_plan, 1)) return VKZG_ERR_MALLOC;
+            CK(cudaMemcpy(t.fb_plan, pl.get(), sizeof(FlatBPlan), cudaMemcpyHostToDevice));
+            t.fb_rounds = pl->rounds;
+            t.fb_stride[0] = pl->stride[1];
+            t.fb_stride[1] = pl->rounds > 1 ? pl->stride[2] : 1;
+        }
+    }
     // recovery coset-shift tables (the reference's k_pow_seq, src/vkzg.cpp:757-774),
     // with 1/8192 folded in and, for the inverse, an extra 1/R (see recover_kernels.cu)
     std::vector<Fr> sf(kExtElems), si(kExtElems);
@@ -388,6 +420,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
         if (v >= 0 && v < 4) p->plan_forced = v;
     }
     if (const char *cache = getenv("VKZG_TUNE_CACHE")) p->tune_cache = cache;
+    if (const char *g = getenv("VKZG_GRAPHS")) p->use_graphs = atoi(g) != 0;
     load_tune_cache(p);
     w.ba_blocks = (int)p->sm_count * batch_affine_blocks_per_sm();
     if (!p->alloc(w.bucket_aff, B * kCells * kBuckets) ||
@@ -402,6 +435,14 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
 // -------------------------------------------------------------- lifecycle
 
 static vkzg_result write_tables_file(const char *out_path, const HostTables &h, const G1A *d_pos);
+
+static bool create_sides(vkzg_prover *p) {
+    for (auto &x : p->side)
+        if (cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) != cudaSuccess) return false;
+    for (auto &e : p->side_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+    return true;
+}
 
 // FNV-1a over 8-byte words (plus the tail), as hex: identifies setup tables.
 static std::string hash_hex(const uint8_t *d, size_t n) {
@@ -448,7 +489,8 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
         }
     if (cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreate(&p->ev_tune[0]) != cudaSuccess || cudaEventCreate(&p->ev_tune[1]) != cudaSuccess) {
+        cudaEventCreate(&p->ev_tune[0]) != cudaSuccess || cudaEventCreate(&p->ev_tune[1]) != cudaSuccess ||
+        !create_sides(p)) {
         delete p;
         return VKZG_ERR_GPU;
     }
@@ -542,6 +584,40 @@ void take_comb(ProofWork &w, const ProofWork &from) {
     w.flat_totinv = from.flat_totinv;
     w.flat_slots = from.flat_slots;
     w.flat_blocks = from.flat_blocks;
+    w.flatb_buf[0] = from.flatb_buf[0];
+    w.flatb_buf[1] = from.flatb_buf[1];
+}
+
+// The proof pipeline of one chunk on the prover's own working set (p->pw with
+// w.plan): 10 to ~45 launches, captured once per (chunk size, plan) into a CUDA
+// graph and replayed with one cudaGraphLaunch.  Launched directly while stage
+// timing is on, for sizes beyond the cache (kMaxGraphs), or when $VKZG_GRAPHS=0.
+constexpr size_t kMaxGraphs = 24;
+
+cudaError_t run_proofs(vkzg_prover *p, const ProofWork &w, uint32_t n) {
+    cudaStream_t s = p->stream;
+    const uint64_t key = ((uint64_t)n << 8) | (uint64_t)w.plan;
+    auto it = p->graphs.find(key);
+    if (p->timing || !p->use_graphs || (it == p->graphs.end() && p->graphs.size() >= kMaxGraphs))
+        return launch_proofs_timed(p->t, w, (int)n, s, p->timing ? p->ev : nullptr);
+    if (it == p->graphs.end()) {
+        const uint64_t before = t_launches;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        e = launch_proofs_timed(p->t, w, (int)n, s, nullptr);
+        const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+        const uint64_t k = t_launches - before;
+        count_launches(-(int)k); // captured, not run
+        if (e == cudaSuccess) e = e2;
+        cudaGraphExec_t ex = nullptr;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        it = p->graphs.emplace(key, vkzg_prover::GraphRec{ex, k}).first;
+    }
+    count_launches((int)it->second.launches);
+    return cudaGraphLaunch(it->second.exec, s);
 }
 constexpr uint32_t kCombMinBlobs = 16; // smaller chunks never pay for the digit table
 
@@ -615,7 +691,9 @@ bool ensure_comb(vkzg_prover *p) {
     ProofWork &w = p->pw;
     if (!p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) || !p->alloc(w.flat_buf[1], z.buf1) ||
         !p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
-        !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32)) {
+        !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
+        !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
+        !p->alloc(w.flatb_buf[1], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[1]))) {
         cudaGetLastError();
         p->comb.reset();
         p->comb_failed = true;
@@ -718,7 +796,7 @@ vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, 
         if (rc != VKZG_OK) return rc;
     }
     p->pw.plan = plan_for(p, n);
-    CK(launch_proofs_timed(p->t, p->pw, (int)n, s, p->timing ? p->ev : nullptr));
+    CK(run_proofs(p, p->pw, n));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (p->timing) collect_times(p->ev, kProofStages, p->last_proof_ms);
@@ -738,13 +816,41 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         if (miss > kCellElems) return VKZG_ERR_BADARGS;
     }
     cudaStream_t s = p->stream;
-    const size_t bytes = (size_t)n * kExtElems * 32;
-    CK(cudaMemcpyAsync(p->rw.cells, cells, bytes, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
-    CK(launch_recover_timed(p->t, p->rw, (int)n, s, p->timing ? p->ev_rec : nullptr));
-    CK(cudaMemcpyAsync(out, p->rw.out, bytes, cudaMemcpyDeviceToHost, s));
+    const size_t ext = (size_t)kExtElems * 32;
+    const uint32_t part = n >= 64 && p->side[0] ? (n + vkzg_prover::kSides - 1) / vkzg_prover::kSides : n;
+    if (p->timing || part == n) {
+        CK(cudaMemcpyAsync(p->rw.cells, cells, n * ext, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
+        CK(launch_recover_timed(p->t, p->rw, (int)n, s, p->timing ? p->ev_rec : nullptr));
+        CK(cudaMemcpyAsync(out, p->rw.out, n * ext, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (p->timing) collect_times(p->ev_rec, kRecoverStages, p->last_recover_ms);
+        return VKZG_OK;
+    }
+    // parts of the chunk on the side streams (after all earlier work of the prover's stream)
+    CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
+    for (int k = 0; k < vkzg_prover::kSides; k++) CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
+    for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
+        const uint32_t cnt = std::min(part, n - off);
+        cudaStream_t st = p->side[k % vkzg_prover::kSides];
+        RecoverWork w = p->rw;
+        w.cells += off * ext;
+        w.present += (size_t)off * kCells;
+        w.out += off * ext;
+        w.scratch += (size_t)off * kExtElems;
+        w.zv += (size_t)off * kCells;
+        w.inv_zc += (size_t)off * kCells;
+        w.err += off;
+        CK(cudaMemcpyAsync(w.cells, cells + off * ext, cnt * ext, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(w.present, present + (size_t)off * kCells, (size_t)cnt * kCells, cudaMemcpyHostToDevice, st));
+        CK(launch_recover_timed(p->t, w, (int)cnt, st, nullptr));
+        CK(cudaMemcpyAsync(out + off * ext, w.out, cnt * ext, cudaMemcpyDeviceToHost, st));
+    }
+    for (int k = 0; k < vkzg_prover::kSides; k++) {
+        CK(cudaEventRecord(p->side_ev[k], p->side[k]));
+        CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
+    }
     CK(cudaStreamSynchronize(s));
-    if (p->timing) collect_times(p->ev_rec, kRecoverStages, p->last_recover_ms);
     return VKZG_OK;
 }
 
@@ -882,16 +988,19 @@ vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, c
     cudaStream_t caller = (cudaStream_t)stream;
     vkzg_result rc = enter_stream(p, caller);
     if (rc != VKZG_OK) return rc;
+    // through the working set (two device copies, ~1 % of the chunk's time), so
+    // that the pipeline captured for this chunk size replays unchanged
+    cudaStream_t s = p->stream;
     for (size_t done = 0; done < num_blobs;) {
         const uint32_t n = (uint32_t)std::min<size_t>(p->cap, num_blobs - done);
-        ProofWork w = p->pw;
-        w.blobs = const_cast<uint8_t *>(d_blobs) + done * kBlobBytes;
-        w.proofs = d_proofs + done * kCells * kProofBytes;
-        w.err = d_err + done;
-        CK(cudaMemsetAsync(w.err, 0, n * sizeof(uint32_t), p->stream));
-        w.plan = plan_for(p, n);
-        take_comb(w, p->pw);
-        CK(launch_proofs_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev : nullptr));
+        CK(cudaMemcpyAsync(p->pw.blobs, d_blobs + done * kBlobBytes, (size_t)n * kBlobBytes, cudaMemcpyDeviceToDevice,
+                           s));
+        CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+        p->pw.plan = plan_for(p, n);
+        CK(run_proofs(p, p->pw, n));
+        CK(cudaMemcpyAsync(d_proofs + done * kCells * kProofBytes, p->pw.proofs, (size_t)n * kCells * kProofBytes,
+                           cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(d_err + done, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         done += n;
     }
     if (p->timing) p->pending_proof = true;
@@ -967,7 +1076,7 @@ vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const u
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
     CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->rw.scratch, p->pw.err, (int)n, s));
     p->pw.plan = plan_for(p, n);
-    if (proofs) CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
+    if (proofs) CK(run_proofs(p, p->pw, n));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (uint32_t b = 0; b < n; b++)
@@ -1092,7 +1201,7 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
         CK(cudaMemcpy2DAsync(p->pw.blobs, kBlobBytes, p->rw.out, ext_bytes, kBlobBytes, n, cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
         p->pw.plan = plan_for(p, n);
-        CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr));
+        CK(run_proofs(p, p->pw, n));
         CK(cudaMemcpyAsync(cells_out + done * ext_bytes, p->rw.out, (size_t)n * ext_bytes, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(proofs_out + done * kCells * kProofBytes, p->pw.proofs, (size_t)n * kCells * kProofBytes,
                            cudaMemcpyDeviceToHost, s));
