@@ -112,7 +112,9 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * (every signed c-bit digit multiple of every base, c = 12 by default: 35 GB
  * of HBM, built on first use and shared by the process's provers with the same
  * setup; $VKZG_COMB_BITS picks c in 10..14 or 0 to disable it; smaller c is used
- * when free memory is short), phase B as plan 1.  The first chunk of each
+ * when free memory is short) summed in grid-wide batch-affine rounds, phase B
+ * also in grid-wide rounds; 4 = phase A as plan 1, phase B as plan 3 (no digit
+ * table).  The first chunk of each
  * power-of-two size class is timed under all plans and the fastest is kept
  * (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
  * vkzg_b200_autotune tunes every size class up to max_blobs (0 = the prover's
@@ -122,7 +124,7 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * vkzg_b200_digit_table returns the digit table's window c (0 = none built),
  * its build time and size.
  */
-#define VKZG_B200_PLANS 4
+#define VKZG_B200_PLANS 5
 vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms, int cap);
 int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes);

@@ -81,18 +81,18 @@ R_MOD = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
 def random_blobs(n, seed):
     """n blobs of field elements uniform in [0, r), 32-byte big-endian (rejection-sampled)."""
     rng = np.random.default_rng(seed)
-    out = np.zeros((n, 4096, 32), np.uint8)
-    for b in range(n):
-        vals = []
-        while len(vals) < 4096:
-            raw = rng.integers(0, 256, size=(8192, 32), dtype=np.uint8)
-            raw[:, 0] &= 0x7F
-            for row in raw:
-                if int.from_bytes(row.tobytes(), "big") < R_MOD:
-                    vals.append(row)
-                    if len(vals) == 4096:
-                        break
-        out[b] = np.stack(vals)
+    r_be = np.frombuffer(R_MOD.to_bytes(32, "big"), np.uint8).astype(np.int16)
+    out = np.empty((n * 4096, 32), np.uint8)
+    filled = 0
+    while filled < out.shape[0]:
+        cand = rng.integers(0, 256, size=(max(1024, 2 * (out.shape[0] - filled)), 32), dtype=np.uint8)
+        cand[:, 0] &= 0x7F
+        diff = cand.astype(np.int16) - r_be
+        first = np.argmax(diff != 0, axis=1)
+        good = cand[diff[np.arange(len(cand)), first] < 0]
+        take = min(len(good), out.shape[0] - filled)
+        out[filled:filled + take] = good[:take]
+        filled += take
     return out.reshape(n, 131072)
 
 

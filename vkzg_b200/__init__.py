@@ -29,7 +29,7 @@ BYTES_PER_EXT_BLOB = CELL_PROOFS_PER_BLOB * BYTES_PER_CELL
 OK, ERR_BADARGS, ERR_MALLOC, ERR_IO, ERR_SETUP, ERR_GPU, ERR_INVALID_BLOB = range(7)
 
 # every symbol declared in include/vkzg.h and include/vkzg_b200.h
-PLANS = 4  # VKZG_B200_PLANS
+PLANS = 5  # VKZG_B200_PLANS
 
 EXPORTED_SYMBOLS = (
     "vkzg_error_string", "vkzg_options_default", "vkzg_prover_new", "vkzg_prover_free",

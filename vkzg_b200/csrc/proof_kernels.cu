@@ -1241,12 +1241,14 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
     mark();
-    // plan: 0 serial Jacobian buckets + serial reduction; 1 batch-affine buckets +
-    // binary-split reduction; 2 batch-affine buckets + serial reduction; 3 phase A
-    // over the digit table (no reduction), phase B as plan 1
+    // plan: 0 serial Jacobian buckets + serial reduction; 1 batch-affine buckets
+    // per warp + binary-split reduction; 2 as 1 with the serial reduction; 3 phase A
+    // over the digit table in grid-wide rounds (no reduction), phase B in grid-wide
+    // rounds + binary-split reduction; 4 phase A as 1, phase B as 3
     const bool affine = w.plan != 0 && w.ba_blocks > 0;
     const bool comb = w.plan == 3 && w.comb != nullptr && w.flat_dig != nullptr && w.ba_blocks > 0;
-    const bool hier = w.plan == 1 || comb;
+    const bool flatb = (w.plan == 3 || w.plan == 4) && w.flat_pre != nullptr && t.fb_rounds > 0 && w.ba_blocks > 0;
+    const bool hier = w.plan == 1 || w.plan == 3 || w.plan == 4;
     int launched = 10;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
     auto reduce = [&]() {
@@ -1275,7 +1277,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     mark();
-    if (comb && t.fb_rounds > 0) {
+    if (flatb) {
         launched += launch_phase_b_flat(t, w, n, s) - 1;
     } else if (affine) {
         k_phase_b_affine<<<ba_grid, kBAThreads, kPhaseBSmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],

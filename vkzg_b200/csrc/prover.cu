@@ -98,10 +98,10 @@ struct vkzg_prover {
     // autotuner: plan per power-of-two chunk size (see choose_plan)
     int plan_forced = -1;
     std::map<uint32_t, int> plan_of;
-    std::map<uint32_t, std::array<double, 4>> plan_ms;
+    std::map<uint32_t, std::array<double, 5>> plan_ms;
     std::string tables_id;            // identity of the setup tables, for sharing the digit table
     std::shared_ptr<CombTable> comb;  // plan 3's digit table, once built
-    bool comb_failed = false;
+    bool comb_failed = false, flat_failed = false;
     // CUDA graphs of the proof pipeline per (chunk size, plan), see run_proofs
     struct GraphRec {
         cudaGraphExec_t exec = nullptr;
@@ -417,7 +417,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     // plan override (0 serial Jacobian, 1 batch-affine + binary split, 2 batch-affine + serial)
     if (const char *plan = getenv("VKZG_PLAN")) {
         const int v = atoi(plan);
-        if (v >= 0 && v < 4) p->plan_forced = v;
+        if (v >= 0 && v < 5) p->plan_forced = v;
     }
     if (const char *cache = getenv("VKZG_TUNE_CACHE")) p->tune_cache = cache;
     if (const char *g = getenv("VKZG_GRAPHS")) p->use_graphs = atoi(g) != 0;
@@ -569,7 +569,7 @@ void collect_times(const cudaEvent_t *ev, int stages, double *dst) {
 // faster depends on the chunk size.  The first chunk of each power-of-two size
 // class is timed under every plan on the stream and the fastest is kept.
 
-constexpr int kPlans = 4;
+constexpr int kPlans = 5;
 
 // plan 3's table and buffers, from the prover's working set into a copy of it
 void take_comb(ProofWork &w, const ProofWork &from) {
@@ -639,6 +639,27 @@ size_t comb_bytes(int c) {
     return (size_t)kCells * kCellElems * D * ((size_t)1 << (c - 1)) * sizeof(G1A);
 }
 
+// The grid-wide rounds' shared working set (prefix products, per-lane and
+// per-warp products) and phase B's round buffers: plans 3 and 4.
+bool ensure_flat_b(vkzg_prover *p) {
+    ProofWork &w = p->pw;
+    if (w.flat_pre) return true;
+    if (p->flat_failed || p->t.fb_rounds == 0) return false;
+    const FlatSizes z = flat_sizes((int)p->cap, 10); // its slots cover every window and phase B
+    if (!p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
+        !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
+        !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
+        !p->alloc(w.flatb_buf[1], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[1]))) {
+        cudaGetLastError();
+        w.flat_pre = nullptr;
+        p->flat_failed = true;
+        return false;
+    }
+    w.flat_slots = z.slots;
+    w.flat_blocks = z.blocks;
+    return true;
+}
+
 // Builds or shares the digit table; the window shrinks (down to 10 bits) until
 // the table fits in free device memory with 4 GB to spare.
 bool ensure_comb(vkzg_prover *p) {
@@ -686,21 +707,17 @@ bool ensure_comb(vkzg_prover *p) {
         p->comb_failed = true;
         return false;
     }
-    // this prover's working set for the grid-wide rounds
+    // this prover's working set for the grid-wide phase-A rounds
     const FlatSizes z = flat_sizes((int)p->cap, p->comb->c);
     ProofWork &w = p->pw;
-    if (!p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) || !p->alloc(w.flat_buf[1], z.buf1) ||
-        !p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
-        !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
-        !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
-        !p->alloc(w.flatb_buf[1], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[1]))) {
+    if (!ensure_flat_b(p) || !p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) ||
+        !p->alloc(w.flat_buf[1], z.buf1)) {
         cudaGetLastError();
+        w.flat_dig = nullptr;
         p->comb.reset();
         p->comb_failed = true;
         return false;
     }
-    w.flat_slots = z.slots;
-    w.flat_blocks = z.blocks;
     w.comb = p->comb->d;
     w.comb_c = p->comb->c;
     return true;
@@ -742,8 +759,8 @@ vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
     cudaStream_t s = p->stream;
     std::array<double, kPlans> ms{};
     for (int plan = 0; plan < kPlans; plan++) {
-        if (plan == 3 && (n < kCombMinBlobs || !ensure_comb(p))) {
-            ms[plan] = 1e30; // not available at this size
+        if ((plan == 3 && (n < kCombMinBlobs || !ensure_comb(p))) || (plan == 4 && !ensure_flat_b(p))) {
+            ms[plan] = 1e30; // not available at this size or in this memory
             continue;
         }
         w.plan = plan;
@@ -773,14 +790,17 @@ int planned(const vkzg_prover *p, uint32_t n) {
     if (p->plan_forced >= 0) return p->plan_forced;
     auto it = p->plan_of.find(size_class(n));
     if (it != p->plan_of.end()) return it->second;
-    if (n >= 128) return p->comb ? 3 : 1;
+    if (n >= 128) return p->comb ? 3 : (p->pw.flat_pre ? 4 : 1);
     return n >= 8 ? 2 : 0;
 }
 
-// planned(), with the digit table made ready for plan 3 (plan 1 without it)
+// planned(), with the digit table or the grid-wide buffers made ready for plans
+// 3 and 4 (plan 1 without them)
 int plan_for(vkzg_prover *p, uint32_t n) {
     const int plan = planned(p, n);
-    return plan == 3 && !ensure_comb(p) ? 1 : plan;
+    if (plan == 3 && !ensure_comb(p)) return ensure_flat_b(p) ? 4 : 1;
+    if (plan == 4 && !ensure_flat_b(p)) return 1;
+    return plan;
 }
 
 bool tuned(const vkzg_prover *p, uint32_t n) {
