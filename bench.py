@@ -491,11 +491,32 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--profile-case", nargs="?", const="proofs", choices=["proofs", "recovery"],
+                    help="small untimed case for ncu captures")
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="per offered load; 0 skips serving")
     ap.add_argument("--serve-loads", default="0.3,0.6,0.9", help="offered loads as fractions of batched capacity")
     args = ap.parse_args()
 
+    if args.profile_case:
+        # a small fixed case for ncu captures: --steps calls on --blobs blobs
+        # (proof plan from $VKZG_PLAN), nothing timed
+        import numpy as np
+        import vkzg_b200
+        prover = vkzg_b200.Prover(max_batch_size=args.blobs)
+        if args.profile_case == "proofs":
+            blobs = make_blobs(args.blobs, 5, adversarial=False)
+            out = np.zeros(args.blobs * PROOFS, np.uint8)
+            for _ in range(args.steps):
+                assert prover.compute_proofs_raw(out, blobs, args.blobs) == 0
+        else:
+            cells, present = make_recovery(args.blobs, 6)
+            out = np.zeros(args.blobs * EXT, np.uint8)
+            for _ in range(args.steps):
+                assert prover.recover_cells_raw(out, cells, present, args.blobs) == 0
+        print(json.dumps({"profile_case": args.profile_case, "blobs": args.blobs, "steps": args.steps,
+                          "launches": vkzg_b200.kernel_launches()}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

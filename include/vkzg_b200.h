@@ -109,7 +109,7 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * k_bucket_reduce.comp); 1 = batch-affine bucket accumulation and a
  * binary-split batch-affine reduction; 2 = batch-affine accumulation with the
  * serial reduction; 3 = phase A as plain sums over a precomputed digit table
- * (every signed c-bit digit multiple of every base, c = 12 by default: 35 GB
+ * (every signed c-bit digit multiple of every base, c = 13 by default: 64 GB
  * of HBM, built on first use and shared by the process's provers with the same
  * setup; $VKZG_COMB_BITS picks c in 10..14 or 0 to disable it; smaller c is used
  * when free memory is short) summed in grid-wide batch-affine rounds, phase B
@@ -193,6 +193,17 @@ vkzg_result vkzg_b200_microbench(int which, double *result);
  */
 vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, const uint32_t *bucket_of, size_t n,
                                            uint8_t *sums_xy);
+
+/*
+ * Sums n_lists lists of m affine points each (points_xy: n_lists * m x 96
+ * bytes, list o first; all zero = infinity) with the grid-wide batch-affine
+ * tree rounds of the proof path's plan 3.  points_xy NULL: seeded pseudo-random
+ * coordinates generated on the device instead (a timing workload, not curve
+ * points).  sums_xy (may be NULL): n_lists x 96 bytes; *ms (may be NULL): the
+ * rounds' device time.  At most 2^27 points.  No counterpart in the reference.
+ */
+vkzg_result vkzg_b200_tree_sums_selftest(const uint8_t *points_xy, size_t n_lists, uint32_t m, uint64_t seed,
+                                         uint8_t *sums_xy, double *ms);
 
 #ifdef __cplusplus
 } /* extern "C" */

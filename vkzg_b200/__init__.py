@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_server_options_default", "vkzg_b200_server_new", "vkzg_b200_server_free",
     "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
     "vkzg_b200_server_stats", "vkzg_b200_kernel_launches", "vkzg_b200_digit_table",
+    "vkzg_b200_tree_sums_selftest",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -145,6 +146,9 @@ def library():
             L.vkzg_b200_server_wait.restype = ctypes.c_int
             L.vkzg_b200_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats), ctypes.c_int]
             L.vkzg_b200_server_stats.restype = ctypes.c_int
+            L.vkzg_b200_tree_sums_selftest.argtypes = [vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, vp,
+                                                       ctypes.POINTER(ctypes.c_double)]
+            L.vkzg_b200_tree_sums_selftest.restype = ctypes.c_int
             L.vkzg_b200_digit_table.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]
             L.vkzg_b200_digit_table.restype = ctypes.c_int
             L.vkzg_b200_kernel_launches.argtypes = []
@@ -400,6 +404,18 @@ def bucket_sums_selftest(points_xy, bucket_of):
     out = np.zeros(128 * 96, np.uint8)
     _check(library().vkzg_b200_bucket_sums_selftest(_ptr(pts), _ptr(idx), len(idx), _ptr(out)))
     return out.tobytes()
+
+
+def tree_sums_selftest(points_xy, n_lists, m, seed=0):
+    """Sums n_lists lists of m points (96-byte x || y each) with the grid-wide tree
+    rounds; points_xy None = seeded device-generated coordinates (timing only).
+    Returns (sums bytes or None, device ms)."""
+    import numpy as np
+    ms = ctypes.c_double()
+    pts = None if points_xy is None else np.ascontiguousarray(np.frombuffer(bytes(points_xy), np.uint8))
+    out = np.zeros(n_lists * 96, np.uint8) if pts is not None else None
+    _check(library().vkzg_b200_tree_sums_selftest(_ptr(pts), n_lists, m, seed, _ptr(out), ctypes.byref(ms)))
+    return (out.tobytes() if out is not None else None), ms.value
 
 
 def write_tables(g1_monomial_compressed, out_path):

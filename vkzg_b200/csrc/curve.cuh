@@ -53,6 +53,33 @@ VK_HD G1J g1_dbl(const G1J &p) {
     return r;
 }
 
+// g1_dbl with the products inlined: the independent products of one doubling
+// (X^2, Y^2, Y Z; then B^2, (X + B)^2, E^2) overlap instead of running as
+// sequential calls.  For latency-bound chains of doublings (the ladder).
+VK_HD Fp fp_mul_inl(const Fp &a, const Fp &b) {
+    Fp r;
+    mont_mul<12>(r.v, a.v, b.v);
+    return r;
+}
+VK_HD G1J g1_dbl_inl(const G1J &p) {
+    if (fp_is_zero(p.z)) return p;
+    const Fp A = fp_mul_inl(p.x, p.x);
+    const Fp B = fp_mul_inl(p.y, p.y);
+    const Fp YZ = fp_mul_inl(p.y, p.z);
+    const Fp C = fp_mul_inl(B, B);
+    const Fp XB = fp_add(p.x, B);
+    Fp t0 = fp_mul_inl(XB, XB);
+    const Fp E = fp_add(fp_dbl(A), A);
+    const Fp F = fp_mul_inl(E, E);
+    t0 = fp_sub(fp_sub(t0, A), C);
+    const Fp D = fp_dbl(t0);
+    G1J r;
+    r.x = fp_sub(F, fp_dbl(D));
+    r.y = fp_sub(fp_mul_inl(E, fp_sub(D, r.x)), fp_dbl(fp_dbl(fp_dbl(C))));
+    r.z = fp_dbl(YZ);
+    return r;
+}
+
 // add-2007-bl: 11M + 5S
 VK_HD G1J g1_add(const G1J &a, const G1J &b) {
     if (fp_is_zero(a.z)) return b;

@@ -77,9 +77,60 @@ __global__ void __launch_bounds__(32) k_bucket_sums_selftest(const G1A *points, 
     }
 }
 
+// Seeded pseudo-random coordinates below 2^380 < p (a timing workload for the
+// tree rounds: field elements, not curve points).
+__global__ void k_seed_lists(G1A *pts, size_t n, uint64_t seed) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+    G1A a;
+    uint32_t *w = reinterpret_cast<uint32_t *>(&a);
+    for (int k = 0; k < 24; k++) {
+        z += 0x9E3779B97F4A7C15ull;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        w[k] = (uint32_t)(x ^ (x >> 31));
+    }
+    a.x.v[11] &= 0x0fffffffu;
+    a.y.v[11] &= 0x0fffffffu;
+    st_vec(&pts[i], a);
+}
+
 } // namespace vkzg
 
 using namespace vkzg;
+
+// 96-byte (x || y canonical big-endian, all zero = infinity) <-> Montgomery affine
+static G1A point_from_be(const uint8_t *xy) {
+    G1A a;
+    bool inf = true;
+    for (int c = 0; c < 2; c++) {
+        Fp v;
+        for (int limb = 0; limb < 12; limb++) {
+            const uint8_t *b = xy + 48 * c + (11 - limb) * 4;
+            v.v[limb] = ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | b[3];
+        }
+        inf &= fp_is_zero(v);
+        (c == 0 ? a.x : a.y) = fp_from_canonical(v);
+    }
+    if (inf) a.x = a.y = fp_zero();
+    return a;
+}
+
+static void point_to_be(const G1A &p, uint8_t *xy) {
+    const bool inf = g1a_is_identity(p);
+    for (int c = 0; c < 2; c++) {
+        const Fp v = inf ? fp_zero() : fp_to_canonical(c == 0 ? p.x : p.y);
+        for (int limb = 0; limb < 12; limb++) {
+            uint8_t *b = xy + 48 * c + (11 - limb) * 4;
+            b[0] = (uint8_t)(v.v[limb] >> 24);
+            b[1] = (uint8_t)(v.v[limb] >> 16);
+            b[2] = (uint8_t)(v.v[limb] >> 8);
+            b[3] = (uint8_t)v.v[limb];
+        }
+    }
+}
 
 // points_xy: n affine points, 96 bytes each (x || y, canonical big-endian; all
 // zero = infinity); bucket_of: n bucket indices < 128.  sums_xy: 128 x 96 bytes.
@@ -95,21 +146,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
     for (int k = 0; k < kBABuckets; k++) start[k + 1] += start[k];
     std::vector<uint32_t> cur(start.begin(), start.end() - 1);
     std::vector<G1A> pts(n > 0 ? n : 1);
-    for (size_t i = 0; i < n; i++) {
-        G1A a;
-        bool inf = true;
-        for (int c = 0; c < 2; c++) {
-            Fp v;
-            for (int limb = 0; limb < 12; limb++) {
-                const uint8_t *b = points_xy + 96 * i + 48 * c + (11 - limb) * 4;
-                v.v[limb] = ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | b[3];
-            }
-            inf &= fp_is_zero(v);
-            (c == 0 ? a.x : a.y) = fp_from_canonical(v);
-        }
-        if (inf) a.x = a.y = fp_zero();
-        pts[cur[bucket_of[i]]++] = a;
-    }
+    for (size_t i = 0; i < n; i++) pts[cur[bucket_of[i]]++] = point_from_be(points_xy + 96 * i);
     G1A *d_pts = nullptr, *d_sums = nullptr, *d_scratch = nullptr;
     uint32_t *d_start = nullptr;
     vkzg_result rc = VKZG_OK;
@@ -129,21 +166,8 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
                 cudaMemcpy(sums.data(), d_sums, kBABuckets * sizeof(G1A), cudaMemcpyDeviceToHost) != cudaSuccess)
                 rc = VKZG_ERR_GPU;
         }
-        if (rc == VKZG_OK) {
-            for (int k = 0; k < kBABuckets; k++) {
-                const bool inf = g1a_is_identity(sums[k]);
-                for (int c = 0; c < 2; c++) {
-                    const Fp v = inf ? fp_zero() : fp_to_canonical(c == 0 ? sums[k].x : sums[k].y);
-                    for (int limb = 0; limb < 12; limb++) {
-                        uint8_t *b = sums_xy + 96 * k + 48 * c + (11 - limb) * 4;
-                        b[0] = (uint8_t)(v.v[limb] >> 24);
-                        b[1] = (uint8_t)(v.v[limb] >> 16);
-                        b[2] = (uint8_t)(v.v[limb] >> 8);
-                        b[3] = (uint8_t)v.v[limb];
-                    }
-                }
-            }
-        }
+        if (rc == VKZG_OK)
+            for (int k = 0; k < kBABuckets; k++) point_to_be(sums[k], sums_xy + 96 * k);
     }
     cudaFree(d_pts);
     cudaFree(d_sums);
@@ -197,4 +221,80 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
     cudaFree(sink);
     *result = best;
     return VKZG_OK;
+}
+
+// Sums n_lists lists of m points each with the proof path's grid-wide
+// batch-affine tree rounds (plan 3's phase-A rounds, without the digit table).
+// points_xy: n_lists * m points of 96 bytes (list o first), or NULL for seeded
+// pseudo-random coordinates generated on the device (a timing workload).
+// sums_xy (may be NULL): n_lists x 96 bytes.  *ms (may be NULL): device time of
+// the rounds.
+extern "C" vkzg_result vkzg_b200_tree_sums_selftest(const uint8_t *points_xy, size_t n_lists, uint32_t m,
+                                                    uint64_t seed, uint8_t *sums_xy, double *ms) {
+    if (n_lists == 0 || m == 0 || n_lists > (1u << 24) || (size_t)n_lists * m > (1ull << 27))
+        return VKZG_ERR_BADARGS;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return VKZG_ERR_GPU;
+    const int blocks = sms * 2;
+    const size_t lanes = (size_t)blocks * 256, total = n_lists * (size_t)m;
+    const size_t slots = (n_lists * (size_t)(m / 2) + lanes - 1) / lanes + 1;
+    G1A *lists = nullptr, *buf0 = nullptr, *buf1 = nullptr, *sums = nullptr;
+    uint32_t *pre = nullptr;
+    Fp *others = nullptr, *tot = nullptr, *totinv = nullptr;
+    vkzg_result rc = VKZG_OK;
+    if (cudaMalloc(&lists, total * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&buf0, n_lists * (size_t)((m + 1) / 2) * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&buf1, n_lists * (size_t)((m + 3) / 4 + 1) * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&sums, n_lists * sizeof(G1A)) != cudaSuccess ||
+        cudaMalloc(&pre, lanes / 32 * slots * 384 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&others, lanes * sizeof(Fp)) != cudaSuccess ||
+        cudaMalloc(&tot, lanes / 32 * sizeof(Fp)) != cudaSuccess ||
+        cudaMalloc(&totinv, lanes / 32 * sizeof(Fp)) != cudaSuccess) {
+        rc = VKZG_ERR_MALLOC;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == VKZG_OK) {
+        if (points_xy) {
+            std::vector<G1A> pts(total);
+            for (size_t i = 0; i < total; i++) pts[i] = point_from_be(points_xy + 96 * i);
+            if (cudaMemcpy(lists, pts.data(), total * sizeof(G1A), cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = VKZG_ERR_GPU;
+        } else {
+            k_seed_lists<<<(unsigned)((total + 255) / 256), 256>>>(lists, total, seed);
+        }
+    }
+    if (rc == VKZG_OK) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0);
+        launch_tree_sums(lists, (int)n_lists, m, buf0, buf1, pre, others, tot, totinv, slots, blocks, sums, 0);
+        cudaEventRecord(e1);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = VKZG_ERR_GPU;
+    }
+    if (rc == VKZG_OK && ms) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        *ms = t;
+    }
+    if (rc == VKZG_OK && sums_xy) {
+        std::vector<G1A> out(n_lists);
+        if (cudaMemcpy(out.data(), sums, n_lists * sizeof(G1A), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            rc = VKZG_ERR_GPU;
+        } else {
+            for (size_t o = 0; o < n_lists; o++) point_to_be(out[o], sums_xy + 96 * o);
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(lists);
+    cudaFree(buf0);
+    cudaFree(buf1);
+    cudaFree(sums);
+    cudaFree(pre);
+    cudaFree(others);
+    cudaFree(tot);
+    cudaFree(totinv);
+    return rc;
 }

@@ -125,6 +125,8 @@ struct FlatSizes {
     size_t lanes = 0, dig = 0, buf0 = 0, buf1 = 0, slots = 0, pre_words = 0;
 };
 FlatSizes flat_sizes(int cap, int c);
+int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *buf1, uint32_t *pre, Fp *others,
+                     Fp *tot, Fp *totinv, size_t slots, int blocks, G1A *sums, cudaStream_t s);
 cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int c, cudaStream_t s);
 cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
                                 uint32_t *d_err, cudaStream_t s);

@@ -204,7 +204,8 @@ __global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *
     for (int d = 0; d < kDigits; d++) {
         st_vec(&dst[d], acc);
         if (d + 1 < kDigits)
-            for (int q = 0; q < 8; q++) acc = g1_dbl(acc);
+#pragma unroll 1
+            for (int q = 0; q < 8; q++) acc = g1_dbl_inl(acc);
     }
 }
 
@@ -543,6 +544,26 @@ struct FlatArgs {
     int n_lists;
 };
 
+// End of every pass-1 kernel: the product of the other lanes' running products
+// (prefix x suffix) for each lane, and the warp's product of all of them.
+__device__ __forceinline__ void flat_pass1_products(const Fp &acc, Fp *others, Fp *tot, size_t gl, size_t wg) {
+    const int lane = threadIdx.x & 31;
+    Fp pr = acc, sf = acc;
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fp u = fp_shfl_up(pr, d);
+        if (lane >= d) pr = fp_mul(pr, u);
+        const Fp w = fp_shfl_down(sf, d);
+        if (lane + d < 32) sf = fp_mul(sf, w);
+    }
+    const Fp total = fp_shfl(pr, 31);
+    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
+    if (lane == 0) pre_x = fp_one();
+    if (lane == 31) suf_x = fp_one();
+    st_vec(&others[gl], fp_mul(pre_x, suf_x));
+    if (lane == 0) st_vec(&tot[wg], total);
+}
+
 template <bool FIRST>
 __device__ __forceinline__ G1A flat_load(const FlatArgs &a, uint32_t o, uint32_t t, uint32_t m) {
     if (FIRST) {
@@ -580,7 +601,6 @@ template <bool FIRST>
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
     const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
     const size_t wg = gl >> 5;
-    const int lane = threadIdx.x & 31;
     const uint32_t h = m >> 1;
     const size_t P = (size_t)a.n_lists * h;
     uint32_t *pre = a.pre + wg * a.slots * 384;
@@ -592,21 +612,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint
         wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
     }
-    // products of the other lanes' values (prefix x suffix) and of all of them
-    Fp pr = acc, sf = acc;
-#pragma unroll 1
-    for (int d = 1; d < 32; d <<= 1) {
-        const Fp u = fp_shfl_up(pr, d);
-        if (lane >= d) pr = fp_mul(pr, u);
-        const Fp w = fp_shfl_down(sf, d);
-        if (lane + d < 32) sf = fp_mul(sf, w);
-    }
-    const Fp total = fp_shfl(pr, 31);
-    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
-    if (lane == 0) pre_x = fp_one();
-    if (lane == 31) suf_x = fp_one();
-    st_vec(&a.others[gl], fp_mul(pre_x, suf_x));
-    if (lane == 0) st_vec(&a.tot[wg], total);
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
 
 // Inverts n warp products, 32 per warp with one inversion.
@@ -668,6 +674,53 @@ FlatSizes flat_sizes(int cap, int c) {
     return z;
 }
 
+// Tree rounds from `first_src` (FIRST: the digit table) until every list is one
+// point; returns the buffer holding the sums and adds the launches to *launched.
+template <bool FIRST>
+const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t m, G1A *buf0, G1A *buf1, int blocks,
+                           cudaStream_t s, int *launched) {
+    const int warps = blocks * kFlatThreads / 32;
+    G1A *bufs[2] = {buf0, buf1};
+    int out = 0;
+    const G1A *cur = first_src;
+    bool first = FIRST;
+    while (m > 1) {
+        a.src = cur;
+        a.dst = bufs[out];
+        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        *launched += 3;
+        cur = bufs[out];
+        out ^= 1;
+        m = (m + 1) >> 1;
+        first = false;
+    }
+    return cur;
+}
+
+// Sums of n_lists lists of m points (list o at lists[o m ..]) by the same
+// grid-wide rounds, for tests and profiles of the rounds alone (the lists
+// buffer is not written unless m == 1).  Returns the launches made.
+int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *buf1, uint32_t *pre, Fp *others,
+                     Fp *tot, Fp *totinv, size_t slots, int blocks, G1A *sums, cudaStream_t s) {
+    FlatArgs a;
+    memset(&a, 0, sizeof a);
+    a.pre = pre;
+    a.others = others;
+    a.tot = tot;
+    a.totinv = totinv;
+    a.slots = slots;
+    a.n_lists = n_lists;
+    int launched = 0;
+    const G1A *res = run_tree_rounds<false>(a, lists, m, buf0, buf1, blocks, s, &launched);
+    cudaMemcpyAsync(sums, res, (size_t)n_lists * sizeof(G1A), cudaMemcpyDeviceToDevice, s);
+    count_launches(launched);
+    return launched;
+}
+
 // Phase A of plan 3 for n blobs: digits, tree rounds, Jacobian outputs in
 // w.points.  Returns the number of kernels launched.
 int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
@@ -685,30 +738,11 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.totinv = w.flat_totinv;
     a.slots = w.flat_slots;
     a.n_lists = lists;
-    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
-    int launched = 0;
+    int launched = 1;
     k_flat_digits<<<(lists * kCellElems + 127) / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
-    launched++;
-    uint32_t m = (uint32_t)L;
-    bool first = true;
-    G1A *bufs[2] = {w.flat_buf[0], w.flat_buf[1]};
-    int out = 0;
-    const G1A *cur = nullptr;
-    while (m > 1) {
-        a.src = cur;
-        a.dst = bufs[out];
-        if (first) k_flat_pass1<true><<<blocks, kFlatThreads, 0, s>>>(a, m);
-        else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
-        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
-        if (first) k_flat_pass2<true><<<blocks, kFlatThreads, 0, s>>>(a, m);
-        else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
-        launched += 3;
-        cur = bufs[out];
-        out ^= 1;
-        m = (m + 1) >> 1;
-        first = false;
-    }
-    k_flat_finish<<<(lists + 127) / 128, 128, 0, s>>>(cur, w.points, lists);
+    const G1A *res =
+        run_tree_rounds<true>(a, nullptr, (uint32_t)L, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s, &launched);
+    k_flat_finish<<<(lists + 127) / 128, 128, 0, s>>>(res, w.points, lists);
     return launched + 1;
 }
 
@@ -844,7 +878,6 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, in
     flatb_stage<FIRST>(a, r, sr, items, offs);
     const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
     const size_t wg = gl >> 5;
-    const int lane = threadIdx.x & 31;
     const size_t P = (size_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
     uint32_t *pre = a.pre + wg * a.slots * 384;
     Fp acc = fp_one();
@@ -858,20 +891,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, in
         wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
     }
-    Fp pr = acc, sf = acc;
-#pragma unroll 1
-    for (int d = 1; d < 32; d <<= 1) {
-        const Fp u = fp_shfl_up(pr, d);
-        if (lane >= d) pr = fp_mul(pr, u);
-        const Fp w = fp_shfl_down(sf, d);
-        if (lane + d < 32) sf = fp_mul(sf, w);
-    }
-    const Fp total = fp_shfl(pr, 31);
-    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
-    if (lane == 0) pre_x = fp_one();
-    if (lane == 31) suf_x = fp_one();
-    st_vec(&a.others[gl], fp_mul(pre_x, suf_x));
-    if (lane == 0) st_vec(&a.tot[wg], total);
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
 
 template <bool FIRST>
@@ -1224,6 +1244,206 @@ cudaError_t configure_reduce_schedule() {
     return cudaMemcpyToSymbol(c_red, &s, sizeof(s));
 }
 
+// The binary-split reduction of plans 3 and 4 as grid-wide rounds: round r of
+// the schedule holds the same operations for every output, so its pairs are
+// (output, operation) dealt to all lanes as in the phase rounds; the Horner
+// tail runs one output per thread.
+struct FlatRArgs {
+    const G1A *buckets; // [output][128] bucket sums
+    G1A *slots;         // [output][kRedOps] intermediate sums
+    uint32_t *pre;
+    Fp *others, *tot, *totinv;
+    size_t slots_pre;
+    int n_out;
+};
+
+__device__ __forceinline__ G1A *red_slot(const FlatRArgs &a, uint32_t o, int s) {
+    return s < kBuckets ? const_cast<G1A *>(&a.buckets[(size_t)o * kBuckets + s])
+                        : &a.slots[(size_t)o * kRedOps + (s - kBuckets)];
+}
+
+// shared copy of round r's operations (the schedule in constant memory is read
+// at a different index by every lane, which constant memory serialises)
+struct RedRound {
+    uint16_t a[kRedOps], b[kRedOps], d[kRedOps];
+    int q0, nops;
+};
+
+__device__ void red_stage(RedRound &rr, int r) {
+    const int q0 = c_red.round_start[r], nops = c_red.round_start[r + 1] - q0;
+    for (int q = threadIdx.x; q < nops; q += blockDim.x) {
+        rr.a[q] = c_red.a[q0 + q];
+        rr.b[q] = c_red.b[q0 + q];
+        rr.d[q] = c_red.dst[q0 + q];
+    }
+    if (threadIdx.x == 0) {
+        rr.q0 = q0;
+        rr.nops = nops;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, int r) {
+    __shared__ RedRound rr;
+    red_stage(rr, r);
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const uint32_t nops = (uint32_t)rr.nops;
+    const size_t P = (size_t)a.n_out * nops;
+    uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (size_t p = gl; p < P; p += NL, s++) {
+        const uint32_t o = (uint32_t)(p / nops), q = (uint32_t)(p - (size_t)o * nops);
+        const G1A x = ld_vec(red_slot(a, o, rr.a[q])), y = ld_vec(red_slot(a, o, rr.b[q]));
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+    }
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, int r) {
+    __shared__ RedRound rr;
+    red_stage(rr, r);
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const uint32_t nops = (uint32_t)rr.nops;
+    const size_t P = (size_t)a.n_out * nops;
+    const uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        const size_t p = gl + (size_t)t * NL;
+        const uint32_t o = (uint32_t)(p / nops), q = (uint32_t)(p - (size_t)o * nops);
+        const G1A x = ld_vec(red_slot(a, o, rr.a[q])), y = ld_vec(red_slot(a, o, rr.b[q]));
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, den);
+        st_vec(red_slot(a, o, rr.d[q]), pair_result(x, y, kind, inv_den));
+    }
+}
+
+// H = sum_b 2^b T_b (Horner over the 7 bit sums), then + S: the reduction's result
+__global__ void __launch_bounds__(128) k_flatr_horner(FlatRArgs a, G1J *out) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= (uint32_t)a.n_out) return;
+    G1J h = g1_from_affine(ld_vec(red_slot(a, o, c_red.t_slot[6])));
+    for (int j = 5; j >= 0; j--) {
+        h = g1_dbl(h);
+        h = g1_madd(h, ld_vec(red_slot(a, o, c_red.t_slot[j])));
+    }
+    st_vec(&out[o], g1_madd(h, ld_vec(red_slot(a, o, c_red.all_slot))));
+}
+
+// sum_k (k + 1) B_k of every output into out; returns the launches made
+int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_out, cudaStream_t s) {
+    static int rounds = -1;
+    if (rounds < 0) {
+        ReduceSchedule h;
+        rounds = build_reduce_schedule(h) ? h.n_rounds : 0;
+    }
+    FlatRArgs a;
+    a.buckets = buckets;
+    a.slots = w.red_scratch;
+    a.pre = w.flat_pre;
+    a.others = w.flat_others;
+    a.tot = w.flat_tot;
+    a.totinv = w.flat_totinv;
+    a.slots_pre = w.flat_slots;
+    a.n_out = n_out;
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    for (int r = 0; r < rounds; r++) {
+        k_flatr_pass1<<<blocks, kFlatThreads, 0, s>>>(a, r);
+        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        k_flatr_pass2<<<blocks, kFlatThreads, 0, s>>>(a, r);
+    }
+    k_flatr_horner<<<(n_out + 127) / 128, 128, 0, s>>>(a, out);
+    return 3 * rounds + 1;
+}
+
+// Plans 3 and 4 fold the ladder after normalising it: L+-[j][d] = L[j][d] +-
+// L[j + 64][d] as one grid-wide round of affine additions (6 Fp multiplies
+// each with the shared inversion) instead of Jacobian additions (16) followed
+// by a normalisation of the results.  Pair q = ((blob * 64 + j) * 32 + d) * 2 +
+// sign writes folded[blob][sign * 64 + j][d].
+struct FoldArgs {
+    const G1A *lad;  // [blob][128][32] normalised ladder
+    G1A *out;        // [blob][128][32]: plus half, then minus half
+    uint32_t *pre;
+    Fp *others, *tot, *totinv;
+    size_t slots_pre;
+    int n_blobs;
+};
+
+__device__ __forceinline__ void fold_pair(const FoldArgs &a, size_t q, G1A &x, G1A &y, size_t &dst) {
+    const int sign = (int)(q & 1);
+    const size_t r = q >> 1;
+    const size_t b = r / (kHalf * kDigits), jd = r % (kHalf * kDigits);
+    const size_t j = jd / kDigits, d = jd % kDigits;
+    const size_t base = b * kCells * kDigits;
+    x = ld_vec(&a.lad[base + j * kDigits + d]);
+    y = ld_vec(&a.lad[base + (j + kHalf) * kDigits + d]);
+    if (sign) y.y = fp_neg(y.y);
+    dst = base + (j + (sign ? kHalf : 0)) * kDigits + d;
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass1(FoldArgs a) {
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const size_t P = (size_t)a.n_blobs * kHalf * kDigits * 2;
+    uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (size_t p = gl; p < P; p += NL, s++) {
+        G1A x, y;
+        size_t dst;
+        fold_pair(a, p, x, y, dst);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+    }
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass2(FoldArgs a) {
+    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
+    const size_t wg = gl >> 5;
+    const size_t P = (size_t)a.n_blobs * kHalf * kDigits * 2;
+    const uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        G1A x, y;
+        size_t dst;
+        fold_pair(a, gl + (size_t)t * NL, x, y, dst);
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, den);
+        st_vec(&a.out[dst], pair_result(x, y, kind, inv_den));
+    }
+}
+
+// normalise the ladder into `scratch`, then fold it into w.ladder_aff; returns the launches made
+int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) {
+    const int n_lad = n * kCells * kDigits;
+    k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, scratch, n_lad);
+    FoldArgs a;
+    a.lad = scratch;
+    a.out = w.ladder_aff;
+    a.pre = w.flat_pre;
+    a.others = w.flat_others;
+    a.tot = w.flat_tot;
+    a.totinv = w.flat_totinv;
+    a.slots_pre = w.flat_slots;
+    a.n_blobs = n;
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    k_fold_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
+    k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+    k_fold_pass2<<<blocks, kFlatThreads, 0, s>>>(a);
+    return 4;
+}
+
 // ---------------------------------------------------------------- launcher
 // ev (nullable): kProofStages + 1 events recorded around the stages.
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev) {
@@ -1252,7 +1472,8 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     int launched = 10;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
     auto reduce = [&]() {
-        if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
+        if (flatb) launched += launch_reduce_flat(w, w.bucket_aff, w.points, n_out, s) - 1;
+        else if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
         else if (hier)
             k_reduce_hier<<<(n_out + kRedOutputs - 1) / kRedOutputs, kRedThreads, 0, s>>>(w.bucket_aff, w.points,
                                                                                        w.red_scratch, n_out);
@@ -1273,9 +1494,15 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
     mark();
-    k_fold<<<(n * kHalf * kDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
-    mark();
-    k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
+    if (flatb) {
+        // normalise, then fold in affine form (the "normalize" stage is empty)
+        launched += launch_fold_affine(w, n, reinterpret_cast<G1A *>(w.folded), s) - 2;
+        mark();
+    } else {
+        k_fold<<<(n * kHalf * kDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
+        mark();
+        k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
+    }
     mark();
     if (flatb) {
         launched += launch_phase_b_flat(t, w, n, s) - 1;
