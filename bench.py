@@ -150,13 +150,14 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU legs
-def cpu_rates(n_proofs, n_recover, seed=7):
-    """Oracle (CPU restatement of the reference algorithm) on all host threads."""
+def cpu_rates(n_proofs, n_recover, seed=7, threads=None):
+    """Oracle (CPU restatement of the reference algorithm) on `threads` host
+    threads (all of them by default)."""
     from oracle import Oracle
     o = Oracle()
     with open(os.path.join(ROOT, "vkzg_b200", "data", "trusted_setup_g1_monomial.bin"), "rb") as f:
         tables = o.tables_from_setup(f.read())
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     # a sample of the 256-blob workload: its random part (the 4 adversarial blobs are ~free)
     blobs = make_blobs(n_proofs, seed, adversarial=False)
     t0 = time.perf_counter()
@@ -433,10 +434,14 @@ def run_ours(args, rank, world, local_rank):
         from oracle import build
         build()
         c = cpu_rates(args.cpu_sample, args.cpu_sample)
+        one = cpu_rates(2, 4, threads=1)
         cpu = {"value": c["combined"], "unit": "blobs/s", "cores": c["threads"], "kind": "port",
                "sample": f"{args.cpu_sample} proof blobs + {args.cpu_sample} recovery blobs of the same workload "
                          f"on {c['threads']} host threads ({c['seconds']:.1f} s)",
-               "proof_blobs_per_s": c["proof_blobs_per_s"], "recovery_blobs_per_s": c["recovery_blobs_per_s"]}
+               "proof_blobs_per_s": c["proof_blobs_per_s"], "recovery_blobs_per_s": c["recovery_blobs_per_s"],
+               "single_core": {"proof_blobs_per_s": one["proof_blobs_per_s"],
+                               "recovery_blobs_per_s": one["recovery_blobs_per_s"],
+                               "sample": "2 proof blobs + 4 recovery blobs on 1 thread"}}
 
     line = {
         "metric": METRIC, "value": value, "unit": "blobs/s", "n_gpus": world, "steps": args.steps,

@@ -13,6 +13,16 @@ void shim_fp_mul(const uint32_t *a, const uint32_t *b, uint32_t *r) {
     memcpy(y.v, b, 48);
     memcpy(r, fp_mul(x, y).v, 48);
 }
+void shim_fp_sqr(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    (void)b;
+    Fp x;
+    memcpy(x.v, a, 48);
+    memcpy(r, fp_sqr(x).v, 48);
+}
+void shim_fr_sqr(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    (void)b;
+    mont_sqr<8>(r, a);
+}
 void shim_fp_add(const uint32_t *a, const uint32_t *b, uint32_t *r) {
     Fp x, y;
     memcpy(x.v, a, 48);

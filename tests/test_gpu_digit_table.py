@@ -37,7 +37,7 @@ def test_plan3_synthetic_vs_oracle(synthetic, oracle, tmp_path, monkeypatch):
     with vkzg_b200.Prover(max_batch_size=len(blobs)) as p:
         assert p.compute_proofs_raw(out, blobs, len(blobs)) == 0
         c, build_ms, nbytes = p.digit_table()
-        assert 10 <= c <= 12 and nbytes > 0
+        assert 10 <= c <= 13 and nbytes > 0
     rc, want = oracle.compute_proofs(tables, blobs)
     assert rc == 0
     for b in range(len(blobs)):

@@ -34,13 +34,18 @@ def test_field_ops(shim, field):
     mod, n, radix = (P_MOD, 12, 1 << 384) if field == "fp" else (R_MOD, 8, 1 << 256)
     rinv = pow(radix, -1, mod)
     rng = random.Random(7)
-    edge = [0, 1, 2, mod - 1, mod - 2, radix % mod, radix * radix % mod, mod // 2, (mod + 1) // 2]
+    top = mod.bit_length() - 1
+    edge = [0, 1, 2, mod - 1, mod - 2, radix % mod, radix * radix % mod, mod // 2, (mod + 1) // 2,
+            (1 << top) - 1, mod - (1 << 32), mod - (1 << 200) - 1, ((1 << top) - 1) ^ (0xFFFF << 64)]
+    edge += [mod - 1 - rng.randrange(1 << 64) for _ in range(50)]  # long runs of high words
     vals = edge + [rng.randrange(mod) for _ in range(2000)]
     out = (ctypes.c_uint32 * n)()
     for k, a in enumerate(vals):
         b = vals[(7 * k + 3) % len(vals)]
         getattr(shim, f"shim_{field}_mul")(words(a, n), words(b, n), out)
         assert value(out, n) == a * b * rinv % mod
+        getattr(shim, f"shim_{field}_sqr")(words(a, n), words(b, n), out)
+        assert value(out, n) == a * a * rinv % mod
         getattr(shim, f"shim_{field}_add")(words(a, n), words(b, n), out)
         assert value(out, n) == (a + b) % mod
         getattr(shim, f"shim_{field}_sub")(words(a, n), words(b, n), out)

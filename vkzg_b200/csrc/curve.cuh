@@ -61,16 +61,21 @@ VK_HD Fp fp_mul_inl(const Fp &a, const Fp &b) {
     mont_mul<12>(r.v, a.v, b.v);
     return r;
 }
+VK_HD Fp fp_sqr_inl(const Fp &a) {
+    Fp r;
+    mont_sqr<12>(r.v, a.v);
+    return r;
+}
 VK_HD G1J g1_dbl_inl(const G1J &p) {
     if (fp_is_zero(p.z)) return p;
-    const Fp A = fp_mul_inl(p.x, p.x);
-    const Fp B = fp_mul_inl(p.y, p.y);
+    const Fp A = fp_sqr_inl(p.x);
+    const Fp B = fp_sqr_inl(p.y);
     const Fp YZ = fp_mul_inl(p.y, p.z);
-    const Fp C = fp_mul_inl(B, B);
+    const Fp C = fp_sqr_inl(B);
     const Fp XB = fp_add(p.x, B);
-    Fp t0 = fp_mul_inl(XB, XB);
+    Fp t0 = fp_sqr_inl(XB);
     const Fp E = fp_add(fp_dbl(A), A);
-    const Fp F = fp_mul_inl(E, E);
+    const Fp F = fp_sqr_inl(E);
     t0 = fp_sub(fp_sub(t0, A), C);
     const Fp D = fp_dbl(t0);
     G1J r;

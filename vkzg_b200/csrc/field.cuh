@@ -241,6 +241,91 @@ VK_HD void mont_mul(uint32_t *r, const uint32_t *a, const uint32_t *b) {
     for (int i = 0; i < N; i++) r[i] = borrow ? t[i] : s[i];
 }
 
+// Montgomery square a^2 / R mod m: the cross products a_i a_j (i < j) once,
+// doubled by a shift, plus the diagonal, then word-by-word reduction of the
+// 2n-word square (separated operand scanning).  n(n-1) + 2n + 2n^2 + n
+// multiply instructions against 4n^2 + n for mont_mul(a, a); same result.
+template <int N>
+VK_HD void mont_sqr(uint32_t *r, const uint32_t *a) {
+    CARRY_DECL
+    uint32_t T[2 * N];
+#pragma unroll
+    for (int i = 0; i < 2 * N; i++) T[i] = 0;
+    // Row i adds a_i a_j (j > i) at T[i + j] in two chains of disjoint word
+    // pairs (j = i+1, i+3, ... and j = i+2, i+4, ...).  T[i + n + 1] is still zero
+    // when row i starts, so each chain's carry stops there.
+#pragma unroll
+    for (int i = 0; i < N - 1; i++) {
+#pragma unroll
+        for (int c = 1; c <= 2; c++) {
+            const int j0 = i + c;
+            if (j0 >= N) continue;
+            MAD_LO_CC(T[i + j0], a[i], a[j0], T[i + j0]);
+            MADC_HI_CC(T[i + j0 + 1], a[i], a[j0], T[i + j0 + 1]);
+            int top = i + j0 + 1;
+#pragma unroll
+            for (int j = j0 + 2; j < N; j += 2) {
+                MADC_LO_CC(T[i + j], a[i], a[j], T[i + j]);
+                MADC_HI_CC(T[i + j + 1], a[i], a[j], T[i + j + 1]);
+                top = i + j + 1;
+            }
+#pragma unroll
+            for (int k = top + 1; k < i + N + 1; k++) ADDC_CC(T[k], T[k], 0u);
+            ADDC(T[i + N + 1], T[i + N + 1], 0u);
+        }
+    }
+    // x2 (the cross sum is below 2^(64n - 1))
+#pragma unroll
+    for (int k = 2 * N - 1; k > 0; k--) T[k] = (T[k] << 1) | (T[k - 1] >> 31);
+    T[0] <<= 1;
+    // + a_i^2 at T[2i]
+    MAD_LO_CC(T[0], a[0], a[0], T[0]);
+    MADC_HI_CC(T[1], a[0], a[0], T[1]);
+#pragma unroll
+    for (int i = 1; i < N - 1; i++) {
+        MADC_LO_CC(T[2 * i], a[i], a[i], T[2 * i]);
+        MADC_HI_CC(T[2 * i + 1], a[i], a[i], T[2 * i + 1]);
+    }
+    MADC_LO_CC(T[2 * N - 2], a[N - 1], a[N - 1], T[2 * N - 2]);
+    MADC_HI(T[2 * N - 1], a[N - 1], a[N - 1], T[2 * N - 1]);
+    // reduction: row i clears T[i] with q m 2^(32 i); its carry out of T[i + n]
+    // is owed to T[i + n + 1] and added by row i + 1 (the last row owes none:
+    // a^2 + q m < m^2 + R m < R^2)
+    uint32_t owed = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint32_t q = T[i] * mod_n0<N>();
+        uint32_t ce, co;
+        MAD_LO_CC(T[i], q, mod_word<N>(0), T[i]);
+        MADC_HI_CC(T[i + 1], q, mod_word<N>(0), T[i + 1]);
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            MADC_LO_CC(T[i + j], q, mod_word<N>(j), T[i + j]);
+            MADC_HI_CC(T[i + j + 1], q, mod_word<N>(j), T[i + j + 1]);
+        }
+        ADDC_CC(T[i + N], T[i + N], owed);
+        ADDC(ce, 0u, 0u);
+        MAD_LO_CC(T[i + 1], q, mod_word<N>(1), T[i + 1]);
+        MADC_HI_CC(T[i + 2], q, mod_word<N>(1), T[i + 2]);
+#pragma unroll
+        for (int j = 3; j < N; j += 2) {
+            MADC_LO_CC(T[i + j], q, mod_word<N>(j), T[i + j]);
+            MADC_HI_CC(T[i + j + 1], q, mod_word<N>(j), T[i + j + 1]);
+        }
+        ADDC(co, 0u, 0u);
+        owed = ce + co;
+    }
+    // T[n..2n) < 2m: one conditional subtraction
+    uint32_t s[N];
+    SUB_CC(s[0], T[N], mod_word<N>(0));
+#pragma unroll
+    for (int i = 1; i < N; i++) SUBC_CC(s[i], T[N + i], mod_word<N>(i));
+    uint32_t borrow;
+    SUBC(borrow, 0u, 0u);
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = borrow ? T[N + i] : s[i];
+}
+
 template <int N>
 VK_HD bool limbs_is_zero(const uint32_t *a) {
     uint32_t acc = 0;
@@ -287,7 +372,22 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
     return r;
 #endif
 }
-VK_HD Fp fp_sqr(const Fp &a) { return fp_mul(a, a); }
+#if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
+__device__ __noinline__ Fp fp_sqr_call(Fp a) {
+    Fp r;
+    mont_sqr<12>(r.v, a.v);
+    return r;
+}
+#endif
+VK_HD Fp fp_sqr(const Fp &a) {
+#if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
+    return fp_sqr_call(a);
+#else
+    Fp r;
+    mont_sqr<12>(r.v, a.v);
+    return r;
+#endif
+}
 VK_HD Fp fp_add(const Fp &a, const Fp &b) {
     Fp r;
     mod_add<12>(r.v, a.v, b.v);
