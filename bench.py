@@ -42,6 +42,9 @@ PHASE_A_FP_MUL_PER_BLOB = 2.87e6     # ~261k madd-2007-bl (11 Fp mul) per blob
 PROOF_IMAD_PER_BLOB = 3.36e9         # 5.81M Fp mul + 74k Fr mul
 RECOVERY_IMAD_PER_BLOB = 118e6       # 0.46M Fr mul (4 NTT-8192 + pointwise + batch division)
 NOMINAL_IMAD_TPS = 148 * 64 * 1.965e9 / 1e12
+# DRAM bytes of phase A per blob under plan 3 (13-bit digit table), from one
+# single-pass ncu capture of a 256-blob proof step (32.3 GB / 256)
+PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 = 32.3e9 / 256
 
 
 # ------------------------------------------------------------------ inputs
@@ -476,7 +479,9 @@ def run_ours(args, rank, world, local_rank):
                                     "reference algorithm's phase-A work (madd-2007-bl bucket accumulation); "
                                     "frac above 1 = fewer operations than the reference, frac_executed = the "
                                     "Fp multiplies this kernel executes",
-                     "traffic": None},
+                     "traffic": PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 * n if plan == 3 and digit and digit[0] == 13
+                     else None,
+                     "traffic_unit": "bytes per phase-A pass over the batch (ncu dram__bytes_read + write)"},
         "digit_table": {"window_bits": digit[0], "build_ms": round(digit[1], 1), "bytes": digit[2]} if digit else None,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),

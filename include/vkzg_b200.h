@@ -150,7 +150,9 @@ uint64_t vkzg_b200_kernel_launches(void);
  * the next batch.  A batch is admitted only while the device working set of
  * all batches in flight stays within hbm_budget_bytes.  Each blob is computed
  * independently, so a request's output is the same alone and in any mix.
- * vkzg_b200_server_wait returns the request's status (VKZG_ERR_INVALID_BLOB /
+ * vkzg_b200_server_new tunes the proof plan of every batch size class up to
+ * max_blobs_per_batch on one lane and gives the choices to all lanes, so that
+ * no request waits for a tuning run.  vkzg_b200_server_wait returns the request's status (VKZG_ERR_INVALID_BLOB /
  * VKZG_ERR_BADARGS as the batch calls would; VKZG_ERR_GPU on timeout, with the
  * ticket still valid).  Stats cover requests completed since the last reset:
  * latency from submit to completion.

@@ -131,6 +131,11 @@ cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, i
 cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
                                 uint32_t *d_err, cudaStream_t s);
 cudaError_t configure_kernels();
+}
+struct vkzg_prover;
+namespace vkzg {
+void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src);
+
 // process-wide count of kernels launched by the launchers above
 void count_launches(int k);
 uint64_t launches_total();

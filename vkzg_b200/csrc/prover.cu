@@ -1164,6 +1164,15 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
     return VKZG_OK;
 }
 
+namespace vkzg {
+// dst takes src's tuned plans (provers of one serving loop share their decisions)
+void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src) {
+    if (!dst || !src || dst == src) return;
+    std::lock_guard<std::mutex> lock(dst->mutex);
+    for (const auto &kv : src->plan_of) dst->plan_of[kv.first] = kv.second;
+}
+} // namespace vkzg
+
 uint64_t vkzg_b200_kernel_launches(void) { return launches_total(); }
 
 int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes) {

@@ -13,6 +13,7 @@
 // batched with.
 #include "../../include/vkzg.h"
 #include "../../include/vkzg_b200.h"
+#include "kernels.h"
 
 #include <cuda_runtime.h>
 
@@ -251,6 +252,14 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
         vkzg_b200_server_free(s);
         return rc;
     }
+    // tune every batch size class once, before any request, and share the
+    // decisions (and with plan 3 the digit table) with every lane: no request
+    // waits for a tuning run
+    if (vkzg_b200_autotune(s->lanes[0]->p, cap) != VKZG_OK) {
+        vkzg_b200_server_free(s);
+        return VKZG_ERR_GPU;
+    }
+    for (auto &l : s->lanes) vkzg::adopt_tuning(l->p, s->lanes[0]->p);
     for (auto &l : s->lanes) {
         Lane *lp = l.get();
         l->worker = std::thread([s, lp] { s->lane_loop(lp); });
