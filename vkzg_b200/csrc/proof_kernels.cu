@@ -615,11 +615,13 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
 
-// Inverts n warp products, 32 per warp with one inversion.
-__global__ void __launch_bounds__(128) k_flat_invert(const Fp *__restrict__ tot, Fp *totinv, int n) {
+// Inverts the n warp products, one per thread: the launch sits on the critical
+// path between the passes, and one divstep inversion per lane (all in parallel)
+// has less latency than a shared batch inversion (a product scan of 32 values,
+// one inversion, a scan back).
+__global__ void __launch_bounds__(64) k_flat_invert(const Fp *__restrict__ tot, Fp *totinv, int n) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const Fp r = warp_batch_inverse_fp(t < n ? ld_vec(&tot[t]) : fp_one());
-    if (t < n) st_vec(&totinv[t], r);
+    if (t < n) st_vec(&totinv[t], fp_inv_fast(ld_vec(&tot[t])));
 }
 
 template <bool FIRST>
@@ -689,7 +691,7 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t m, G1A *bu
         a.dst = bufs[out];
         if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
         else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
-        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
         if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
         else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
         *launched += 3;
@@ -978,7 +980,7 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
         a.dst = bufs[out];
         if (r == 0) k_flatb_pass1<true><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
         else k_flatb_pass1<false><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
-        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
         if (r == 0) k_flatb_pass2<true><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
         else k_flatb_pass2<false><<<blocks, kFlatThreads, kFlatBSmem, s>>>(a, r);
         launched += 3;
@@ -1355,7 +1357,7 @@ int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_o
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     for (int r = 0; r < rounds; r++) {
         k_flatr_pass1<<<blocks, kFlatThreads, 0, s>>>(a, r);
-        k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+        k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
         k_flatr_pass2<<<blocks, kFlatThreads, 0, s>>>(a, r);
     }
     k_flatr_horner<<<(n_out + 127) / 128, 128, 0, s>>>(a, out);
@@ -1439,7 +1441,7 @@ int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) 
     a.n_blobs = n;
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     k_fold_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
-    k_flat_invert<<<(warps + 127) / 128, 128, 0, s>>>(a.tot, a.totinv, warps);
+    k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
     k_fold_pass2<<<blocks, kFlatThreads, 0, s>>>(a);
     return 4;
 }
