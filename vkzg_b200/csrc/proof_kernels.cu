@@ -597,20 +597,44 @@ __global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scal
     }
 }
 
+// Pair p = o h + i of a round (list o, pair i); a lane walks p = gl, gl + NL,
+// ... (pass 1) or back (pass 2), stepping (o, i) by (NL / h, NL % h) instead of
+// dividing for every pair.  All indices fit in 32 bits (at most 2^32 pairs per
+// round: the working set caps a chunk far below that).
+__device__ __forceinline__ void pair_step_up(uint32_t &o, uint32_t &i, uint32_t h, uint32_t dq, uint32_t dr) {
+    i += dr;
+    o += dq;
+    if (i >= h) {
+        i -= h;
+        o++;
+    }
+}
+__device__ __forceinline__ void pair_step_down(uint32_t &o, uint32_t &i, uint32_t h, uint32_t dq, uint32_t dr) {
+    if (i < dr) {
+        i += h - dr;
+        o -= dq + 1;
+    } else {
+        i -= dr;
+        o -= dq;
+    }
+}
+
 template <bool FIRST>
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1;
-    const size_t P = (size_t)a.n_lists * h;
-    uint32_t *pre = a.pre + wg * a.slots * 384;
+    const uint32_t P = (uint32_t)a.n_lists * h;
+    const uint32_t dq = NL / h, dr = NL % h;
+    uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp acc = fp_one();
     int s = 0;
-    for (size_t p = gl; p < P; p += NL, s++) {
-        const uint32_t o = (uint32_t)(p / h), i = (uint32_t)(p - (size_t)o * h);
+    uint32_t o = gl / h, i = gl % h;
+    for (uint32_t p = gl; p < P; p += NL, s++) {
         const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
         wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+        pair_step_up(o, i, h, dq, dr);
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
@@ -626,16 +650,22 @@ __global__ void __launch_bounds__(64) k_flat_invert(const Fp *__restrict__ tot, 
 
 template <bool FIRST>
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint32_t m) {
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1, m_next = (m + 1) >> 1;
-    const size_t P = (size_t)a.n_lists * h;
-    const uint32_t *pre = a.pre + wg * a.slots * 384;
+    const uint32_t P = (uint32_t)a.n_lists * h;
+    const uint32_t dq = NL / h, dr = NL % h;
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    uint32_t o = 0, i = 0;
+    if (S > 0) {
+        const uint32_t p_last = gl + (uint32_t)(S - 1) * NL;
+        o = p_last / h;
+        i = p_last % h;
+    }
     for (int t = S - 1; t >= 0; t--) {
-        const size_t p = gl + (size_t)t * NL;
-        const uint32_t o = (uint32_t)(p / h), i = (uint32_t)(p - (size_t)o * h);
+        if (t < S - 1) pair_step_down(o, i, h, dq, dr);
         const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
         const int kind = pair_kind(x, y);
         const Fp den = pair_denominator(x, y, kind);
@@ -644,8 +674,8 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint
         st_vec(&a.dst[(size_t)o * m_next + i], pair_result(x, y, kind, inv_den));
     }
     if (m & 1u)
-        for (size_t o = gl; o < (size_t)a.n_lists; o += NL)
-            st_vec(&a.dst[o * m_next + h], flat_load<FIRST>(a, (uint32_t)o, m - 1, m));
+        for (uint32_t l = gl; l < (uint32_t)a.n_lists; l += NL)
+            st_vec(&a.dst[(size_t)l * m_next + h], flat_load<FIRST>(a, l, m - 1, m));
 }
 
 __global__ void __launch_bounds__(128) k_flat_finish(const G1A *__restrict__ sums, G1J *points, int n) {
@@ -860,13 +890,13 @@ __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &
 }
 
 // pair p of the round -> output, half, bucket, index
-__device__ __forceinline__ void flatb_pair(const FlatBRound &sr, int n_blobs, size_t p, uint32_t &o, int &h, int &k,
+__device__ __forceinline__ void flatb_pair(const FlatBRound &sr, int n_blobs, uint32_t p, uint32_t &o, int &h, int &k,
                                            uint32_t &i) {
-    const size_t p_plus = (size_t)n_blobs * kHalf * sr.pairs[0];
+    const uint32_t p_plus = (uint32_t)n_blobs * kHalf * sr.pairs[0];
     h = p < p_plus ? 0 : 1;
-    const size_t pp = h ? p - p_plus : p;
+    const uint32_t pp = h ? p - p_plus : p;
     const uint32_t per = sr.pairs[h];
-    const uint32_t ol = (uint32_t)(pp / per), q = (uint32_t)(pp - (size_t)ol * per);
+    const uint32_t ol = pp / per, q = pp - ol * per;
     o = (ol / kHalf) * kCells + h * kHalf + ol % kHalf;
     k = ba_bucket_of<kBuckets>(sr.pscan[h], q);
     i = q - sr.pscan[h][k];
@@ -878,13 +908,13 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, in
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
     uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
-    uint32_t *pre = a.pre + wg * a.slots * 384;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    const uint32_t P = (uint32_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp acc = fp_one();
     int s = 0;
-    for (size_t p = gl; p < P; p += NL, s++) {
+    for (uint32_t p = gl; p < P; p += NL, s++) {
         uint32_t o, i;
         int h, k;
         flatb_pair(sr, a.n_blobs, p, o, h, k, i);
@@ -902,14 +932,14 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
     uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
-    const uint32_t *pre = a.pre + wg * a.slots * 384;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    const uint32_t P = (uint32_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
     for (int t = S - 1; t >= 0; t--) {
-        const size_t p = gl + (size_t)t * NL;
+        const uint32_t p = gl + (uint32_t)t * NL;
         uint32_t o, i;
         int h, k;
         flatb_pair(sr, a.n_blobs, p, o, h, k, i);
@@ -1288,15 +1318,15 @@ __device__ void red_stage(RedRound &rr, int r) {
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, int r) {
     __shared__ RedRound rr;
     red_stage(rr, r);
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
     const uint32_t nops = (uint32_t)rr.nops;
-    const size_t P = (size_t)a.n_out * nops;
-    uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    const uint32_t P = (uint32_t)a.n_out * nops;
+    uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
     Fp acc = fp_one();
     int s = 0;
-    for (size_t p = gl; p < P; p += NL, s++) {
-        const uint32_t o = (uint32_t)(p / nops), q = (uint32_t)(p - (size_t)o * nops);
+    for (uint32_t p = gl; p < P; p += NL, s++) {
+        const uint32_t o = p / nops, q = p - o * nops;
         const G1A x = ld_vec(red_slot(a, o, rr.a[q])), y = ld_vec(red_slot(a, o, rr.b[q]));
         wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
@@ -1307,16 +1337,16 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, in
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, int r) {
     __shared__ RedRound rr;
     red_stage(rr, r);
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
     const uint32_t nops = (uint32_t)rr.nops;
-    const size_t P = (size_t)a.n_out * nops;
-    const uint32_t *pre = a.pre + wg * a.slots_pre * 384;
+    const uint32_t P = (uint32_t)a.n_out * nops;
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
     for (int t = S - 1; t >= 0; t--) {
-        const size_t p = gl + (size_t)t * NL;
-        const uint32_t o = (uint32_t)(p / nops), q = (uint32_t)(p - (size_t)o * nops);
+        const uint32_t p = gl + (uint32_t)t * NL;
+        const uint32_t o = p / nops, q = p - o * nops;
         const G1A x = ld_vec(red_slot(a, o, rr.a[q])), y = ld_vec(red_slot(a, o, rr.b[q]));
         const int kind = pair_kind(x, y);
         const Fp den = pair_denominator(x, y, kind);

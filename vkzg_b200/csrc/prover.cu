@@ -645,7 +645,8 @@ size_t comb_bytes(int c) {
 bool ensure_flat_b(vkzg_prover *p) {
     ProofWork &w = p->pw;
     if (w.flat_pre) return true;
-    if (p->flat_failed || p->t.fb_rounds == 0) return false;
+    // (chunks beyond 4096 blobs would overflow the rounds' 32-bit pair indices)
+    if (p->flat_failed || p->t.fb_rounds == 0 || p->cap > 4096) return false;
     const FlatSizes z = flat_sizes((int)p->cap, 10); // its slots cover every window and phase B
     if (!p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
         !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
