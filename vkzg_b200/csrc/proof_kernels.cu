@@ -1456,10 +1456,73 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass2(FoldArgs a) {
     }
 }
 
+// Jacobian -> affine for n points as one grid-wide round (plans 3-4): Z values
+// dealt to all lanes, one inversion per warp product, x = X / Z^2, y = Y / Z^3;
+// infinity (Z = 0) -> (0, 0).
+struct NormArgs {
+    const G1J *in;
+    G1A *out;
+    uint32_t *pre;
+    Fp *others, *tot, *totinv;
+    size_t slots_pre;
+    uint32_t n;
+};
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass1(NormArgs a) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (uint32_t p = gl; p < a.n; p += NL, s++) {
+        const Fp z = ld_vec(&a.in[p].z);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, fp_is_zero(z) ? fp_one() : z);
+    }
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = a.n > gl ? (int)((a.n - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        const uint32_t p = gl + (uint32_t)t * NL;
+        const G1J q = ld_vec(&a.in[p]);
+        const bool inf = fp_is_zero(q.z);
+        const Fp zi = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, inf ? fp_one() : q.z);
+        G1A r;
+        if (inf) {
+            r.x = fp_zero();
+            r.y = fp_zero();
+        } else {
+            const Fp z2 = fp_sqr(zi);
+            r.x = fp_mul(q.x, z2);
+            r.y = fp_mul(q.y, fp_mul(z2, zi));
+        }
+        st_vec(&a.out[p], r);
+    }
+}
+
 // normalise the ladder into `scratch`, then fold it into w.ladder_aff; returns the launches made
 int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) {
     const int n_lad = n * kCells * kDigits;
-    k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, scratch, n_lad);
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    NormArgs na;
+    na.in = w.ladder;
+    na.out = scratch;
+    na.pre = w.flat_pre;
+    na.others = w.flat_others;
+    na.tot = w.flat_tot;
+    na.totinv = w.flat_totinv;
+    na.slots_pre = w.flat_slots;
+    na.n = (uint32_t)n_lad;
+    k_norm_pass1<<<blocks, kFlatThreads, 0, s>>>(na);
+    k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(na.tot, na.totinv, warps);
+    k_norm_pass2<<<blocks, kFlatThreads, 0, s>>>(na);
     FoldArgs a;
     a.lad = scratch;
     a.out = w.ladder_aff;
@@ -1469,11 +1532,10 @@ int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) 
     a.totinv = w.flat_totinv;
     a.slots_pre = w.flat_slots;
     a.n_blobs = n;
-    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     k_fold_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
     k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
     k_fold_pass2<<<blocks, kFlatThreads, 0, s>>>(a);
-    return 4;
+    return 6;
 }
 
 // ---------------------------------------------------------------- launcher

@@ -592,7 +592,7 @@ void take_comb(ProofWork &w, const ProofWork &from) {
 // w.plan): 10 to ~45 launches, captured once per (chunk size, plan) into a CUDA
 // graph and replayed with one cudaGraphLaunch.  Launched directly while stage
 // timing is on, for sizes beyond the cache (kMaxGraphs), or when $VKZG_GRAPHS=0.
-constexpr size_t kMaxGraphs = 24;
+constexpr size_t kMaxGraphs = 160; // every chunk size of a 128-blob serving lane, and then some
 
 cudaError_t run_proofs(vkzg_prover *p, const ProofWork &w, uint32_t n) {
     cudaStream_t s = p->stream;
@@ -1166,11 +1166,21 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
 }
 
 namespace vkzg {
-// dst takes src's tuned plans (provers of one serving loop share their decisions)
+// dst takes src's tuned plans (provers of one serving loop share their
+// decisions) and allocates what those plans need now, so that no later call
+// stops for a device allocation
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src) {
-    if (!dst || !src || dst == src) return;
+    if (!dst || !src) return;
     std::lock_guard<std::mutex> lock(dst->mutex);
-    for (const auto &kv : src->plan_of) dst->plan_of[kv.first] = kv.second;
+    if (cudaSetDevice(dst->device) != cudaSuccess) return;
+    bool want_comb = false, want_flat = false;
+    for (const auto &kv : src->plan_of) {
+        dst->plan_of[kv.first] = kv.second;
+        want_comb |= kv.second == 3;
+        want_flat |= kv.second == 4;
+    }
+    if (want_comb) ensure_comb(dst);
+    if (want_flat) ensure_flat_b(dst);
 }
 } // namespace vkzg
 
