@@ -69,3 +69,16 @@ def test_plans_agree_and_tuner_times_plan3(monkeypatch):
         assert np.array_equal(out, outs[0])
         q.autotune(16)
         assert q.digit_table()[1] == p.digit_table()[1]  # same table object: same build record
+
+
+def test_plan3_without_digit_table_falls_back(golden_proofs, monkeypatch):
+    """With the digit table disabled ($VKZG_COMB_BITS=0, as when it cannot be
+    allocated) a forced plan 3 runs as plan 4 and still proves the vectors."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.setenv("VKZG_PLAN", "3")
+    monkeypatch.setenv("VKZG_COMB_BITS", "0")
+    n = len(golden_proofs["valid_names"])
+    with vkzg_b200.Prover(max_batch_size=n) as p:
+        out = p.compute_cell_kzg_proofs_batch(golden_proofs["valid_blobs"].tobytes(), n)
+        assert p.digit_table() is None
+    assert out == golden_proofs["valid_proofs"].tobytes()
