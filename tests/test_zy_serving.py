@@ -60,3 +60,24 @@ def test_mix_equals_alone(golden_proofs, golden_recover):
         assert np.array_equal(big.reshape(20, 6144), alone_proofs[:20])
         st = srv.stats()
         assert st["requests"] == len(reqs) + 2 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_mix_equals_alone_digit_table_lanes():
+    """Batches of up to 32 blobs: the lanes run the digit-table plan (chosen by
+    the server's tuning) and share one table; every request's proofs equal the
+    direct call's."""
+    from conftest import random_blobs
+    rng = np.random.default_rng(57)
+    blobs = random_blobs(64, 1234)
+    with vkzg_b200.Prover(max_batch_size=64) as p:
+        alone = np.frombuffer(p.compute_cell_kzg_proofs_batch(blobs.tobytes(), 64), np.uint8).reshape(64, 6144)
+    with vkzg_b200.Server(max_blobs_per_batch=32, lanes=2) as srv:
+        reqs = []
+        for _ in range(40):
+            n = int(rng.integers(1, 9))
+            s0 = int(rng.integers(0, 64 - n + 1))
+            out = np.zeros(n * 6144, np.uint8)
+            reqs.append((srv.submit_proofs(out, np.ascontiguousarray(blobs[s0:s0 + n]), n), s0, n, out))
+        for t, s0, n, out in reqs:
+            assert srv.wait(t) == 0
+            assert np.array_equal(out.reshape(n, 6144), alone[s0:s0 + n]), (s0, n)
