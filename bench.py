@@ -10,10 +10,16 @@ patterns.  value = blobs per second through both entry points
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The line also carries the same step through the public C ABI with host
+buffers (e2e), the one-call-per-blob form, a served mixed stream with latency
+percentiles, the phase-A roofline, the CPU oracle's rate and the clocks.
+
 --impl reference times the CPU restatement of the reference's algorithm on the
-host cores (the reference itself is Vulkan/GLSL and cannot run on this machine;
-see DESIGN.md).  Under torchrun (N > 1) every rank runs an independent replica
-(blobs are independent; no collective on the data path) and rank 0 prints.
+host cores (the reference itself is Vulkan/GLSL and has no CPU path; no Vulkan
+driver or software renderer is available here).  Under torchrun (N > 1) every
+rank runs an independent replica (blobs are independent; no collective on the
+data path) and rank 0 prints.
+--profile-case [proofs|recovery] runs a small untimed case for ncu captures.
 """
 import argparse
 import json
