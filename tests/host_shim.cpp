@@ -13,6 +13,16 @@ void shim_fp_mul(const uint32_t *a, const uint32_t *b, uint32_t *r) {
     memcpy(y.v, b, 48);
     memcpy(r, fp_mul(x, y).v, 48);
 }
+void shim_fp_mul_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<12>(r, a, b); }
+void shim_fr_mul_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<8>(r, a, b); }
+void shim_fp_sqr_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    (void)b;
+    mont_sqr_ks<12>(r, a);
+}
+void shim_fr_sqr_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    (void)b;
+    mont_sqr_ks<8>(r, a);
+}
 void shim_fp_sqr(const uint32_t *a, const uint32_t *b, uint32_t *r) {
     (void)b;
     Fp x;

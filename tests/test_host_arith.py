@@ -38,13 +38,21 @@ def test_field_ops(shim, field):
     edge = [0, 1, 2, mod - 1, mod - 2, radix % mod, radix * radix % mod, mod // 2, (mod + 1) // 2,
             (1 << top) - 1, mod - (1 << 32), mod - (1 << 200) - 1, ((1 << top) - 1) ^ (0xFFFF << 64)]
     edge += [mod - 1 - rng.randrange(1 << 64) for _ in range(50)]  # long runs of high words
+    half = 16 * n  # Karatsuba halves: equal, one apart, all-ones low half
+    edge += [(x << half) | x for x in (1, (1 << (top - half)) - 1, rng.randrange(1 << (top - half)))]
+    edge += [(x << half) | (x + 1) for x in (0, rng.randrange(1 << (top - half)))]
+    edge += [(x << half) | ((1 << half) - 1) for x in (0, 1, (1 << (top - half)) - 1)]
     vals = edge + [rng.randrange(mod) for _ in range(2000)]
     out = (ctypes.c_uint32 * n)()
     for k, a in enumerate(vals):
         b = vals[(7 * k + 3) % len(vals)]
         getattr(shim, f"shim_{field}_mul")(words(a, n), words(b, n), out)
         assert value(out, n) == a * b * rinv % mod
+        getattr(shim, f"shim_{field}_mul_ks")(words(a, n), words(b, n), out)
+        assert value(out, n) == a * b * rinv % mod
         getattr(shim, f"shim_{field}_sqr")(words(a, n), words(b, n), out)
+        assert value(out, n) == a * a * rinv % mod
+        getattr(shim, f"shim_{field}_sqr_ks")(words(a, n), words(b, n), out)
         assert value(out, n) == a * a * rinv % mod
         getattr(shim, f"shim_{field}_add")(words(a, n), words(b, n), out)
         assert value(out, n) == (a + b) % mod

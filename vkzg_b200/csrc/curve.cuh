@@ -58,7 +58,11 @@ VK_HD G1J g1_dbl(const G1J &p) {
 // sequential calls.  For latency-bound chains of doublings (the ladder).
 VK_HD Fp fp_mul_inl(const Fp &a, const Fp &b) {
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_mul_ks<12>(r.v, a.v, b.v);
+#else
     mont_mul<12>(r.v, a.v, b.v);
+#endif
     return r;
 }
 VK_HD Fp fp_sqr_inl(const Fp &a) {

@@ -28,27 +28,59 @@ __global__ void __launch_bounds__(256) k_probe_imad(uint32_t seed, uint32_t *sin
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
-// independent Fp products per thread (2 chains)
+__device__ __noinline__ Fp fp_mul_ks_call(Fp a, Fp b) {
+    Fp r;
+    mont_mul_ks<12>(r.v, a.v, b.v);
+    return r;
+}
+
+__device__ __noinline__ Fp fp_sqr_ks_call(Fp a) {
+    Fp r;
+    mont_sqr_ks<12>(r.v, a.v);
+    return r;
+}
+
+// independent Fp products per thread (2 chains); OP 0: fp_mul, 1: fp_sqr, 2: the
+// Karatsuba product, 3: the Karatsuba square
+template <int OP>
 __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint32_t *sink) {
     Fp a = fp_one(), b = fp_one();
     a.v[0] ^= seed + threadIdx.x;
     b.v[1] ^= seed * 3u + blockIdx.x;
     const Fp c = a;
     for (int i = 0; i < iters; i++) {
-        a = fp_mul(a, c);
-        b = fp_mul(b, c);
+        if (OP == 0) {
+            a = fp_mul(a, c);
+            b = fp_mul(b, c);
+        } else if (OP == 1) {
+            a = fp_sqr(a);
+            b = fp_sqr(b);
+        } else if (OP == 2) {
+            a = fp_mul_ks_call(a, c);
+            b = fp_mul_ks_call(b, c);
+        } else {
+            a = fp_sqr_ks_call(a);
+            b = fp_sqr_ks_call(b);
+        }
     }
     if ((a.v[0] ^ b.v[0]) == 0x12345678u) sink[0] = a.v[1];
 }
 
+// OP 0: fr_mul (CIOS), 1: the Karatsuba product
+template <int OP>
 __global__ void __launch_bounds__(256) k_probe_fr(uint32_t seed, int iters, uint32_t *sink) {
     Fr a = fr_one(), b = fr_one();
     a.v[0] ^= seed + threadIdx.x;
     b.v[1] ^= seed * 3u + blockIdx.x;
     const Fr c = a;
     for (int i = 0; i < iters; i++) {
-        a = fr_mul(a, c);
-        b = fr_mul(b, c);
+        if (OP == 0) {
+            a = fr_mul(a, c);
+            b = fr_mul(b, c);
+        } else {
+            mont_mul_ks<8>(a.v, a.v, c.v);
+            mont_mul_ks<8>(b.v, b.v, c.v);
+        }
     }
     if ((a.v[0] ^ b.v[0]) == 0x12345678u) sink[0] = a.v[1];
 }
@@ -178,7 +210,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 2) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 6) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -197,13 +229,17 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
             const int blocks = sms * 8;
             k_probe_imad<<<blocks, 256>>>(rep + 1, sink);
             ops = (double)blocks * 256 * 8 * kProbeIters;
-        } else if (which == 1) {
+        } else if (which != 2 && which != 5) {
             const int blocks = sms * 4;
-            k_probe_fp<<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            if (which == 1) k_probe_fp<0><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 3) k_probe_fp<1><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 4) k_probe_fp<2><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else k_probe_fp<3><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             ops = (double)blocks * 128 * 2 * fp_iters;
         } else {
             const int blocks = sms * 8;
-            k_probe_fr<<<blocks, 256>>>(rep + 1, fr_iters, sink);
+            if (which == 2) k_probe_fr<0><<<blocks, 256>>>(rep + 1, fr_iters, sink);
+            else k_probe_fr<1><<<blocks, 256>>>(rep + 1, fr_iters, sink);
             ops = (double)blocks * 256 * 2 * fr_iters;
         }
         cudaEventRecord(e1);

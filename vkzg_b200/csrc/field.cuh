@@ -3,11 +3,13 @@
 // R = 2^384 / 2^256.  The memory image of a value is identical to the
 // reference's (src/shaders/field.glsl.inc:1-4), so its setup tables load as-is.
 //
-// Multiplication is word-serial Montgomery (CIOS).  On the device it is a PTX
-// carry chain: each 32x32 partial product is one mad.lo.cc / madc.hi.cc, with
-// the even-index and odd-index products of a row on two separate chains
-// (their 64-bit results never overlap, so a row is two passes of n
-// instructions instead of n wide multiplies plus carry fix-ups).  The same
+// Multiplication is Montgomery: word-serial (CIOS) for Fr, and for Fp one
+// Karatsuba level over 6-word halves followed by a separated word-by-word
+// reduction.  On the device every product row is a PTX carry chain: each 32x32
+// partial product is one mad.lo.cc / madc.hi.cc, with the even-index and
+// odd-index products of a row on two separate chains (their 64-bit results
+// never overlap, so a row is two passes of n instructions instead of n wide
+// multiplies plus carry fix-ups).  The same
 // code compiles for the host with the carry flag emulated in a local
 // variable, which is how the CPU tests check the exact instruction sequence
 // against the oracle.
@@ -241,14 +243,14 @@ VK_HD void mont_mul(uint32_t *r, const uint32_t *a, const uint32_t *b) {
     for (int i = 0; i < N; i++) r[i] = borrow ? t[i] : s[i];
 }
 
-// Montgomery square a^2 / R mod m: the cross products a_i a_j (i < j) once,
-// doubled by a shift, plus the diagonal, then word-by-word reduction of the
-// 2n-word square (separated operand scanning).  n(n-1) + 2n + 2n^2 + n
-// multiply instructions against 4n^2 + n for mont_mul(a, a); same result.
 template <int N>
-VK_HD void mont_sqr(uint32_t *r, const uint32_t *a) {
+VK_HD void sos_reduce(uint32_t *r, uint32_t *T);
+
+// T (2n words) = a^2: the cross products a_i a_j (i < j) once, doubled by a
+// shift, plus the diagonal; n(n-1) + 2n multiply instructions.
+template <int N>
+VK_HD void sqr_words(uint32_t *T, const uint32_t *a) {
     CARRY_DECL
-    uint32_t T[2 * N];
 #pragma unroll
     for (int i = 0; i < 2 * N; i++) T[i] = 0;
     // Row i adds a_i a_j (j > i) at T[i + j] in two chains of disjoint word
@@ -288,9 +290,25 @@ VK_HD void mont_sqr(uint32_t *r, const uint32_t *a) {
     }
     MADC_LO_CC(T[2 * N - 2], a[N - 1], a[N - 1], T[2 * N - 2]);
     MADC_HI(T[2 * N - 1], a[N - 1], a[N - 1], T[2 * N - 1]);
-    // reduction: row i clears T[i] with q m 2^(32 i); its carry out of T[i + n]
-    // is owed to T[i + n + 1] and added by row i + 1 (the last row owes none:
-    // a^2 + q m < m^2 + R m < R^2)
+}
+
+// Montgomery square a^2 / R mod m: sqr_words, then word-by-word reduction of
+// the 2n-word square (separated operand scanning).  n(n-1) + 2n + 2n^2 + n
+// multiply instructions against 4n^2 + n for mont_mul(a, a); same result.
+template <int N>
+VK_HD void mont_sqr(uint32_t *r, const uint32_t *a) {
+    uint32_t T[2 * N];
+    sqr_words<N>(T, a);
+    sos_reduce<N>(r, T);
+}
+
+// r = T / R mod m for a 2n-word T < m R (separated operand scanning): row i
+// clears T[i] with q m 2^(32 i); its carry out of T[i + n] is owed to
+// T[i + n + 1] and added by row i + 1 (the last row owes none: T + q m <
+// m R + R m < R^2).  T is clobbered.
+template <int N>
+VK_HD void sos_reduce(uint32_t *r, uint32_t *T) {
+    CARRY_DECL
     uint32_t owed = 0;
 #pragma unroll
     for (int i = 0; i < N; i++) {
@@ -326,6 +344,131 @@ VK_HD void mont_sqr(uint32_t *r, const uint32_t *a) {
     for (int i = 0; i < N; i++) r[i] = borrow ? T[N + i] : s[i];
 }
 
+// z (2h words) = x y (h words each), one row per y_i in an even and an odd
+// chain of disjoint word pairs.  After row i the partial product is below
+// 2^(32(h + i + 1)), so neither chain carries out of word i + h.
+template <int H>
+VK_HD void mul_words(uint32_t *z, const uint32_t *x, const uint32_t *y) {
+    CARRY_DECL
+#pragma unroll
+    for (int i = 0; i < 2 * H; i++) z[i] = 0;
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+        const uint32_t yi = y[i];
+        MAD_LO_CC(z[i], x[0], yi, z[i]);
+        MADC_HI_CC(z[i + 1], x[0], yi, z[i + 1]);
+#pragma unroll
+        for (int j = 2; j < H; j += 2) {
+            MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+            MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+        }
+        ADDC(z[i + H], z[i + H], 0u);
+        MAD_LO_CC(z[i + 1], x[1], yi, z[i + 1]);
+        MADC_HI_CC(z[i + 2], x[1], yi, z[i + 2]);
+#pragma unroll
+        for (int j = 3; j < H - 1; j += 2) {
+            MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+            MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+        }
+        MADC_LO_CC(z[i + H - 1], x[H - 1], yi, z[i + H - 1]);
+        MADC_HI(z[i + H], x[H - 1], yi, z[i + H]);
+    }
+}
+
+// Montgomery product through one Karatsuba level (n even, h = n/2):
+// a b = a0 b0 + (a0 b1 + a1 b0) 2^(32h) + a1 b1 2^(32n), with the middle term
+// a0 b0 + a1 b1 + (a0 - a1)(b1 - b0) taken from |a0 - a1| |b1 - b0| and the
+// sign of the factors.  3 h^2 word products instead of n^2, then the same
+// reduction as mont_sqr; the same bounds as mont_mul (a b < m R).
+template <int N>
+VK_HD void mont_mul_ks(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+    static_assert(N % 2 == 0 && N >= 8, "even word count");
+    constexpr int H = N / 2;
+    CARRY_DECL
+    uint32_t T[2 * N];
+    mul_words<H>(T, a, b);
+    mul_words<H>(T + N, a + H, b + H);
+    // da = |a0 - a1|, db = |b1 - b0|: the difference, then (t ^ mask) - mask,
+    // which negates it when the subtraction borrowed (mask all ones)
+    uint32_t da[H], db[H], ma, mb;
+    SUB_CC(da[0], a[0], a[H]);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(da[i], a[i], a[H + i]);
+    SUBC(ma, 0u, 0u);
+    SUB_CC(da[0], da[0] ^ ma, ma);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(da[i], da[i] ^ ma, ma);
+    SUB_CC(db[0], b[H], b[0]);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(db[i], b[H + i], b[i]);
+    SUBC(mb, 0u, 0u);
+    SUB_CC(db[0], db[0] ^ mb, mb);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(db[i], db[i] ^ mb, mb);
+    uint32_t M[N];
+    mul_words<H>(M, da, db);
+    // mid = a0 b0 + a1 b1 +- M in n + 1 words (it equals a0 b1 + a1 b0 < 2^(32n + 1));
+    // -M is (M ^ s) + 1 with s all ones, the + 1 entering as the carry of s + 1
+    const uint32_t s = ma ^ mb;
+    uint32_t mid[N + 1], dummy;
+    ADD_CC(mid[0], T[0], T[N]);
+#pragma unroll
+    for (int i = 1; i < N; i++) ADDC_CC(mid[i], T[i], T[N + i]);
+    ADDC(mid[N], 0u, 0u);
+    ADD_CC(dummy, s, 1u);
+#pragma unroll
+    for (int i = 0; i < N; i++) ADDC_CC(mid[i], mid[i], M[i] ^ s);
+    ADDC(mid[N], mid[N], s);
+    (void)dummy;
+    // T += mid 2^(32h); the full product is below 2^(64n), so the last word takes no carry out
+    ADD_CC(T[H], T[H], mid[0]);
+#pragma unroll
+    for (int i = 1; i <= N; i++) ADDC_CC(T[H + i], T[H + i], mid[i]);
+#pragma unroll
+    for (int k = H + N + 1; k < 2 * N - 1; k++) ADDC_CC(T[k], T[k], 0u);
+    ADDC(T[2 * N - 1], T[2 * N - 1], 0u);
+    sos_reduce<N>(r, T);
+}
+
+// Montgomery square through one Karatsuba level: a^2 = a0^2 + 2 a0 a1 2^(32h)
+// + a1^2 2^(32n) with 2 a0 a1 = a0^2 + a1^2 - (a0 - a1)^2, three h-word squares.
+template <int N>
+VK_HD void mont_sqr_ks(uint32_t *r, const uint32_t *a) {
+    static_assert(N % 2 == 0 && N >= 8, "even word count");
+    constexpr int H = N / 2;
+    CARRY_DECL
+    uint32_t T[2 * N];
+    sqr_words<H>(T, a);
+    sqr_words<H>(T + N, a + H);
+    uint32_t d[H], md;
+    SUB_CC(d[0], a[0], a[H]);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(d[i], a[i], a[H + i]);
+    SUBC(md, 0u, 0u);
+    SUB_CC(d[0], d[0] ^ md, md);
+#pragma unroll
+    for (int i = 1; i < H; i++) SUBC_CC(d[i], d[i] ^ md, md);
+    uint32_t M[N];
+    sqr_words<H>(M, d);
+    // mid = a0^2 + a1^2 - M in n + 1 words (it equals 2 a0 a1 < 2^(32n + 1))
+    uint32_t mid[N + 1];
+    ADD_CC(mid[0], T[0], T[N]);
+#pragma unroll
+    for (int i = 1; i < N; i++) ADDC_CC(mid[i], T[i], T[N + i]);
+    ADDC(mid[N], 0u, 0u);
+    SUB_CC(mid[0], mid[0], M[0]);
+#pragma unroll
+    for (int i = 1; i < N; i++) SUBC_CC(mid[i], mid[i], M[i]);
+    SUBC(mid[N], mid[N], 0u);
+    ADD_CC(T[H], T[H], mid[0]);
+#pragma unroll
+    for (int i = 1; i <= N; i++) ADDC_CC(T[H + i], T[H + i], mid[i]);
+#pragma unroll
+    for (int k = H + N + 1; k < 2 * N - 1; k++) ADDC_CC(T[k], T[k], 0u);
+    ADDC(T[2 * N - 1], T[2 * N - 1], 0u);
+    sos_reduce<N>(r, T);
+}
+
 template <int N>
 VK_HD bool limbs_is_zero(const uint32_t *a) {
     uint32_t acc = 0;
@@ -356,10 +499,20 @@ VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
 #ifndef VKZG_FP_INLINE
 #define VKZG_FP_INLINE 0
 #endif
+// The 12-limb product goes through one Karatsuba level (mont_mul_ks): 516
+// multiply instructions against 588 for CIOS, about 9% more products per second
+// on the integer pipe; VKZG_FP_KARATSUBA=0 selects CIOS.
+#ifndef VKZG_FP_KARATSUBA
+#define VKZG_FP_KARATSUBA 1
+#endif
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_mul_call(Fp a, Fp b) {
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_mul_ks<12>(r.v, a.v, b.v);
+#else
     mont_mul<12>(r.v, a.v, b.v);
+#endif
     return r;
 }
 #endif
@@ -368,7 +521,11 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
     return fp_mul_call(a, b);
 #else
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_mul_ks<12>(r.v, a.v, b.v);
+#else
     mont_mul<12>(r.v, a.v, b.v);
+#endif
     return r;
 #endif
 }
