@@ -122,8 +122,27 @@ int shim_g1_mul(const uint8_t *p48, const uint32_t *k, uint8_t *out48) {
 }
 }
 
+#include "../vkzg_b200/csrc/glv.h"
 #include "../vkzg_b200/csrc/inverse.cuh"
 extern "C" {
+// compressed P -> compressed phi(P)
+int shim_g1_phi(const uint8_t *p48, uint8_t *out48) {
+    G1A p;
+    if (!g1_decompress(p, p48)) return -1;
+    g1_compress(out48, g1_phi(p));
+    return 0;
+}
+// k (8 LE words, < r) -> the two halves as 4 LE words each, signs, and their
+// 16 signed digits each; returns 0 when the digits hold both halves
+int shim_glv_split(const uint32_t *k, uint32_t *mag8, int *neg2, int *dig32) {
+    const GlvSplit s = glv_split(k);
+    for (int h = 0; h < 2; h++) {
+        for (int i = 0; i < 4; i++) mag8[4 * h + i] = (uint32_t)(s.mag[h] >> (32 * i));
+        neg2[h] = s.neg[h];
+        if (!glv_digits(s.mag[h], s.neg[h], dig32 + kGlvDigits * h)) return -1;
+    }
+    return 0;
+}
 void shim_fp_inv_fast(const uint32_t *a, uint32_t *r) {
     Fp x;
     memcpy(x.v, a, 48);

@@ -107,3 +107,36 @@ def test_divstep_inverse(shim, field):
         assert value(out, n) == pow(x, -1, mod) * radix % mod, hex(x)
     fn(words(0, n), out)
     assert value(out, n) == 0
+
+
+Z2 = 0xD201000000010000 ** 2
+
+
+def test_endomorphism_and_tap_split(shim, oracle, mainnet_setup):
+    """phi(x, y) = (beta x, y) equals (-z^2) P on setup points, and the tap split
+    k = k1 + k2 z^2 (mod r) with both halves in 16 signed base-256 digits, which
+    the proof ladder relies on."""
+    lam = (-Z2) % R_MOD
+    pts = [bytes(mainnet_setup[48 * i:48 * i + 48]) for i in (0, 1, 2, 4095)]
+    for p in pts:
+        o = ctypes.create_string_buffer(48)
+        assert shim.shim_g1_phi(p, o) == 0
+        _, want = oracle.g1_mul(p, lam.to_bytes(32, "big"))
+        assert o.raw == want
+    rng = random.Random(13)
+    ks = [0, 1, 2, R_MOD - 1, R_MOD - 2, Z2 - 1, Z2, Z2 + 1, Z2 // 2, Z2 // 2 + 1, Z2 * (Z2 // 2),
+          Z2 * (Z2 // 2 + 1), Z2 * (Z2 // 2 + 1) + Z2 // 2 + 1, (Z2 - 1) * Z2 + Z2 - 1, R_MOD // 2]
+    ks += [rng.randrange(R_MOD) for _ in range(3000)]
+    mag = (ctypes.c_uint32 * 8)()
+    neg = (ctypes.c_int * 2)()
+    dig = (ctypes.c_int * 32)()
+    for k in ks:
+        k %= R_MOD
+        assert shim.shim_glv_split(words(k, 8), mag, neg, dig) == 0, hex(k)
+        m1, m2 = value(mag, 4), sum(mag[4 + i] << (32 * i) for i in range(4))
+        c1, c2 = (-m1 if neg[0] else m1), (-m2 if neg[1] else m2)
+        assert max(m1, m2) <= Z2 // 2 + 1
+        assert (c1 + c2 * lam - k) % R_MOD == 0, hex(k)
+        assert sum(dig[d] << (8 * d) for d in range(16)) == c1
+        assert sum(dig[16 + d] << (8 * d) for d in range(16)) == c2
+        assert all(-128 <= v <= 128 for v in dig)

@@ -26,6 +26,19 @@ VK_HD G1J g1_identity() {
 VK_HD bool g1a_is_identity(const G1A &p) { return fp_is_zero(p.x) && fp_is_zero(p.y); }
 VK_HD bool g1j_is_identity(const G1J &p) { return fp_is_zero(p.z); }
 
+// The order-3 endomorphism phi(x, y) = (beta x, y), beta the cube root of unity
+// 0x5f19672fdf76ce51ba69c6076a0f77eaddb3a93be6f89688de17d813620a00022e01fffffffefffe
+// (here in Montgomery form).  On G1, phi(P) = -z^2 P with z = -0xd201000000010000
+// the curve parameter; (0, 0) stays (0, 0).
+VK_HD G1A g1_phi(const G1A &p) {
+    const Fp beta = {{0x798a64e8u, 0x30f1361bu, 0x7ece5a2au, 0xf3b8ddabu, 0xc61577f7u, 0x16a8ca3au,
+                      0x74fd029bu, 0xc26a2ff8u, 0x60701c6eu, 0x3636b766u, 0x241b6160u, 0x051ba4abu}};
+    G1A r;
+    r.x = fp_mul(beta, p.x);
+    r.y = p.y;
+    return r;
+}
+
 VK_HD G1J g1_from_affine(const G1A &a) {
     if (g1a_is_identity(a)) return g1_identity();
     G1J r;

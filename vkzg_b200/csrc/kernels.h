@@ -17,6 +17,7 @@ constexpr int kExtElems = 8192;
 constexpr int kCells = 128;        // cells per blob = proofs per blob = circulant size
 constexpr int kCellElems = 64;     // field elements per cell = terms per phase-A output
 constexpr int kDigits = 32;        // signed 8-bit windows per scalar
+constexpr int kLadderDigits = 16;  // doubled ladder rows; phase B reads slots d >= 16 as phi images
 constexpr int kBuckets = 128;      // |digit| in 1..128
 constexpr int kHalf = 64;
 constexpr size_t kBlobBytes = 131072;
@@ -63,9 +64,9 @@ struct ProofWork {
     Fr *scalars = nullptr;      // [cap][128 j][64 i] canonical
     G1J *buckets = nullptr;     // [cap][128][128]
     G1J *points = nullptr;      // [cap][128] reduce outputs
-    G1J *ladder = nullptr;      // [cap][128][32]
-    G1J *folded = nullptr;      // [cap][128][32]
-    G1A *ladder_aff = nullptr;  // [cap][128][32]
+    G1J *ladder = nullptr;      // [cap][128][16] 2^(8d) u[j]
+    G1J *folded = nullptr;      // [cap][128][16] (plans 0-2; plans 3-4 use it as affine scratch)
+    G1A *ladder_aff = nullptr;  // [cap][128][32]: d < 16 the folded ladder, d >= 16 its phi images
     uint8_t *proofs = nullptr;  // [cap][128][48]
     uint32_t *err = nullptr;    // [cap]
     // batch-affine accumulation (plans 1, 2)

@@ -8,9 +8,11 @@
 //                        shared memory, fixed-base bucket accumulation over the
 //                        position table                     (k_phase_a_sort, k_phase_a)
 //   4 k_reduce           sum_k k * B_k, 8 lanes per output  (k_bucket_reduce)
-//   5 k_ladder           L[j][d] = 2^(8d) u[j]              (k_ladder)
+//   5 k_ladder           L[j][d] = 2^(8d) u[j], d < 16      (k_ladder, d < 32: the
+//                        taps are split as k1 + k2 z^2 and slots 16..31 read phi(L))
 //   6 k_fold             L+- = L[j] +- L[j+64]              (k_fold_ladder)
-//   7 k_normalize        Jacobian -> affine, block batch inversion (k_normalize)
+//   7 k_normalize        Jacobian -> affine, block batch inversion, phi images
+//                                                           (k_normalize)
 //   8 k_phase_b          split-circulant bucket MSM with the fixed taps (k_phase_b_split)
 //   4'k_reduce
 //   9 k_finish           combine C+ +- C-, normalise, compress, write slot brev7(a)
@@ -200,10 +202,10 @@ __global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= n_points) return;
     G1J acc = ld_vec(&u[gid]);
-    G1J *dst = ladder + (size_t)gid * kDigits;
-    for (int d = 0; d < kDigits; d++) {
+    G1J *dst = ladder + (size_t)gid * kLadderDigits;
+    for (int d = 0; d < kLadderDigits; d++) {
         st_vec(&dst[d], acc);
-        if (d + 1 < kDigits)
+        if (d + 1 < kLadderDigits)
 #pragma unroll 1
             for (int q = 0; q < 8; q++) acc = g1_dbl_inl(acc);
     }
@@ -212,14 +214,14 @@ __global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *
 // ---------------------------------------------------------------- stage 6
 __global__ void __launch_bounds__(128) k_fold(const G1J *__restrict__ ladder, G1J *folded, int n_blobs) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= n_blobs * kHalf * kDigits) return;
-    const int b = gid / (kHalf * kDigits), r = gid % (kHalf * kDigits);
-    const int j = r / kDigits, d = r % kDigits;
-    const size_t base = (size_t)b * kCells * kDigits;
-    const G1J a = ld_vec(&ladder[base + j * kDigits + d]);
-    const G1J c = ld_vec(&ladder[base + (j + kHalf) * kDigits + d]);
-    st_vec(&folded[base + j * kDigits + d], g1_add(a, c));
-    st_vec(&folded[base + (j + kHalf) * kDigits + d], g1_sub(a, c));
+    if (gid >= n_blobs * kHalf * kLadderDigits) return;
+    const int b = gid / (kHalf * kLadderDigits), r = gid % (kHalf * kLadderDigits);
+    const int j = r / kLadderDigits, d = r % kLadderDigits;
+    const size_t base = (size_t)b * kCells * kLadderDigits;
+    const G1J a = ld_vec(&ladder[base + j * kLadderDigits + d]);
+    const G1J c = ld_vec(&ladder[base + (j + kHalf) * kLadderDigits + d]);
+    st_vec(&folded[base + j * kLadderDigits + d], g1_add(a, c));
+    st_vec(&folded[base + (j + kHalf) * kLadderDigits + d], g1_sub(a, c));
 }
 
 // ---------------------------------------------------------------- stage 7
@@ -240,7 +242,10 @@ __global__ void __launch_bounds__(kNormThreads) k_normalize(const G1J *__restric
         a.x = fp_mul(p.x, z2);
         a.y = fp_mul(p.y, fp_mul(z2, zi));
     }
-    st_vec(&out[gid], a);
+    // in: [row][16] folded ladder; out: [row][32], slot 16 + d = phi(slot d)
+    const size_t dst = (size_t)(gid / kLadderDigits) * kDigits + gid % kLadderDigits;
+    st_vec(&out[dst], a);
+    st_vec(&out[dst + kLadderDigits], g1_phi(a));
 }
 
 // ---------------------------------------------------------------- stage 8
@@ -1400,8 +1405,8 @@ int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_o
 // by a normalisation of the results.  Pair q = ((blob * 64 + j) * 32 + d) * 2 +
 // sign writes folded[blob][sign * 64 + j][d].
 struct FoldArgs {
-    const G1A *lad;  // [blob][128][32] normalised ladder
-    G1A *out;        // [blob][128][32]: plus half, then minus half
+    const G1A *lad;  // [blob][128][16] normalised ladder
+    G1A *out;        // [blob][128][32]: plus half, then minus half; slot 16 + d = phi(slot d)
     uint32_t *pre;
     Fp *others, *tot, *totinv;
     size_t slots_pre;
@@ -1411,19 +1416,19 @@ struct FoldArgs {
 __device__ __forceinline__ void fold_pair(const FoldArgs &a, size_t q, G1A &x, G1A &y, size_t &dst) {
     const int sign = (int)(q & 1);
     const size_t r = q >> 1;
-    const size_t b = r / (kHalf * kDigits), jd = r % (kHalf * kDigits);
-    const size_t j = jd / kDigits, d = jd % kDigits;
-    const size_t base = b * kCells * kDigits;
-    x = ld_vec(&a.lad[base + j * kDigits + d]);
-    y = ld_vec(&a.lad[base + (j + kHalf) * kDigits + d]);
+    const size_t b = r / (kHalf * kLadderDigits), jd = r % (kHalf * kLadderDigits);
+    const size_t j = jd / kLadderDigits, d = jd % kLadderDigits;
+    const size_t base = b * kCells * kLadderDigits;
+    x = ld_vec(&a.lad[base + j * kLadderDigits + d]);
+    y = ld_vec(&a.lad[base + (j + kHalf) * kLadderDigits + d]);
     if (sign) y.y = fp_neg(y.y);
-    dst = base + (j + (sign ? kHalf : 0)) * kDigits + d;
+    dst = (b * kCells + j + (sign ? kHalf : 0)) * kDigits + d;
 }
 
 __global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass1(FoldArgs a) {
     const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
     const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * kDigits * 2;
+    const size_t P = (size_t)a.n_blobs * kHalf * kLadderDigits * 2;
     uint32_t *pre = a.pre + wg * a.slots_pre * 384;
     Fp acc = fp_one();
     int s = 0;
@@ -1440,7 +1445,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass1(FoldArgs a) {
 __global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass2(FoldArgs a) {
     const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
     const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * kDigits * 2;
+    const size_t P = (size_t)a.n_blobs * kHalf * kLadderDigits * 2;
     const uint32_t *pre = a.pre + wg * a.slots_pre * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
@@ -1452,7 +1457,9 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass2(FoldArgs a) {
         const Fp den = pair_denominator(x, y, kind);
         const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
         inv = fp_mul(inv, den);
-        st_vec(&a.out[dst], pair_result(x, y, kind, inv_den));
+        const G1A f = pair_result(x, y, kind, inv_den);
+        st_vec(&a.out[dst], f);
+        st_vec(&a.out[dst + kLadderDigits], g1_phi(f));
     }
 }
 
@@ -1509,7 +1516,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
 
 // normalise the ladder into `scratch`, then fold it into w.ladder_aff; returns the launches made
 int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) {
-    const int n_lad = n * kCells * kDigits;
+    const int n_lad = n * kCells * kLadderDigits;
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     NormArgs na;
     na.in = w.ladder;
@@ -1549,7 +1556,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     const size_t smem_ntt = (size_t)kBlobElems * sizeof(Fr);
     const int n_out = n * kCells;
     const int red_blocks = (n_out * kReduceLanes + kReduceThreads - 1) / kReduceThreads;
-    const int n_lad = n * kCells * kDigits;
+    const int n_lad = n * kCells * kLadderDigits;
     mark();
     k_blob_to_coeffs<<<n, kNttThreads, smem_ntt, s>>>(w.blobs, w.coeffs, t.roots_inv, t.inv_blob_r2, w.err);
     mark();
@@ -1593,7 +1600,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         launched += launch_fold_affine(w, n, reinterpret_cast<G1A *>(w.folded), s) - 2;
         mark();
     } else {
-        k_fold<<<(n * kHalf * kDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
+        k_fold<<<(n * kHalf * kLadderDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
         mark();
         k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
     }

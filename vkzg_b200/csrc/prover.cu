@@ -9,6 +9,7 @@
 #include "../../include/vkzg.h"
 #include "../../include/vkzg_b200.h"
 #include "device_util.cuh"
+#include "glv.h"
 #include "kernels.h"
 
 #include <dlfcn.h>
@@ -201,9 +202,13 @@ void host_roots(std::vector<Fr> &fwd, std::vector<Fr> &inv) {
 
 // Phase-B half taps c+-[e] = (c[e] +- c[e+64]) / 2, c[e] = (1/128) sum_{t<64} w_128^(e t),
 // recoded into signed base-256 digits and grouped by bucket (the reference's
-// kernel_items/offsets/perm tables, src/precomputed_tables.cpp:45-49).
-void host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2], uint32_t offsets[2][kBuckets + 1],
-                     uint32_t perm[2][kBuckets]) {
+// kernel_items/offsets/perm tables, src/precomputed_tables.cpp:45-49).  With
+// split_phi, each tap is k1 + k2 z^2 (glv.h): digit slots 0..15 hold k1's digits
+// (applied to 2^(8d) L), slots 16..31 the digits of -k2 (applied to 2^(8d) phi(L));
+// without it, the reference's 32 digits of the full tap (its tables file).
+// Returns false if a split does not fit its 16 digits (it always does).
+bool host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2], uint32_t offsets[2][kBuckets + 1],
+                     uint32_t perm[2][kBuckets], bool split_phi) {
     Fr c[kCells];
     const Fr inv128 = fr_inv(fr_from_u32(128)), inv2 = fr_inv(fr_from_u32(2));
     for (int e = 0; e < kCells; e++) {
@@ -217,17 +222,25 @@ void host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2],
         for (int e = 0; e < kHalf; e++) {
             const Fr tap = fr_mul(h == 0 ? fr_add(c[e], c[e + kHalf]) : fr_sub(c[e], c[e + kHalf]), inv2);
             const Fr can = fr_to_canonical(tap);
-            int carry = 0;
-            for (int d = 0; d < kDigits; d++) {
-                int v = (int)((can.v[d >> 2] >> ((d & 3) * 8)) & 0xffu) + carry;
-                carry = 0;
-                if (v > kBuckets) {
-                    v -= 2 * kBuckets;
-                    carry = 1;
+            if (split_phi) {
+                const GlvSplit sp = glv_split(can.v);
+                if (!glv_digits(sp.mag[0], sp.neg[0], dig[e]) ||
+                    !glv_digits(sp.mag[1], sp.neg[1], dig[e] + kGlvDigits))
+                    return false;
+            } else {
+                int carry = 0;
+                for (int d = 0; d < kDigits; d++) {
+                    int v = (int)((can.v[d >> 2] >> ((d & 3) * 8)) & 0xffu) + carry;
+                    carry = 0;
+                    if (v > kBuckets) {
+                        v -= 2 * kBuckets;
+                        carry = 1;
+                    }
+                    dig[e][d] = v;
                 }
-                dig[e][d] = v;
-                if (v) count[abs(v) - 1]++;
             }
+            for (int d = 0; d < kDigits; d++)
+                if (dig[e][d]) count[abs(dig[e][d]) - 1]++;
         }
         uint32_t acc = 0;
         for (int k = 0; k < kBuckets; k++) {
@@ -252,6 +265,7 @@ void host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2],
         });
         for (int k = 0; k < kBuckets; k++) perm[h][k] = (uint32_t)order[k];
     }
+    return true;
 }
 
 struct HostTables {
@@ -319,18 +333,24 @@ vkzg_result read_file(const std::string &path, std::vector<uint8_t> &out) {
         if ((call) != cudaSuccess) return VKZG_ERR_GPU;                                               \
     } while (0)
 
+// The device's phase-B tables are always the split ones, computed from the
+// roots (a tables file's own items are the reference's 32-digit recoding and
+// are kept only for writing the file back out).
 vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
     DeviceTables &t = p->t;
+    std::vector<uint32_t> items[2];
+    uint32_t offsets[2][kBuckets + 1], perm[2][kBuckets];
+    if (!host_tap_tables(h.roots_fwd, items, offsets, perm, true)) return VKZG_ERR_SETUP;
     if (!p->alloc(t.roots_fwd, kExtElems) || !p->alloc(t.roots_inv, kExtElems) || !p->alloc(t.shift_fwd, kExtElems) ||
         !p->alloc(t.shift_inv, kExtElems) || !p->alloc(t.inv_blob_r2, 1))
         return VKZG_ERR_MALLOC;
     for (int s = 0; s < 2; s++) {
-        if (!p->alloc(t.tap_items[s], std::max<size_t>(1, h.items[s].size())) || !p->alloc(t.tap_offsets[s], kBuckets + 1) ||
+        if (!p->alloc(t.tap_items[s], std::max<size_t>(1, items[s].size())) || !p->alloc(t.tap_offsets[s], kBuckets + 1) ||
             !p->alloc(t.tap_perm[s], kBuckets))
             return VKZG_ERR_MALLOC;
-        CK(cudaMemcpy(t.tap_items[s], h.items[s].data(), 4 * h.items[s].size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(t.tap_offsets[s], h.offsets[s], sizeof h.offsets[s], cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(t.tap_perm[s], h.perm[s], sizeof h.perm[s], cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.tap_items[s], items[s].data(), 4 * items[s].size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.tap_offsets[s], offsets[s], sizeof offsets[s], cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.tap_perm[s], perm[s], sizeof perm[s], cudaMemcpyHostToDevice));
     }
     CK(cudaMemcpy(t.roots_fwd, h.roots_fwd.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(t.roots_inv, h.roots_inv.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
@@ -338,7 +358,7 @@ vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
     // plan 3's phase-B round structure, from the tap offsets
     {
         std::unique_ptr<FlatBPlan> pl(new FlatBPlan);
-        if (build_flatb_plan(h.offsets, *pl) && pl->rounds > 0) {
+        if (build_flatb_plan(offsets, *pl) && pl->rounds > 0) {
             if (!p->alloc(t.fb_plan, 1)) return VKZG_ERR_MALLOC;
             CK(cudaMemcpy(t.fb_plan, pl.get(), sizeof(FlatBPlan), cudaMemcpyHostToDevice));
             t.fb_rounds = pl->rounds;
@@ -392,7 +412,7 @@ vkzg_result generate_position_table(vkzg_prover *p, const std::vector<uint8_t> &
 
 void computed_small_tables(HostTables &h) {
     host_roots(h.roots_fwd, h.roots_inv);
-    host_tap_tables(h.roots_fwd, h.items, h.offsets, h.perm);
+    host_tap_tables(h.roots_fwd, h.items, h.offsets, h.perm, false);
     h.inv_blob = fr_inv(fr_from_u32(kBlobElems));
 }
 
