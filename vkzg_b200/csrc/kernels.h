@@ -25,21 +25,51 @@ constexpr size_t kProofBytes = 48;
 constexpr size_t kCellBytes = 2048;
 constexpr size_t kPositionPoints = (size_t)kCells * kCellElems * kDigits; // 262144
 
+// Phase B's convolution parts.  The 128-point cyclic convolution of a blob's
+// u[j] with the fixed taps is split by `levels` radix-2 folds (points
+// v[j] +- v[j + m], taps (t[e] +- t[e + m]) / 2): one cyclic part of
+// 128 >> levels points at slots [0, 128 >> levels) and, for each level l, a
+// negacyclic part of 128 >> l points at slots [128 >> l, 128 >> (l - 1)).
+// Plans 0-2 use one level (the two halves); plans 3-4 kPartLevels.
+constexpr int kFBMaxParts = 4;
+constexpr int kPartLevels = 2;
+struct PartLayout {
+    int n;                          // levels + 1
+    uint32_t size[kFBMaxParts];     // outputs = points = taps of the part
+    uint32_t off[kFBMaxParts];      // first slot; its tap items start at item 32 * off
+    uint32_t nega[kFBMaxParts];     // 1: negacyclic
+};
+inline PartLayout part_layout(int levels) {
+    PartLayout L{};
+    L.n = levels + 1;
+    L.size[0] = (uint32_t)kCells >> levels;
+    L.off[0] = 0;
+    L.nega[0] = 0;
+    for (int q = 1; q <= levels; q++) {
+        const int l = levels + 1 - q;
+        L.size[q] = (uint32_t)kCells >> l;
+        L.off[q] = (uint32_t)kCells >> l;
+        L.nega[q] = 1;
+    }
+    return L;
+}
+
 // Round structure of plan 3's phase B (see build_flatb_plan): per round r and
-// half h (0: plus taps, 1: minus taps), each bucket's list length, element
-// offsets, pair offsets and odd buckets, identical for every output of a half.
+// part q, each bucket's list length, element offsets, pair offsets and odd
+// buckets, identical for every output of a part.
 constexpr int kFBMaxRounds = 12;
 struct FlatBPlan {
     int rounds;
-    uint32_t stride[kFBMaxRounds + 1];           // elements per output in round r's buffer
-    uint32_t pairs[kFBMaxRounds][2];             // pairs per output
-    uint32_t n_odd[kFBMaxRounds][2];
-    uint32_t cnt[kFBMaxRounds + 1][2][kBuckets];
-    uint32_t base[kFBMaxRounds + 1][2][kBuckets + 1];
-    uint32_t pscan[kFBMaxRounds][2][kBuckets + 1];
-    uint8_t odd[kFBMaxRounds][2][kBuckets];
+    PartLayout parts;
+    uint32_t stride[kFBMaxRounds + 1];                    // elements per output in round r's buffer
+    uint32_t pairs[kFBMaxRounds][kFBMaxParts];            // pairs per output
+    uint32_t n_odd[kFBMaxRounds][kFBMaxParts];
+    uint32_t cnt[kFBMaxRounds + 1][kFBMaxParts][kBuckets];
+    uint32_t base[kFBMaxRounds + 1][kFBMaxParts][kBuckets + 1];
+    uint32_t pscan[kFBMaxRounds][kFBMaxParts][kBuckets + 1];
+    uint8_t odd[kFBMaxRounds][kFBMaxParts][kBuckets];
 };
-bool build_flatb_plan(const uint32_t offsets[2][kBuckets + 1], FlatBPlan &plan);
+bool build_flatb_plan(const PartLayout &parts, const uint32_t offsets[][kBuckets + 1], FlatBPlan &plan);
 
 // Setup-derived device tables (immutable once built).
 struct DeviceTables {
@@ -52,6 +82,8 @@ struct DeviceTables {
     Fr *shift_fwd = nullptr;        // 7^k / 8192                (recovery)
     Fr *shift_inv = nullptr;        // 7^-k / 8192 / R           (recovery; output lands canonical)
     Fr *inv_blob_r2 = nullptr;      // [1] (1/4096) in Montgomery form
+    uint32_t *part_items = nullptr;   // plans 3-4: tap items of the kPartLevels parts, part q from 32 * off[q]
+    uint32_t *part_offsets = nullptr; // [kFBMaxParts][129]
     FlatBPlan *fb_plan = nullptr;   // plan 3's phase-B rounds
     int fb_rounds = 0;              // 0: plan 3 uses the per-warp phase B
     uint32_t fb_stride[2] = {0, 0}; // elements per output after rounds 1 and 2
@@ -64,9 +96,8 @@ struct ProofWork {
     Fr *scalars = nullptr;      // [cap][128 j][64 i] canonical
     G1J *buckets = nullptr;     // [cap][128][128]
     G1J *points = nullptr;      // [cap][128] reduce outputs
-    G1J *ladder = nullptr;      // [cap][128][16] 2^(8d) u[j]
-    G1J *folded = nullptr;      // [cap][128][16] (plans 0-2; plans 3-4 use it as affine scratch)
-    G1A *ladder_aff = nullptr;  // [cap][128][32]: d < 16 the folded ladder, d >= 16 its phi images
+    G1J *ladder = nullptr;      // [cap][128][16] 2^(8d) v[j] of the folded parts
+    G1A *ladder_aff = nullptr;  // [cap][128][32]: d < 16 the ladder, d >= 16 its phi images
     uint8_t *proofs = nullptr;  // [cap][128][48]
     uint32_t *err = nullptr;    // [cap]
     // batch-affine accumulation (plans 1, 2)

@@ -8,14 +8,15 @@
 //                        shared memory, fixed-base bucket accumulation over the
 //                        position table                     (k_phase_a_sort, k_phase_a)
 //   4 k_reduce           sum_k k * B_k, 8 lanes per output  (k_bucket_reduce)
-//   5 k_ladder           L[j][d] = 2^(8d) u[j], d < 16      (k_ladder, d < 32: the
+//   5 k_fold_points      u+- = u[j] +- u[j+64], and for plans 3-4 once more on
+//                        the cyclic half: the convolution's parts (k_fold_ladder)
+//   6 k_ladder           L[j][d] = 2^(8d) u[j], d < 16      (k_ladder, d < 32: the
 //                        taps are split as k1 + k2 z^2 and slots 16..31 read phi(L))
-//   6 k_fold             L+- = L[j] +- L[j+64]              (k_fold_ladder)
 //   7 k_normalize        Jacobian -> affine, block batch inversion, phi images
 //                                                           (k_normalize)
 //   8 k_phase_b          split-circulant bucket MSM with the fixed taps (k_phase_b_split)
 //   4'k_reduce
-//   9 k_finish           combine C+ +- C-, normalise, compress, write slot brev7(a)
+//   9 k_finish           unfold the parts (C+ +- C-), normalise, compress, write slot brev7(a)
 //                                                           (k_combine_split, k_normalize, k_compress_proofs)
 #include "bucket_sum.cuh"
 #include "device_util.cuh"
@@ -212,16 +213,29 @@ __global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *
 }
 
 // ---------------------------------------------------------------- stage 6
-__global__ void __launch_bounds__(128) k_fold(const G1J *__restrict__ ladder, G1J *folded, int n_blobs) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= n_blobs * kHalf * kLadderDigits) return;
-    const int b = gid / (kHalf * kLadderDigits), r = gid % (kHalf * kLadderDigits);
-    const int j = r / kLadderDigits, d = r % kLadderDigits;
-    const size_t base = (size_t)b * kCells * kLadderDigits;
-    const G1J a = ld_vec(&ladder[base + j * kLadderDigits + d]);
-    const G1J c = ld_vec(&ladder[base + (j + kHalf) * kLadderDigits + d]);
-    st_vec(&folded[base + j * kLadderDigits + d], g1_add(a, c));
-    st_vec(&folded[base + (j + kHalf) * kLadderDigits + d], g1_sub(a, c));
+// The parts of phase B's convolution (PartLayout), in place per blob: level l
+// folds the cyclic vector v of 2m = 256 >> l points into v[j] + v[j + m] (the
+// next cyclic vector, slots [0, m)) and v[j] - v[j + m] (the negacyclic part,
+// slots [m, 2m)).  One level is the reference's k_fold_ladder split, applied to
+// u before the ladder instead of to every ladder row.
+__global__ void __launch_bounds__(kHalf) k_fold_points(G1J *points, int levels) {
+    __shared__ G1J v[kCells];
+    const int b = blockIdx.x, t = threadIdx.x;
+    G1J *pb = points + (size_t)b * kCells;
+    st_vec(&v[t], ld_vec(&pb[t]));
+    st_vec(&v[t + kHalf], ld_vec(&pb[t + kHalf]));
+    __syncthreads();
+    for (int l = 1; l <= levels; l++) {
+        const int m = kCells >> l;
+        if (t < m) {
+            const G1J x = ld_vec(&v[t]), y = ld_vec(&v[t + m]);
+            st_vec(&v[t], g1_add(x, y));
+            st_vec(&v[t + m], g1_sub(x, y));
+        }
+        __syncthreads();
+    }
+    st_vec(&pb[t], ld_vec(&v[t]));
+    st_vec(&pb[t + kHalf], ld_vec(&v[t + kHalf]));
 }
 
 // ---------------------------------------------------------------- stage 7
@@ -279,17 +293,24 @@ __global__ void __launch_bounds__(kBuckets) k_phase_b(const G1A *__restrict__ la
 }
 
 // ---------------------------------------------------------------- stage 9
-__global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, uint8_t *proofs) {
+// The parts' results unfold level by level, innermost first (the inverse
+// butterflies of k_fold_points; the taps carry the factors 1/2): y[a] = C+[a] +
+// C-[a], y[a + m] = C+[a] - C-[a].
+__global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, uint8_t *proofs, int levels) {
     __shared__ Fp tree[2 * kCells];
     __shared__ G1J outp[kCells];
     const int b = blockIdx.x, t = threadIdx.x;
-    if (t < kHalf) {
-        const G1J cp = ld_vec(&c[(size_t)b * kCells + t]);
-        const G1J cm = ld_vec(&c[(size_t)b * kCells + t + kHalf]);
-        st_vec(&outp[t], g1_add(cp, cm));
-        st_vec(&outp[t + kHalf], g1_sub(cp, cm));
-    }
+    st_vec(&outp[t], ld_vec(&c[(size_t)b * kCells + t]));
     __syncthreads();
+    for (int l = levels; l >= 1; l--) {
+        const int m = kCells >> l;
+        if (t < m) {
+            const G1J cp = ld_vec(&outp[t]), cm = ld_vec(&outp[t + m]);
+            st_vec(&outp[t], g1_add(cp, cm));
+            st_vec(&outp[t + m], g1_sub(cp, cm));
+        }
+        __syncthreads();
+    }
     const G1J p = ld_vec(&outp[t]);
     const bool inf = fp_is_zero(p.z);
     const Fp zi = block_batch_inverse_fp<kCells>(inf ? fp_one() : p.z, tree);
@@ -784,47 +805,50 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
 }
 
 // Plan 3's phase B as grid-wide rounds.  The bucket lists of an output are the
-// tap items of its half (plus: a < 64, minus: a >= 64), so every output of a
-// half has the same bucket lengths in every round: the round structure is a
-// setup constant (FlatBPlan, built on the host) and the pairs of all outputs
-// are dealt to all lanes as in phase A.  Round r keeps bucket k of output o at
-// buf[o * stride[r] + base[r][half][k] ..]; the last round leaves one point or
-// none per bucket, scattered into bucket_aff for the reduction.
-bool build_flatb_plan(const uint32_t offsets[2][kBuckets + 1], FlatBPlan &pl) {
+// tap items of its part (PartLayout: the cyclic part and the negacyclic parts
+// of the folds), so every output of a part has the same bucket lengths in every
+// round: the round structure is a setup constant (FlatBPlan, built on the host)
+// and the pairs of all outputs are dealt to all lanes as in phase A.  Round r
+// keeps bucket k of output o (part q) at buf[o * stride[r] + base[r][q][k] ..];
+// the last round leaves one point or none per bucket, scattered into
+// bucket_aff for the reduction.
+bool build_flatb_plan(const PartLayout &parts, const uint32_t offsets[][kBuckets + 1], FlatBPlan &pl) {
     memset(&pl, 0, sizeof pl);
-    uint32_t cnt[2][kBuckets];
-    for (int h = 0; h < 2; h++)
-        for (int k = 0; k < kBuckets; k++) cnt[h][k] = offsets[h][k + 1] - offsets[h][k];
+    if (parts.n < 1 || parts.n > kFBMaxParts) return false;
+    pl.parts = parts;
+    uint32_t cnt[kFBMaxParts][kBuckets];
+    for (int q = 0; q < parts.n; q++)
+        for (int k = 0; k < kBuckets; k++) cnt[q][k] = offsets[q][k + 1] - offsets[q][k];
     int r = 0;
     for (;; r++) {
         if (r > kFBMaxRounds) return false;
         bool more = false;
         uint32_t stride = 0;
-        for (int h = 0; h < 2; h++) {
+        for (int q = 0; q < parts.n; q++) {
             uint32_t b = 0, ps = 0, no = 0;
             for (int k = 0; k < kBuckets; k++) {
-                pl.cnt[r][h][k] = cnt[h][k];
-                pl.base[r][h][k] = b;
-                b += cnt[h][k];
-                more |= cnt[h][k] > 1;
+                pl.cnt[r][q][k] = cnt[q][k];
+                pl.base[r][q][k] = b;
+                b += cnt[q][k];
+                more |= cnt[q][k] > 1;
                 if (r < kFBMaxRounds) {
-                    pl.pscan[r][h][k] = ps;
-                    ps += cnt[h][k] >> 1;
-                    if (cnt[h][k] & 1u) pl.odd[r][h][no++] = (uint8_t)k;
+                    pl.pscan[r][q][k] = ps;
+                    ps += cnt[q][k] >> 1;
+                    if (cnt[q][k] & 1u) pl.odd[r][q][no++] = (uint8_t)k;
                 }
             }
-            pl.base[r][h][kBuckets] = b;
+            pl.base[r][q][kBuckets] = b;
             stride = std::max(stride, b);
             if (r < kFBMaxRounds) {
-                pl.pscan[r][h][kBuckets] = ps;
-                pl.pairs[r][h] = ps;
-                pl.n_odd[r][h] = no;
+                pl.pscan[r][q][kBuckets] = ps;
+                pl.pairs[r][q] = ps;
+                pl.n_odd[r][q] = no;
             }
         }
         pl.stride[r] = stride;
         if (!more) break;
-        for (int h = 0; h < 2; h++)
-            for (int k = 0; k < kBuckets; k++) cnt[h][k] = (cnt[h][k] + 1) >> 1;
+        for (int q = 0; q < parts.n; q++)
+            for (int k = 0; k < kBuckets; k++) cnt[q][k] = (cnt[q][k] + 1) >> 1;
     }
     pl.rounds = r;
     return true;
@@ -833,8 +857,8 @@ bool build_flatb_plan(const uint32_t offsets[2][kBuckets + 1], FlatBPlan &pl) {
 struct FlatBArgs {
     const FlatBPlan *plan;
     const G1A *ladder_aff;
-    const uint32_t *items[2];
-    const uint32_t *offsets[2];
+    const uint32_t *items;   // part q's items from kDigits * off[q]
+    const uint32_t *offsets; // [kFBMaxParts][kBuckets + 1]
     const G1A *src;
     G1A *dst;
     uint32_t *pre;
@@ -845,86 +869,104 @@ struct FlatBArgs {
 
 // shared copy of one round's plan (and, in round 0, the tap items)
 struct FlatBRound {
-    uint32_t pscan[2][kBuckets + 1];
-    uint32_t base[2][kBuckets + 1];
-    uint32_t base_next[2][kBuckets + 1];
-    uint32_t cnt[2][kBuckets];
-    uint32_t stride, stride_next, pairs[2];
+    uint32_t pscan[kFBMaxParts][kBuckets + 1];
+    uint32_t base[kFBMaxParts][kBuckets + 1];
+    uint32_t base_next[kFBMaxParts][kBuckets + 1];
+    uint32_t cnt[kFBMaxParts][kBuckets];
+    uint32_t pairs[kFBMaxParts];
+    uint32_t pair_end[kFBMaxParts]; // all blobs' pairs of parts 0..q
+    uint32_t size[kFBMaxParts], off[kFBMaxParts], nega[kFBMaxParts];
+    uint32_t stride, stride_next;
+    int n_parts;
 };
-constexpr size_t kFlatBSmem = sizeof(FlatBRound) + (2 * kTapItemsMax + 2 * (kBuckets + 1)) * sizeof(uint32_t);
+constexpr int kPartItemsMax = kCells * kDigits;
+constexpr size_t kFlatBSmem =
+    sizeof(FlatBRound) + (kPartItemsMax + kFBMaxParts * (kBuckets + 1)) * sizeof(uint32_t);
 
 template <bool FIRST>
 __device__ void flatb_stage(const FlatBArgs &a, int r, FlatBRound &sr, uint32_t *items, uint32_t *offs) {
     const FlatBPlan &pl = *a.plan;
-    for (int x = threadIdx.x; x < 2 * (kBuckets + 1); x += blockDim.x) {
-        const int h = x / (kBuckets + 1), k = x % (kBuckets + 1);
-        sr.pscan[h][k] = pl.pscan[r][h][k];
-        sr.base[h][k] = pl.base[r][h][k];
-        sr.base_next[h][k] = pl.base[r + 1][h][k];
-        if (k < kBuckets) sr.cnt[h][k] = pl.cnt[r][h][k];
-        if (FIRST) offs[x] = __ldg(&a.offsets[h][k]);
+    const int np = pl.parts.n;
+    for (int x = threadIdx.x; x < np * (kBuckets + 1); x += blockDim.x) {
+        const int q = x / (kBuckets + 1), k = x % (kBuckets + 1);
+        sr.pscan[q][k] = pl.pscan[r][q][k];
+        sr.base[q][k] = pl.base[r][q][k];
+        sr.base_next[q][k] = pl.base[r + 1][q][k];
+        if (k < kBuckets) sr.cnt[q][k] = pl.cnt[r][q][k];
+        if (FIRST) offs[x] = __ldg(&a.offsets[x]);
     }
     if (threadIdx.x == 0) {
         sr.stride = pl.stride[r];
         sr.stride_next = pl.stride[r + 1];
-        sr.pairs[0] = pl.pairs[r][0];
-        sr.pairs[1] = pl.pairs[r][1];
+        sr.n_parts = np;
+        uint32_t end = 0;
+        for (int q = 0; q < np; q++) {
+            sr.pairs[q] = pl.pairs[r][q];
+            sr.size[q] = pl.parts.size[q];
+            sr.off[q] = pl.parts.off[q];
+            sr.nega[q] = pl.parts.nega[q];
+            end += (uint32_t)a.n_blobs * pl.parts.size[q] * pl.pairs[r][q];
+            sr.pair_end[q] = end;
+        }
     }
     if (FIRST) {
         __syncthreads();
-        for (int h = 0; h < 2; h++)
-            for (uint32_t k = threadIdx.x; k < offs[h * (kBuckets + 1) + kBuckets]; k += blockDim.x)
-                items[h * kTapItemsMax + k] = __ldg(&a.items[h][k]);
+        for (int q = 0; q < np; q++) {
+            const uint32_t b = kDigits * pl.parts.off[q], m = offs[q * (kBuckets + 1) + kBuckets];
+            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) items[b + k] = __ldg(&a.items[b + k]);
+        }
     }
     __syncthreads();
 }
 
-// element e of bucket k of output o (half h)
+// element e of bucket k of output o (part q)
 template <bool FIRST>
 __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
-                                          const uint32_t *offs, uint32_t o, int h, int k, uint32_t e) {
+                                          const uint32_t *offs, uint32_t o, int q, int k, uint32_t e) {
     if (FIRST) {
-        const uint32_t packed = items[h * kTapItemsMax + offs[h * (kBuckets + 1) + k] + e];
+        const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
         const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
-        const uint32_t b = o / kCells, aa = o % kHalf;
-        G1A pt = ld_vec(&a.ladder_aff[((size_t)b * kCells + h * kHalf + ((aa - tap) & (kHalf - 1))) * kDigits + d]);
-        if (((packed >> 16) & 1u) != (h == 1 && tap > (int)aa)) pt.y = fp_neg(pt.y);
+        const uint32_t b = o / kCells, aa = o % kCells - sr.off[q];
+        const uint32_t slot = sr.off[q] + ((aa - (uint32_t)tap) & (sr.size[q] - 1));
+        G1A pt = ld_vec(&a.ladder_aff[((size_t)b * kCells + slot) * kDigits + d]);
+        if (((packed >> 16) & 1u) != (sr.nega[q] && tap > (int)aa)) pt.y = fp_neg(pt.y);
         return pt;
     }
-    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[h][k] + e]);
+    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e]);
 }
 
-// pair p of the round -> output, half, bucket, index
-__device__ __forceinline__ void flatb_pair(const FlatBRound &sr, int n_blobs, uint32_t p, uint32_t &o, int &h, int &k,
+// pair p of the round -> output, part, bucket, index
+__device__ __forceinline__ void flatb_pair(const FlatBRound &sr, uint32_t p, uint32_t &o, int &q, int &k,
                                            uint32_t &i) {
-    const uint32_t p_plus = (uint32_t)n_blobs * kHalf * sr.pairs[0];
-    h = p < p_plus ? 0 : 1;
-    const uint32_t pp = h ? p - p_plus : p;
-    const uint32_t per = sr.pairs[h];
-    const uint32_t ol = pp / per, q = pp - ol * per;
-    o = (ol / kHalf) * kCells + h * kHalf + ol % kHalf;
-    k = ba_bucket_of<kBuckets>(sr.pscan[h], q);
-    i = q - sr.pscan[h][k];
+    q = 0;
+    while (q + 1 < sr.n_parts && p >= sr.pair_end[q]) q++;
+    const uint32_t pp = q ? p - sr.pair_end[q - 1] : p;
+    const uint32_t per = sr.pairs[q];
+    const uint32_t ol = pp / per, r = pp - ol * per;
+    const uint32_t m = sr.size[q];
+    o = (ol / m) * kCells + sr.off[q] + ol % m;
+    k = ba_bucket_of<kBuckets>(sr.pscan[q], r);
+    i = r - sr.pscan[q][k];
 }
 
 template <bool FIRST>
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, int r) {
     extern __shared__ uint4 dyn_smem[];
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
-    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
+    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + kPartItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
-    const uint32_t P = (uint32_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    const uint32_t P = sr.pair_end[sr.n_parts - 1];
     uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp acc = fp_one();
     int s = 0;
     for (uint32_t p = gl; p < P; p += NL, s++) {
         uint32_t o, i;
-        int h, k;
-        flatb_pair(sr, a.n_blobs, p, o, h, k, i);
-        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i);
-        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i + 1);
+        int q, k;
+        flatb_pair(sr, p, o, q, k, i);
+        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
+        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
         wb_store_pre(pre, s, acc);
         acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
     }
@@ -935,42 +977,46 @@ template <bool FIRST>
 __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, int r) {
     extern __shared__ uint4 dyn_smem[];
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
-    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + 2 * kTapItemsMax;
+    uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + kPartItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
-    const uint32_t P = (uint32_t)a.n_blobs * kHalf * (sr.pairs[0] + sr.pairs[1]);
+    const uint32_t P = sr.pair_end[sr.n_parts - 1];
     const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
     for (int t = S - 1; t >= 0; t--) {
         const uint32_t p = gl + (uint32_t)t * NL;
         uint32_t o, i;
-        int h, k;
-        flatb_pair(sr, a.n_blobs, p, o, h, k, i);
-        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i);
-        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, h, k, 2 * i + 1);
+        int q, k;
+        flatb_pair(sr, p, o, q, k, i);
+        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
+        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
         const int kind = pair_kind(x, y);
         const Fp den = pair_denominator(x, y, kind);
         const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
         inv = fp_mul(inv, den);
-        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[h][k] + i], pair_result(x, y, kind, inv_den));
+        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + i], pair_result(x, y, kind, inv_den));
     }
     // odd last elements move up unchanged
     const FlatBPlan &pl = *a.plan;
-    const size_t n_half = (size_t)a.n_blobs * kHalf;
-    const size_t odd_all = n_half * (pl.n_odd[r][0] + pl.n_odd[r][1]);
-    for (size_t x = gl; x < odd_all; x += NL) {
-        const size_t x_plus = n_half * pl.n_odd[r][0];
-        const int h = x < x_plus ? 0 : 1;
-        const size_t xx = h ? x - x_plus : x;
-        const uint32_t no = pl.n_odd[r][h];
-        const uint32_t ol = (uint32_t)(xx / no), j = (uint32_t)(xx - (size_t)ol * no);
-        const int k = pl.odd[r][h][j];
-        const uint32_t o = (ol / kHalf) * kCells + h * kHalf + ol % kHalf;
-        const uint32_t c = sr.cnt[h][k];
-        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[h][k] + (c >> 1)],
-               flatb_load<FIRST>(a, sr, items, offs, o, h, k, c - 1));
+    size_t odd_begin = 0;
+    for (int q = 0; q < sr.n_parts; q++) {
+        const uint32_t no = pl.n_odd[r][q], m = sr.size[q];
+        const size_t odd_q = (size_t)a.n_blobs * m * no;
+        // this part's odd elements are x in [odd_begin, odd_begin + odd_q) of the
+        // grid-wide sequence; lane gl takes those with x = gl (mod NL)
+        const size_t first = odd_begin + (gl + NL - odd_begin % NL) % NL;
+        for (size_t x = first; x < odd_begin + odd_q; x += NL) {
+            const size_t xx = x - odd_begin;
+            const uint32_t ol = (uint32_t)(xx / no), j = (uint32_t)(xx - (size_t)ol * no);
+            const int k = pl.odd[r][q][j];
+            const uint32_t o = (ol / m) * kCells + sr.off[q] + ol % m;
+            const uint32_t c = sr.cnt[q][k];
+            st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + (c >> 1)],
+                   flatb_load<FIRST>(a, sr, items, offs, o, q, k, c - 1));
+        }
+        odd_begin += odd_q;
     }
 }
 
@@ -980,10 +1026,13 @@ __global__ void __launch_bounds__(128) k_flatb_finish(const FlatBPlan *__restric
     const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= (size_t)n_out * kBuckets) return;
     const uint32_t o = (uint32_t)(x / kBuckets), k = (uint32_t)(x % kBuckets);
-    const int h = (o % kCells) >= kHalf ? 1 : 0, R = plan->rounds;
+    const uint32_t slot = o % kCells;
+    int q = 0;
+    while (q + 1 < plan->parts.n && slot >= plan->parts.off[q + 1]) q++;
+    const int R = plan->rounds;
     G1A v;
-    if (plan->cnt[R][h][k]) {
-        v = ld_vec(&last[(size_t)o * plan->stride[R] + plan->base[R][h][k]]);
+    if (plan->cnt[R][q][k]) {
+        v = ld_vec(&last[(size_t)o * plan->stride[R] + plan->base[R][q][k]]);
     } else {
         v.x = fp_zero();
         v.y = fp_zero();
@@ -996,10 +1045,8 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
     FlatBArgs a;
     a.plan = t.fb_plan;
     a.ladder_aff = w.ladder_aff;
-    for (int h = 0; h < 2; h++) {
-        a.items[h] = t.tap_items[h];
-        a.offsets[h] = t.tap_offsets[h];
-    }
+    a.items = t.part_items;
+    a.offsets = t.part_offsets;
     a.pre = w.flat_pre;
     a.others = w.flat_others;
     a.tot = w.flat_tot;
@@ -1399,73 +1446,9 @@ int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_o
     return 3 * rounds + 1;
 }
 
-// Plans 3 and 4 fold the ladder after normalising it: L+-[j][d] = L[j][d] +-
-// L[j + 64][d] as one grid-wide round of affine additions (6 Fp multiplies
-// each with the shared inversion) instead of Jacobian additions (16) followed
-// by a normalisation of the results.  Pair q = ((blob * 64 + j) * 32 + d) * 2 +
-// sign writes folded[blob][sign * 64 + j][d].
-struct FoldArgs {
-    const G1A *lad;  // [blob][128][16] normalised ladder
-    G1A *out;        // [blob][128][32]: plus half, then minus half; slot 16 + d = phi(slot d)
-    uint32_t *pre;
-    Fp *others, *tot, *totinv;
-    size_t slots_pre;
-    int n_blobs;
-};
-
-__device__ __forceinline__ void fold_pair(const FoldArgs &a, size_t q, G1A &x, G1A &y, size_t &dst) {
-    const int sign = (int)(q & 1);
-    const size_t r = q >> 1;
-    const size_t b = r / (kHalf * kLadderDigits), jd = r % (kHalf * kLadderDigits);
-    const size_t j = jd / kLadderDigits, d = jd % kLadderDigits;
-    const size_t base = b * kCells * kLadderDigits;
-    x = ld_vec(&a.lad[base + j * kLadderDigits + d]);
-    y = ld_vec(&a.lad[base + (j + kHalf) * kLadderDigits + d]);
-    if (sign) y.y = fp_neg(y.y);
-    dst = (b * kCells + j + (sign ? kHalf : 0)) * kDigits + d;
-}
-
-__global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass1(FoldArgs a) {
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * kLadderDigits * 2;
-    uint32_t *pre = a.pre + wg * a.slots_pre * 384;
-    Fp acc = fp_one();
-    int s = 0;
-    for (size_t p = gl; p < P; p += NL, s++) {
-        G1A x, y;
-        size_t dst;
-        fold_pair(a, p, x, y, dst);
-        wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
-    }
-    flat_pass1_products(acc, a.others, a.tot, gl, wg);
-}
-
-__global__ void __launch_bounds__(kFlatThreads, 2) k_fold_pass2(FoldArgs a) {
-    const size_t gl = (size_t)blockIdx.x * blockDim.x + threadIdx.x, NL = (size_t)gridDim.x * blockDim.x;
-    const size_t wg = gl >> 5;
-    const size_t P = (size_t)a.n_blobs * kHalf * kLadderDigits * 2;
-    const uint32_t *pre = a.pre + wg * a.slots_pre * 384;
-    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
-    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
-    for (int t = S - 1; t >= 0; t--) {
-        G1A x, y;
-        size_t dst;
-        fold_pair(a, gl + (size_t)t * NL, x, y, dst);
-        const int kind = pair_kind(x, y);
-        const Fp den = pair_denominator(x, y, kind);
-        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
-        inv = fp_mul(inv, den);
-        const G1A f = pair_result(x, y, kind, inv_den);
-        st_vec(&a.out[dst], f);
-        st_vec(&a.out[dst + kLadderDigits], g1_phi(f));
-    }
-}
-
-// Jacobian -> affine for n points as one grid-wide round (plans 3-4): Z values
-// dealt to all lanes, one inversion per warp product, x = X / Z^2, y = Y / Z^3;
-// infinity (Z = 0) -> (0, 0).
+// The ladder to affine form as one grid-wide round (plans 3-4): Z values dealt
+// to all lanes, one inversion per warp product, x = X / Z^2, y = Y / Z^3;
+// infinity (Z = 0) -> (0, 0); each point is written with its phi image.
 struct NormArgs {
     const G1J *in;
     G1A *out;
@@ -1510,39 +1493,29 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
             r.x = fp_mul(q.x, z2);
             r.y = fp_mul(q.y, fp_mul(z2, zi));
         }
-        st_vec(&a.out[p], r);
+        // in: [row][16] ladder; out: [row][32], slot 16 + d = phi(slot d)
+        const size_t dst = (size_t)(p / kLadderDigits) * kDigits + p % kLadderDigits;
+        st_vec(&a.out[dst], r);
+        st_vec(&a.out[dst + kLadderDigits], g1_phi(r));
     }
 }
 
-// normalise the ladder into `scratch`, then fold it into w.ladder_aff; returns the launches made
-int launch_fold_affine(const ProofWork &w, int n, G1A *scratch, cudaStream_t s) {
-    const int n_lad = n * kCells * kLadderDigits;
+// the ladder to affine form with its phi images, into w.ladder_aff; returns the launches made
+int launch_normalize_flat(const ProofWork &w, int n, cudaStream_t s) {
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     NormArgs na;
     na.in = w.ladder;
-    na.out = scratch;
+    na.out = w.ladder_aff;
     na.pre = w.flat_pre;
     na.others = w.flat_others;
     na.tot = w.flat_tot;
     na.totinv = w.flat_totinv;
     na.slots_pre = w.flat_slots;
-    na.n = (uint32_t)n_lad;
+    na.n = (uint32_t)(n * kCells * kLadderDigits);
     k_norm_pass1<<<blocks, kFlatThreads, 0, s>>>(na);
     k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(na.tot, na.totinv, warps);
     k_norm_pass2<<<blocks, kFlatThreads, 0, s>>>(na);
-    FoldArgs a;
-    a.lad = scratch;
-    a.out = w.ladder_aff;
-    a.pre = w.flat_pre;
-    a.others = w.flat_others;
-    a.tot = w.flat_tot;
-    a.totinv = w.flat_totinv;
-    a.slots_pre = w.flat_slots;
-    a.n_blobs = n;
-    k_fold_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
-    k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
-    k_fold_pass2<<<blocks, kFlatThreads, 0, s>>>(a);
-    return 6;
+    return 3;
 }
 
 // ---------------------------------------------------------------- launcher
@@ -1593,17 +1566,14 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     if (!comb) reduce();
     mark();
+    // plans 3-4 split phase B into the kPartLevels parts, plans 0-2 into two halves
+    const int levels = flatb ? kPartLevels : 1;
+    k_fold_points<<<n, kHalf, 0, s>>>(w.points, levels);
+    mark();
     k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
     mark();
-    if (flatb) {
-        // normalise, then fold in affine form (the "normalize" stage is empty)
-        launched += launch_fold_affine(w, n, reinterpret_cast<G1A *>(w.folded), s) - 2;
-        mark();
-    } else {
-        k_fold<<<(n * kHalf * kLadderDigits + 127) / 128, 128, 0, s>>>(w.ladder, w.folded, n);
-        mark();
-        k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.folded, w.ladder_aff, n_lad);
-    }
+    if (flatb) launched += launch_normalize_flat(w, n, s) - 1;
+    else k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, w.ladder_aff, n_lad);
     mark();
     if (flatb) {
         launched += launch_phase_b_flat(t, w, n, s) - 1;
@@ -1619,7 +1589,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     mark();
     reduce();
     mark();
-    k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs);
+    k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs, levels);
     mark();
     count_launches(launched);
     return cudaGetLastError();

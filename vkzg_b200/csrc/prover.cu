@@ -51,7 +51,7 @@ uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 static constexpr int kProofStages = 10;
 static constexpr int kRecoverStages = 2;
 static const char *kProofStageNames[kProofStages] = {"blob_to_coeffs", "circulant", "phase_a",  "reduce_a",
-                                                     "ladder",         "fold",      "normalize", "phase_b",
+                                                     "fold",           "ladder",    "normalize", "phase_b",
                                                      "reduce_b",       "finish"};
 static const char *kRecoverStageNames[kRecoverStages] = {"recover_prep", "recover_main"};
 
@@ -200,70 +200,122 @@ void host_roots(std::vector<Fr> &fwd, std::vector<Fr> &inv) {
     }
 }
 
-// Phase-B half taps c+-[e] = (c[e] +- c[e+64]) / 2, c[e] = (1/128) sum_{t<64} w_128^(e t),
-// recoded into signed base-256 digits and grouped by bucket (the reference's
-// kernel_items/offsets/perm tables, src/precomputed_tables.cpp:45-49).  With
-// split_phi, each tap is k1 + k2 z^2 (glv.h): digit slots 0..15 hold k1's digits
-// (applied to 2^(8d) L), slots 16..31 the digits of -k2 (applied to 2^(8d) phi(L));
-// without it, the reference's 32 digits of the full tap (its tables file).
-// Returns false if a split does not fit its 16 digits (it always does).
-bool host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2], uint32_t offsets[2][kBuckets + 1],
-                     uint32_t perm[2][kBuckets], bool split_phi) {
-    Fr c[kCells];
-    const Fr inv128 = fr_inv(fr_from_u32(128)), inv2 = fr_inv(fr_from_u32(2));
+// c[e] = (1/128) sum_{t<64} w_128^(e t), e < 128: the taps of the 128-point
+// cyclic convolution phase B computes (src/precomputed_tables.cpp:45-49).
+static void host_taps128(const std::vector<Fr> &fwd, Fr c[kCells]) {
+    const Fr inv128 = fr_inv(fr_from_u32(128));
     for (int e = 0; e < kCells; e++) {
         Fr acc = fr_zero();
         for (int t = 0; t < kHalf; t++) acc = fr_add(acc, fwd[((e * t) % kCells) * (kExtElems / kCells)]);
         c[e] = fr_mul(acc, inv128);
     }
-    for (int h = 0; h < 2; h++) {
-        int dig[kHalf][kDigits];
-        uint32_t count[kBuckets] = {0};
-        for (int e = 0; e < kHalf; e++) {
-            const Fr tap = fr_mul(h == 0 ? fr_add(c[e], c[e + kHalf]) : fr_sub(c[e], c[e + kHalf]), inv2);
-            const Fr can = fr_to_canonical(tap);
-            if (split_phi) {
-                const GlvSplit sp = glv_split(can.v);
-                if (!glv_digits(sp.mag[0], sp.neg[0], dig[e]) ||
-                    !glv_digits(sp.mag[1], sp.neg[1], dig[e] + kGlvDigits))
-                    return false;
-            } else {
-                int carry = 0;
-                for (int d = 0; d < kDigits; d++) {
-                    int v = (int)((can.v[d >> 2] >> ((d & 3) * 8)) & 0xffu) + carry;
-                    carry = 0;
-                    if (v > kBuckets) {
-                        v -= 2 * kBuckets;
-                        carry = 1;
-                    }
-                    dig[e][d] = v;
-                }
-            }
-            for (int d = 0; d < kDigits; d++)
-                if (dig[e][d]) count[abs(dig[e][d]) - 1]++;
+}
+
+// Signed base-256 digits of one tap (Montgomery form).  With split_phi the tap
+// is k1 + k2 z^2 (glv.h): slots 0..15 hold k1's digits (applied to 2^(8d) L),
+// slots 16..31 the digits of -k2 (applied to 2^(8d) phi(L)); without it, the
+// reference's 32 digits of the full tap.  False if a split does not fit its
+// 16 digits (it always does).
+static bool tap_digits(const Fr &tap, bool split_phi, int dig[kDigits]) {
+    const Fr can = fr_to_canonical(tap);
+    if (split_phi) {
+        const GlvSplit sp = glv_split(can.v);
+        return glv_digits(sp.mag[0], sp.neg[0], dig) && glv_digits(sp.mag[1], sp.neg[1], dig + kGlvDigits);
+    }
+    int carry = 0;
+    for (int d = 0; d < kDigits; d++) {
+        int v = (int)((can.v[d >> 2] >> ((d & 3) * 8)) & 0xffu) + carry;
+        carry = 0;
+        if (v > kBuckets) {
+            v -= 2 * kBuckets;
+            carry = 1;
         }
-        uint32_t acc = 0;
-        for (int k = 0; k < kBuckets; k++) {
-            offsets[h][k] = acc;
-            acc += count[k];
+        dig[d] = v;
+    }
+    return true;
+}
+
+// Items e | d << 8 | neg << 16 of n_taps taps grouped by bucket |digit| - 1,
+// bucket offsets, and the buckets by descending load (the reference's
+// kernel_items / offsets / perm layout).
+static void group_items(const int (*dig)[kDigits], int n_taps, uint32_t *items, uint32_t offsets[kBuckets + 1],
+                        uint32_t perm[kBuckets]) {
+    uint32_t count[kBuckets] = {0};
+    for (int e = 0; e < n_taps; e++)
+        for (int d = 0; d < kDigits; d++)
+            if (dig[e][d]) count[abs(dig[e][d]) - 1]++;
+    uint32_t acc = 0;
+    for (int k = 0; k < kBuckets; k++) {
+        offsets[k] = acc;
+        acc += count[k];
+    }
+    offsets[kBuckets] = acc;
+    uint32_t cur[kBuckets];
+    memcpy(cur, offsets, sizeof cur);
+    for (int e = 0; e < n_taps; e++)
+        for (int d = 0; d < kDigits; d++) {
+            const int v = dig[e][d];
+            if (!v) continue;
+            items[cur[abs(v) - 1]++] = (uint32_t)e | ((uint32_t)d << 8) | ((v < 0 ? 1u : 0u) << 16);
         }
-        offsets[h][kBuckets] = acc;
-        items[h].assign(acc, 0);
-        uint32_t cur[kBuckets];
-        memcpy(cur, offsets[h], sizeof cur);
-        for (int e = 0; e < kHalf; e++)
-            for (int d = 0; d < kDigits; d++) {
-                const int v = dig[e][d];
-                if (!v) continue;
-                items[h][cur[abs(v) - 1]++] = (uint32_t)e | ((uint32_t)d << 8) | ((v < 0 ? 1u : 0u) << 16);
-            }
-        // buckets by descending load, stable
+    if (perm) {
         std::vector<int> order(kBuckets);
         for (int k = 0; k < kBuckets; k++) order[k] = k;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
             return std::min(count[a], 63u) > std::min(count[b], 63u);
         });
-        for (int k = 0; k < kBuckets; k++) perm[h][k] = (uint32_t)order[k];
+        for (int k = 0; k < kBuckets; k++) perm[k] = (uint32_t)order[k];
+    }
+}
+
+// Phase-B half taps c+-[e] = (c[e] +- c[e+64]) / 2 (one fold), recoded and
+// grouped per half; split_phi as in tap_digits.
+bool host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2], uint32_t offsets[2][kBuckets + 1],
+                     uint32_t perm[2][kBuckets], bool split_phi) {
+    Fr c[kCells];
+    host_taps128(fwd, c);
+    const Fr inv2 = fr_inv(fr_from_u32(2));
+    for (int h = 0; h < 2; h++) {
+        int dig[kHalf][kDigits];
+        for (int e = 0; e < kHalf; e++) {
+            const Fr tap = fr_mul(h == 0 ? fr_add(c[e], c[e + kHalf]) : fr_sub(c[e], c[e + kHalf]), inv2);
+            if (!tap_digits(tap, split_phi, dig[e])) return false;
+        }
+        items[h].assign((size_t)kHalf * kDigits, 0);
+        group_items(dig, kHalf, items[h].data(), offsets[h], perm[h]);
+        items[h].resize(offsets[h][kBuckets]);
+    }
+    return true;
+}
+
+// Tap items of the parts of `levels` folds (part_layout), split for phi: the
+// taps fold like the points, t+-[e] = (t[e] +- t[e + m]) / 2.  items holds
+// 32 * 128 entries, part q's from 32 * off[q].
+bool host_part_tables(const std::vector<Fr> &fwd, int levels, std::vector<uint32_t> &items,
+                      uint32_t offsets[kFBMaxParts][kBuckets + 1]) {
+    const PartLayout L = part_layout(levels);
+    Fr v[kCells];
+    host_taps128(fwd, v);
+    const Fr inv2 = fr_inv(fr_from_u32(2));
+    std::vector<Fr> taps[kFBMaxParts];
+    for (int l = 1; l <= levels; l++) {
+        const int m = kCells >> l;
+        std::vector<Fr> &neg = taps[levels + 1 - l];
+        neg.resize(m);
+        for (int e = 0; e < m; e++) {
+            neg[e] = fr_mul(fr_sub(v[e], v[e + m]), inv2);
+            v[e] = fr_mul(fr_add(v[e], v[e + m]), inv2);
+        }
+    }
+    taps[0].assign(v, v + (kCells >> levels));
+    items.assign((size_t)kCells * kDigits, 0);
+    memset(offsets, 0, sizeof(uint32_t) * kFBMaxParts * (kBuckets + 1));
+    for (int q = 0; q < L.n; q++) {
+        std::vector<std::array<int, kDigits>> dig(L.size[q]);
+        for (uint32_t e = 0; e < L.size[q]; e++)
+            if (!tap_digits(taps[q][e], true, dig[e].data())) return false;
+        group_items(reinterpret_cast<const int(*)[kDigits]>(dig.data()), (int)L.size[q],
+                    items.data() + (size_t)kDigits * L.off[q], offsets[q], nullptr);
     }
     return true;
 }
@@ -355,10 +407,17 @@ vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
     CK(cudaMemcpy(t.roots_fwd, h.roots_fwd.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(t.roots_inv, h.roots_inv.data(), kExtElems * sizeof(Fr), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(t.inv_blob_r2, &h.inv_blob, sizeof(Fr), cudaMemcpyHostToDevice));
-    // plan 3's phase-B round structure, from the tap offsets
+    // plans 3-4: the tap items of the kPartLevels parts and their round structure
     {
+        std::vector<uint32_t> pitems;
+        uint32_t poffs[kFBMaxParts][kBuckets + 1];
+        if (!host_part_tables(h.roots_fwd, kPartLevels, pitems, poffs)) return VKZG_ERR_SETUP;
+        if (!p->alloc(t.part_items, pitems.size()) || !p->alloc(t.part_offsets, (size_t)kFBMaxParts * (kBuckets + 1)))
+            return VKZG_ERR_MALLOC;
+        CK(cudaMemcpy(t.part_items, pitems.data(), 4 * pitems.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t.part_offsets, poffs, sizeof poffs, cudaMemcpyHostToDevice));
         std::unique_ptr<FlatBPlan> pl(new FlatBPlan);
-        if (build_flatb_plan(offsets, *pl) && pl->rounds > 0) {
+        if (build_flatb_plan(part_layout(kPartLevels), poffs, *pl) && pl->rounds > 0) {
             if (!p->alloc(t.fb_plan, 1)) return VKZG_ERR_MALLOC;
             CK(cudaMemcpy(t.fb_plan, pl.get(), sizeof(FlatBPlan), cudaMemcpyHostToDevice));
             t.fb_rounds = pl->rounds;
@@ -425,8 +484,8 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     const size_t B = cap;
     bool ok = p->alloc(w.blobs, B * kBlobBytes) && p->alloc(w.coeffs, B * kBlobElems) &&
               p->alloc(w.scalars, B * kCells * kCellElems) && p->alloc(w.buckets, B * kCells * kBuckets) &&
-              p->alloc(w.points, B * kCells) && p->alloc(w.ladder, B * kCells * kDigits) &&
-              p->alloc(w.folded, B * kCells * kDigits) && p->alloc(w.ladder_aff, B * kCells * kDigits) &&
+              p->alloc(w.points, B * kCells) && p->alloc(w.ladder, B * kCells * kLadderDigits) &&
+              p->alloc(w.ladder_aff, B * kCells * kDigits) &&
               p->alloc(w.proofs, B * kCells * kProofBytes) && p->alloc(w.err, B) &&
               p->alloc(r.cells, B * kExtElems * 32) && p->alloc(r.present, B * kCells) &&
               p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.scratch, B * kExtElems) &&
