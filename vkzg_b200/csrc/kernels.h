@@ -32,7 +32,7 @@ constexpr size_t kPositionPoints = (size_t)kCells * kCellElems * kDigits; // 262
 // negacyclic part of 128 >> l points at slots [128 >> l, 128 >> (l - 1)).
 // Plans 0-2 use one level (the two halves); plans 3-4 kPartLevels.
 constexpr int kFBMaxParts = 4;
-constexpr int kPartLevels = 2;
+constexpr int kPartLevels = 3;
 struct PartLayout {
     int n;                          // levels + 1
     uint32_t size[kFBMaxParts];     // outputs = points = taps of the part
