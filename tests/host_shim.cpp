@@ -15,6 +15,8 @@ void shim_fp_mul(const uint32_t *a, const uint32_t *b, uint32_t *r) {
 }
 void shim_fp_mul_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<12>(r, a, b); }
 void shim_fr_mul_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<8>(r, a, b); }
+void shim_fp_mul_ks2(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<12, 2>(r, a, b); }
+void shim_fr_mul_ks2(const uint32_t *a, const uint32_t *b, uint32_t *r) { mont_mul_ks<8, 2>(r, a, b); }
 void shim_fp_sqr_ks(const uint32_t *a, const uint32_t *b, uint32_t *r) {
     (void)b;
     mont_sqr_ks<12>(r, a);

@@ -42,6 +42,9 @@ def test_field_ops(shim, field):
     edge += [(x << half) | x for x in (1, (1 << (top - half)) - 1, rng.randrange(1 << (top - half)))]
     edge += [(x << half) | (x + 1) for x in (0, rng.randrange(1 << (top - half)))]
     edge += [(x << half) | ((1 << half) - 1) for x in (0, 1, (1 << (top - half)) - 1)]
+    quarter = 8 * n  # second Karatsuba level: equal quarters
+    edge += [sum(x << (quarter * k) for k in range(4)) % mod for x in (1, (1 << quarter) - 1, rng.randrange(1 << quarter))]
+    edge += [((1 << quarter) - 1) | (x << (2 * quarter)) for x in (0, 1, rng.randrange(1 << (top - 2 * quarter)))]
     vals = edge + [rng.randrange(mod) for _ in range(2000)]
     out = (ctypes.c_uint32 * n)()
     for k, a in enumerate(vals):
@@ -49,6 +52,8 @@ def test_field_ops(shim, field):
         getattr(shim, f"shim_{field}_mul")(words(a, n), words(b, n), out)
         assert value(out, n) == a * b * rinv % mod
         getattr(shim, f"shim_{field}_mul_ks")(words(a, n), words(b, n), out)
+        assert value(out, n) == a * b * rinv % mod
+        getattr(shim, f"shim_{field}_mul_ks2")(words(a, n), words(b, n), out)
         assert value(out, n) == a * b * rinv % mod
         getattr(shim, f"shim_{field}_sqr")(words(a, n), words(b, n), out)
         assert value(out, n) == a * a * rinv % mod

@@ -72,7 +72,7 @@ VK_HD G1J g1_dbl(const G1J &p) {
 VK_HD Fp fp_mul_inl(const Fp &a, const Fp &b) {
     Fp r;
 #if VKZG_FP_KARATSUBA
-    mont_mul_ks<12>(r.v, a.v, b.v);
+    mont_mul_ks<12, VKZG_FP_KARATSUBA>(r.v, a.v, b.v);
 #else
     mont_mul<12>(r.v, a.v, b.v);
 #endif
@@ -80,7 +80,11 @@ VK_HD Fp fp_mul_inl(const Fp &a, const Fp &b) {
 }
 VK_HD Fp fp_sqr_inl(const Fp &a) {
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_sqr_ks<12>(r.v, a.v);
+#else
     mont_sqr<12>(r.v, a.v);
+#endif
     return r;
 }
 VK_HD G1J g1_dbl_inl(const G1J &p) {

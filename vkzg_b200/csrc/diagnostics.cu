@@ -34,6 +34,12 @@ __device__ __noinline__ Fp fp_mul_ks_call(Fp a, Fp b) {
     return r;
 }
 
+__device__ __noinline__ Fp fp_mul_ks2_call(Fp a, Fp b) {
+    Fp r;
+    mont_mul_ks<12, 2>(r.v, a.v, b.v);
+    return r;
+}
+
 __device__ __noinline__ Fp fp_sqr_ks_call(Fp a) {
     Fp r;
     mont_sqr_ks<12>(r.v, a.v);
@@ -41,7 +47,7 @@ __device__ __noinline__ Fp fp_sqr_ks_call(Fp a) {
 }
 
 // independent Fp products per thread (2 chains); OP 0: fp_mul, 1: fp_sqr, 2: the
-// Karatsuba product, 3: the Karatsuba square
+// one-level Karatsuba product, 3: the Karatsuba square, 4: the two-level product
 template <int OP>
 __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint32_t *sink) {
     Fp a = fp_one(), b = fp_one();
@@ -58,9 +64,12 @@ __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint
         } else if (OP == 2) {
             a = fp_mul_ks_call(a, c);
             b = fp_mul_ks_call(b, c);
-        } else {
+        } else if (OP == 3) {
             a = fp_sqr_ks_call(a);
             b = fp_sqr_ks_call(b);
+        } else {
+            a = fp_mul_ks2_call(a, c);
+            b = fp_mul_ks2_call(b, c);
         }
     }
     if ((a.v[0] ^ b.v[0]) == 0x12345678u) sink[0] = a.v[1];
@@ -210,7 +219,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 6) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 7) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -234,7 +243,8 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
             if (which == 1) k_probe_fp<0><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 3) k_probe_fp<1><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 4) k_probe_fp<2><<<blocks, 128>>>(rep + 1, fp_iters, sink);
-            else k_probe_fp<3><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 6) k_probe_fp<3><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else k_probe_fp<4><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             ops = (double)blocks * 128 * 2 * fp_iters;
         } else {
             const int blocks = sms * 8;

@@ -349,84 +349,117 @@ VK_HD void sos_reduce(uint32_t *r, uint32_t *T) {
 // 2^(32(h + i + 1)), so neither chain carries out of word i + h.
 template <int H>
 VK_HD void mul_words(uint32_t *z, const uint32_t *x, const uint32_t *y) {
+    static_assert(H >= 3, "at least three words");
     CARRY_DECL
 #pragma unroll
     for (int i = 0; i < 2 * H; i++) z[i] = 0;
 #pragma unroll
     for (int i = 0; i < H; i++) {
         const uint32_t yi = y[i];
-        MAD_LO_CC(z[i], x[0], yi, z[i]);
-        MADC_HI_CC(z[i + 1], x[0], yi, z[i + 1]);
+        if constexpr (H % 2 == 0) {
+            // even j: words i .. i+h-1, then the carry into i+h; odd j: i+1 .. i+h
+            MAD_LO_CC(z[i], x[0], yi, z[i]);
+            MADC_HI_CC(z[i + 1], x[0], yi, z[i + 1]);
 #pragma unroll
-        for (int j = 2; j < H; j += 2) {
-            MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
-            MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
-        }
-        ADDC(z[i + H], z[i + H], 0u);
-        MAD_LO_CC(z[i + 1], x[1], yi, z[i + 1]);
-        MADC_HI_CC(z[i + 2], x[1], yi, z[i + 2]);
+            for (int j = 2; j < H; j += 2) {
+                MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+                MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+            }
+            ADDC(z[i + H], z[i + H], 0u);
+            MAD_LO_CC(z[i + 1], x[1], yi, z[i + 1]);
+            MADC_HI_CC(z[i + 2], x[1], yi, z[i + 2]);
 #pragma unroll
-        for (int j = 3; j < H - 1; j += 2) {
-            MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
-            MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+            for (int j = 3; j < H - 1; j += 2) {
+                MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+                MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+            }
+            MADC_LO_CC(z[i + H - 1], x[H - 1], yi, z[i + H - 1]);
+            MADC_HI(z[i + H], x[H - 1], yi, z[i + H]);
+        } else {
+            // even j: words i .. i+h; odd j: i+1 .. i+h-1, then the carry into i+h
+            MAD_LO_CC(z[i], x[0], yi, z[i]);
+            MADC_HI_CC(z[i + 1], x[0], yi, z[i + 1]);
+#pragma unroll
+            for (int j = 2; j < H - 1; j += 2) {
+                MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+                MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+            }
+            MADC_LO_CC(z[i + H - 1], x[H - 1], yi, z[i + H - 1]);
+            MADC_HI(z[i + H], x[H - 1], yi, z[i + H]);
+            MAD_LO_CC(z[i + 1], x[1], yi, z[i + 1]);
+            MADC_HI_CC(z[i + 2], x[1], yi, z[i + 2]);
+#pragma unroll
+            for (int j = 3; j < H; j += 2) {
+                MADC_LO_CC(z[i + j], x[j], yi, z[i + j]);
+                MADC_HI_CC(z[i + j + 1], x[j], yi, z[i + j + 1]);
+            }
+            ADDC(z[i + H], z[i + H], 0u);
         }
-        MADC_LO_CC(z[i + H - 1], x[H - 1], yi, z[i + H - 1]);
-        MADC_HI(z[i + H], x[H - 1], yi, z[i + H]);
     }
 }
 
-// Montgomery product through one Karatsuba level (n even, h = n/2):
-// a b = a0 b0 + (a0 b1 + a1 b0) 2^(32h) + a1 b1 2^(32n), with the middle term
-// a0 b0 + a1 b1 + (a0 - a1)(b1 - b0) taken from |a0 - a1| |b1 - b0| and the
-// sign of the factors.  3 h^2 word products instead of n^2, then the same
-// reduction as mont_sqr; the same bounds as mont_mul (a b < m R).
-template <int N>
+// z (2h words) = x y through LV Karatsuba levels (each level needs an even word
+// count; schoolbook below): x y = x0 y0 + (x0 y1 + x1 y0) 2^(32g) + x1 y1 2^(32h),
+// g = h/2, with the middle term x0 y0 + x1 y1 + (x0 - x1)(y1 - y0) taken from
+// |x0 - x1| |y1 - y0| and the sign of the factors: 3 products of g words.
+template <int H, int LV>
+VK_HD void kara_words(uint32_t *z, const uint32_t *x, const uint32_t *y) {
+    if constexpr (LV == 0 || H % 2 != 0 || H < 6) {
+        mul_words<H>(z, x, y);
+    } else {
+        constexpr int G = H / 2;
+        CARRY_DECL
+        kara_words<G, LV - 1>(z, x, y);
+        kara_words<G, LV - 1>(z + H, x + G, y + G);
+        // dx = |x0 - x1|, dy = |y1 - y0|: the difference, then (t ^ mask) - mask,
+        // which negates it when the subtraction borrowed (mask all ones)
+        uint32_t dx[G], dy[G], mx, my;
+        SUB_CC(dx[0], x[0], x[G]);
+#pragma unroll
+        for (int i = 1; i < G; i++) SUBC_CC(dx[i], x[i], x[G + i]);
+        SUBC(mx, 0u, 0u);
+        SUB_CC(dx[0], dx[0] ^ mx, mx);
+#pragma unroll
+        for (int i = 1; i < G; i++) SUBC_CC(dx[i], dx[i] ^ mx, mx);
+        SUB_CC(dy[0], y[G], y[0]);
+#pragma unroll
+        for (int i = 1; i < G; i++) SUBC_CC(dy[i], y[G + i], y[i]);
+        SUBC(my, 0u, 0u);
+        SUB_CC(dy[0], dy[0] ^ my, my);
+#pragma unroll
+        for (int i = 1; i < G; i++) SUBC_CC(dy[i], dy[i] ^ my, my);
+        uint32_t M[H];
+        kara_words<G, LV - 1>(M, dx, dy);
+        // mid = x0 y0 + x1 y1 +- M in h + 1 words (it equals x0 y1 + x1 y0 < 2^(32h + 1));
+        // -M is (M ^ s) + 1 with s all ones, the + 1 entering as the carry of s + 1
+        const uint32_t s = mx ^ my;
+        uint32_t mid[H + 1], dummy;
+        ADD_CC(mid[0], z[0], z[H]);
+#pragma unroll
+        for (int i = 1; i < H; i++) ADDC_CC(mid[i], z[i], z[H + i]);
+        ADDC(mid[H], 0u, 0u);
+        ADD_CC(dummy, s, 1u);
+#pragma unroll
+        for (int i = 0; i < H; i++) ADDC_CC(mid[i], mid[i], M[i] ^ s);
+        ADDC(mid[H], mid[H], s);
+        (void)dummy;
+        // z += mid 2^(32g); the full product is below 2^(64h), so the last word takes no carry out
+        ADD_CC(z[G], z[G], mid[0]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) ADDC_CC(z[G + i], z[G + i], mid[i]);
+#pragma unroll
+        for (int k = G + H + 1; k < 2 * H - 1; k++) ADDC_CC(z[k], z[k], 0u);
+        ADDC(z[2 * H - 1], z[2 * H - 1], 0u);
+    }
+}
+
+// Montgomery product with the 2n-word product through LV Karatsuba levels, then
+// the same reduction as mont_sqr; the same bounds as mont_mul (a b < m R).
+// One level for 12 words: 3 x 36 word products instead of 144.
+template <int N, int LV = 1>
 VK_HD void mont_mul_ks(uint32_t *r, const uint32_t *a, const uint32_t *b) {
-    static_assert(N % 2 == 0 && N >= 8, "even word count");
-    constexpr int H = N / 2;
-    CARRY_DECL
     uint32_t T[2 * N];
-    mul_words<H>(T, a, b);
-    mul_words<H>(T + N, a + H, b + H);
-    // da = |a0 - a1|, db = |b1 - b0|: the difference, then (t ^ mask) - mask,
-    // which negates it when the subtraction borrowed (mask all ones)
-    uint32_t da[H], db[H], ma, mb;
-    SUB_CC(da[0], a[0], a[H]);
-#pragma unroll
-    for (int i = 1; i < H; i++) SUBC_CC(da[i], a[i], a[H + i]);
-    SUBC(ma, 0u, 0u);
-    SUB_CC(da[0], da[0] ^ ma, ma);
-#pragma unroll
-    for (int i = 1; i < H; i++) SUBC_CC(da[i], da[i] ^ ma, ma);
-    SUB_CC(db[0], b[H], b[0]);
-#pragma unroll
-    for (int i = 1; i < H; i++) SUBC_CC(db[i], b[H + i], b[i]);
-    SUBC(mb, 0u, 0u);
-    SUB_CC(db[0], db[0] ^ mb, mb);
-#pragma unroll
-    for (int i = 1; i < H; i++) SUBC_CC(db[i], db[i] ^ mb, mb);
-    uint32_t M[N];
-    mul_words<H>(M, da, db);
-    // mid = a0 b0 + a1 b1 +- M in n + 1 words (it equals a0 b1 + a1 b0 < 2^(32n + 1));
-    // -M is (M ^ s) + 1 with s all ones, the + 1 entering as the carry of s + 1
-    const uint32_t s = ma ^ mb;
-    uint32_t mid[N + 1], dummy;
-    ADD_CC(mid[0], T[0], T[N]);
-#pragma unroll
-    for (int i = 1; i < N; i++) ADDC_CC(mid[i], T[i], T[N + i]);
-    ADDC(mid[N], 0u, 0u);
-    ADD_CC(dummy, s, 1u);
-#pragma unroll
-    for (int i = 0; i < N; i++) ADDC_CC(mid[i], mid[i], M[i] ^ s);
-    ADDC(mid[N], mid[N], s);
-    (void)dummy;
-    // T += mid 2^(32h); the full product is below 2^(64n), so the last word takes no carry out
-    ADD_CC(T[H], T[H], mid[0]);
-#pragma unroll
-    for (int i = 1; i <= N; i++) ADDC_CC(T[H + i], T[H + i], mid[i]);
-#pragma unroll
-    for (int k = H + N + 1; k < 2 * N - 1; k++) ADDC_CC(T[k], T[k], 0u);
-    ADDC(T[2 * N - 1], T[2 * N - 1], 0u);
+    kara_words<N, LV>(T, a, b);
     sos_reduce<N>(r, T);
 }
 
@@ -499,9 +532,9 @@ VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
 #ifndef VKZG_FP_INLINE
 #define VKZG_FP_INLINE 0
 #endif
-// The 12-limb product goes through one Karatsuba level (mont_mul_ks): 516
-// multiply instructions against 588 for CIOS, about 9% more products per second
-// on the integer pipe; VKZG_FP_KARATSUBA=0 selects CIOS.
+// The 12-limb product goes through VKZG_FP_KARATSUBA Karatsuba levels
+// (mont_mul_ks): one level is 516 multiply instructions against 588 for CIOS,
+// about 9% more products per second on the integer pipe; 0 selects CIOS.
 #ifndef VKZG_FP_KARATSUBA
 #define VKZG_FP_KARATSUBA 1
 #endif
@@ -509,7 +542,7 @@ VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
 __device__ __noinline__ Fp fp_mul_call(Fp a, Fp b) {
     Fp r;
 #if VKZG_FP_KARATSUBA
-    mont_mul_ks<12>(r.v, a.v, b.v);
+    mont_mul_ks<12, VKZG_FP_KARATSUBA>(r.v, a.v, b.v);
 #else
     mont_mul<12>(r.v, a.v, b.v);
 #endif
@@ -522,7 +555,7 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
 #else
     Fp r;
 #if VKZG_FP_KARATSUBA
-    mont_mul_ks<12>(r.v, a.v, b.v);
+    mont_mul_ks<12, VKZG_FP_KARATSUBA>(r.v, a.v, b.v);
 #else
     mont_mul<12>(r.v, a.v, b.v);
 #endif
@@ -532,7 +565,11 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_sqr_call(Fp a) {
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_sqr_ks<12>(r.v, a.v);
+#else
     mont_sqr<12>(r.v, a.v);
+#endif
     return r;
 }
 #endif
@@ -541,7 +578,11 @@ VK_HD Fp fp_sqr(const Fp &a) {
     return fp_sqr_call(a);
 #else
     Fp r;
+#if VKZG_FP_KARATSUBA
+    mont_sqr_ks<12>(r.v, a.v);
+#else
     mont_sqr<12>(r.v, a.v);
+#endif
     return r;
 #endif
 }

@@ -607,6 +607,17 @@ __device__ __forceinline__ G1A flat_load(const FlatArgs &a, uint32_t o, uint32_t
     return ld_vec(&a.src[(size_t)o * m + t]);
 }
 
+// the x coordinate of flat_load's point (0 for a zero digit)
+template <bool FIRST>
+__device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, uint32_t o, uint32_t t, uint32_t m) {
+    if (FIRST) {
+        const int v = a.dig[(size_t)o * a.L + t];
+        if (v == 0) return fp_zero();
+        return ldg_vec(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)].x);
+    }
+    return ld_vec(&a.src[(size_t)o * m + t].x);
+}
+
 // Signed c-bit digits of every scalar: scalar q = o 64 + i fills dig[q D ..].
 __global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, int c, int D,
                                                     int n_scalars) {
@@ -657,9 +668,10 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint
     int s = 0;
     uint32_t o = gl / h, i = gl % h;
     for (uint32_t p = gl; p < P; p += NL, s++) {
-        const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
+        const Fp x = flat_load_x<FIRST>(a, o, 2 * i, m), y = flat_load_x<FIRST>(a, o, 2 * i + 1, m);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<FIRST>(a, o, 2 * i, m); },
+                                             [&] { return flat_load<FIRST>(a, o, 2 * i + 1, m); }));
         pair_step_up(o, i, h, dq, dr);
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
@@ -935,6 +947,20 @@ __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &
     return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e]);
 }
 
+// the x coordinate of flatb_load's point
+template <bool FIRST>
+__device__ __forceinline__ Fp flatb_load_x(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
+                                           const uint32_t *offs, uint32_t o, int q, int k, uint32_t e) {
+    if (FIRST) {
+        const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
+        const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
+        const uint32_t b = o / kCells, aa = o % kCells - sr.off[q];
+        const uint32_t slot = sr.off[q] + ((aa - (uint32_t)tap) & (sr.size[q] - 1));
+        return ld_vec(&a.ladder_aff[((size_t)b * kCells + slot) * kDigits + d].x);
+    }
+    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e].x);
+}
+
 // pair p of the round -> output, part, bucket, index
 __device__ __forceinline__ void flatb_pair(const FlatBRound &sr, uint32_t p, uint32_t &o, int &q, int &k,
                                            uint32_t &i) {
@@ -965,10 +991,11 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, in
         uint32_t o, i;
         int q, k;
         flatb_pair(sr, p, o, q, k, i);
-        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
-        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
+        const Fp x = flatb_load_x<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
+        const Fp y = flatb_load_x<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i); },
+                                             [&] { return flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1); }));
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
@@ -1379,9 +1406,10 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, in
     int s = 0;
     for (uint32_t p = gl; p < P; p += NL, s++) {
         const uint32_t o = p / nops, q = p - o * nops;
-        const G1A x = ld_vec(red_slot(a, o, rr.a[q])), y = ld_vec(red_slot(a, o, rr.b[q]));
+        const G1A *pa = red_slot(a, o, rr.a[q]), *pb = red_slot(a, o, rr.b[q]);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
+        acc = fp_mul(acc, pair_denominator_x(ld_vec(&pa->x), ld_vec(&pb->x), [&] { return ld_vec(pa); },
+                                             [&] { return ld_vec(pb); }));
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
