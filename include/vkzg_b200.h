@@ -184,7 +184,8 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
  * 2: Fr (255-bit) multiplies in giga-ops/s; 3: Fp squares; 4: Fp multiplies through
  * one Karatsuba level; 5: Fr multiplies through one Karatsuba level; 6: Fp
  * squares through one Karatsuba level; 7: Fp multiplies through two Karatsuba
- * levels (all giga-ops/s).  Best of three timed launches.
+ * levels (all giga-ops/s); 8: mad.wide.u32 (32x32+64-bit) issue rate and 9:
+ * fma.rn.f64 issue rate, in tera-ops/s.  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
 

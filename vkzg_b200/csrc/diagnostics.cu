@@ -28,6 +28,40 @@ __global__ void __launch_bounds__(256) k_probe_imad(uint32_t seed, uint32_t *sin
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
+// 8 independent mad.wide.u32 chains per thread (64-bit addend and result):
+// 8 * kProbeIters wide multiply-adds per thread.
+__global__ void __launch_bounds__(256) k_probe_imad_wide(uint32_t seed, uint32_t *sink) {
+    uint64_t a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + threadIdx.x * 8 + k;
+    const uint32_t m = seed | 1u;
+    for (int i = 0; i < kProbeIters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(a[k]) : "r"(m), "r"((uint32_t)a[(k + 1) & 7]));
+    }
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc ^= a[k];
+    if ((uint32_t)acc == 0x12345678u) sink[0] = (uint32_t)(acc >> 32);
+}
+
+// 8 independent fma.rn.f64 chains per thread
+__global__ void __launch_bounds__(256) k_probe_dfma(uint32_t seed, uint32_t *sink) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = 1.0 + 1e-9 * (seed + threadIdx.x * 8 + k);
+    const double m = 1.0 - 1e-12 * seed;
+    for (int i = 0; i < kProbeIters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(a[k]) : "d"(m), "d"(a[(k + 1) & 7]));
+    }
+    double acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc += a[k];
+    if (acc == 0.125) sink[0] = 1u;
+}
+
 __device__ __noinline__ Fp fp_mul_ks_call(Fp a, Fp b) {
     Fp r;
     mont_mul_ks<12>(r.v, a.v, b.v);
@@ -219,7 +253,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 7) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 9) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -234,9 +268,11 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
     for (int rep = 0; rep < 4; rep++) {
         cudaEventRecord(e0);
         double ops = 0.0;
-        if (which == 0) {
+        if (which == 0 || which == 8 || which == 9) {
             const int blocks = sms * 8;
-            k_probe_imad<<<blocks, 256>>>(rep + 1, sink);
+            if (which == 0) k_probe_imad<<<blocks, 256>>>(rep + 1, sink);
+            else if (which == 8) k_probe_imad_wide<<<blocks, 256>>>(rep + 1, sink);
+            else k_probe_dfma<<<blocks, 256>>>(rep + 1, sink);
             ops = (double)blocks * 256 * 8 * kProbeIters;
         } else if (which != 2 && which != 5) {
             const int blocks = sms * 4;
@@ -259,7 +295,7 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        const double rate = ops / (ms * 1e-3) / (which == 0 ? 1e12 : 1e9);
+        const double rate = ops / (ms * 1e-3) / ((which == 0 || which >= 8) ? 1e12 : 1e9);
         if (rep > 0 && rate > best) best = rate;
     }
     cudaEventDestroy(e0);

@@ -716,9 +716,27 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint
             st_vec(&a.dst[(size_t)l * m_next + h], flat_load<FIRST>(a, l, m - 1, m));
 }
 
-__global__ void __launch_bounds__(128) k_flat_finish(const G1A *__restrict__ sums, G1J *points, int n) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o < n) st_vec(&points[o], g1_from_affine(ld_vec(&sums[o])));
+// The last m <= kTreeTail points of each list (affine, left by the tree
+// rounds) summed in Jacobian form: the rounds below that length cost an
+// inversion launch each for little work.  Two threads per list, each a chain of
+// mixed additions over alternate points, then one addition.
+constexpr uint32_t kTreeTail = 10;
+__global__ void __launch_bounds__(64) k_flat_finish(const G1A *__restrict__ lists, uint32_t m, G1J *points, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = t >> 1, h = t & 1;
+    G1J acc = g1_identity();
+    if (o < n) {
+        const G1A *l = lists + (size_t)o * m;
+        for (uint32_t k = h; k < m; k += 2) acc = g1_madd(acc, ld_vec(&l[k]));
+    }
+    G1J other;
+#pragma unroll
+    for (int w = 0; w < 12; w++) {
+        other.x.v[w] = __shfl_xor_sync(0xffffffffu, acc.x.v[w], 1);
+        other.y.v[w] = __shfl_xor_sync(0xffffffffu, acc.y.v[w], 1);
+        other.z.v[w] = __shfl_xor_sync(0xffffffffu, acc.z.v[w], 1);
+    }
+    if (o < n && h == 0) st_vec(&points[o], g1_add(acc, other));
 }
 
 int flat_blocks() {
@@ -744,17 +762,19 @@ FlatSizes flat_sizes(int cap, int c) {
     return z;
 }
 
-// Tree rounds from `first_src` (FIRST: the digit table) until every list is one
-// point; returns the buffer holding the sums and adds the launches to *launched.
+// Tree rounds from `first_src` (FIRST: the digit table) until every list has
+// at most `stop` points (their count left in *m); returns the buffer holding
+// the lists and adds the launches to *launched.
 template <bool FIRST>
-const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t m, G1A *buf0, G1A *buf1, int blocks,
-                           cudaStream_t s, int *launched) {
+const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t *m_io, uint32_t stop, G1A *buf0, G1A *buf1,
+                           int blocks, cudaStream_t s, int *launched) {
+    uint32_t m = *m_io;
     const int warps = blocks * kFlatThreads / 32;
     G1A *bufs[2] = {buf0, buf1};
     int out = 0;
     const G1A *cur = first_src;
     bool first = FIRST;
-    while (m > 1) {
+    while (m > stop) {
         a.src = cur;
         a.dst = bufs[out];
         if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
@@ -768,6 +788,7 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t m, G1A *bu
         m = (m + 1) >> 1;
         first = false;
     }
+    *m_io = m;
     return cur;
 }
 
@@ -785,7 +806,7 @@ int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *
     a.slots = slots;
     a.n_lists = n_lists;
     int launched = 0;
-    const G1A *res = run_tree_rounds<false>(a, lists, m, buf0, buf1, blocks, s, &launched);
+    const G1A *res = run_tree_rounds<false>(a, lists, &m, 1, buf0, buf1, blocks, s, &launched);
     cudaMemcpyAsync(sums, res, (size_t)n_lists * sizeof(G1A), cudaMemcpyDeviceToDevice, s);
     count_launches(launched);
     return launched;
@@ -810,9 +831,10 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.n_lists = lists;
     int launched = 1;
     k_flat_digits<<<(lists * kCellElems + 127) / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
+    uint32_t m = (uint32_t)L;
     const G1A *res =
-        run_tree_rounds<true>(a, nullptr, (uint32_t)L, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s, &launched);
-    k_flat_finish<<<(lists + 127) / 128, 128, 0, s>>>(res, w.points, lists);
+        run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s, &launched);
+    k_flat_finish<<<(2 * lists + 63) / 64, 64, 0, s>>>(res, m, w.points, lists);
     return launched + 1;
 }
 
@@ -1243,12 +1265,16 @@ constexpr int kRedOutputs = 128;                 // outputs per block (one blob)
 constexpr int kRedThreads = 256;
 constexpr int kRedMaxPairs = 96 * kRedOutputs / kRedThreads; // round 1 has the most operations (96)
 
+// The last kRedTail rounds (8 and 1 operations per output) are not run as
+// rounds: the Horner step adds their operands instead, so each Horner term
+// T_b (terms 0..6) and S (term 7) is a sum of up to 4 slots of the earlier rounds.
+constexpr int kRedTail = 2;
 struct ReduceSchedule {
     uint16_t dst[kRedOps], a[kRedOps], b[kRedOps];
     uint16_t round_start[kRedMaxRounds + 1];
-    uint16_t t_slot[7];
-    uint16_t all_slot;
-    int n_rounds;
+    uint16_t term_slot[8][4];
+    uint8_t term_n[8];
+    int n_rounds; // rounds run as batch-affine rounds
 };
 __constant__ ReduceSchedule c_red;
 
@@ -1266,6 +1292,7 @@ static bool build_reduce_schedule(ReduceSchedule &s) {
     };
     std::vector<int> cur(kBuckets);
     for (int i = 0; i < kBuckets; i++) cur[i] = i;
+    int t_slot[8];
     for (int j = 0; j < 7; j++) {
         std::vector<int> odd;
         for (size_t m = 1; m < cur.size(); m += 2) odd.push_back(cur[m]);
@@ -1277,10 +1304,10 @@ static bool build_reduce_schedule(ReduceSchedule &s) {
             if (odd.size() & 1) nl.push_back(odd.back());
             odd.swap(nl);
         }
-        s.t_slot[j] = (uint16_t)odd[0];
+        t_slot[j] = odd[0];
         cur.swap(nxt);
     }
-    s.all_slot = (uint16_t)cur[0];
+    t_slot[7] = cur[0];
     if ((int)ops.size() != kRedOps) return false;
     std::stable_sort(ops.begin(), ops.end(), [](const Op &x, const Op &y) { return x.round < y.round; });
     int nr = 0;
@@ -1290,8 +1317,27 @@ static bool build_reduce_schedule(ReduceSchedule &s) {
         s.b[q] = (uint16_t)ops[q].b;
         nr = std::max(nr, ops[q].round);
     }
-    if (nr > kRedMaxRounds) return false;
-    s.n_rounds = nr;
+    if (nr > kRedMaxRounds || nr <= kRedTail) return false;
+    s.n_rounds = nr - kRedTail;
+    // Horner terms: a slot made in a tail round expands into its two operands
+    std::vector<int> op_of(kRedSlots, -1);
+    for (int q = 0; q < kRedOps; q++) op_of[ops[q].dst] = q;
+    for (int j = 0; j < 8; j++) {
+        std::vector<int> todo{t_slot[j]}, terms;
+        while (!todo.empty()) {
+            const int x = todo.back();
+            todo.pop_back();
+            if (x >= kBuckets && ready[x] > s.n_rounds) {
+                todo.push_back(ops[op_of[x]].a);
+                todo.push_back(ops[op_of[x]].b);
+            } else {
+                terms.push_back(x);
+            }
+        }
+        if (terms.size() > 4) return false;
+        s.term_n[j] = (uint8_t)terms.size();
+        for (size_t k = 0; k < terms.size(); k++) s.term_slot[j][k] = (uint16_t)terms[k];
+    }
     int q = 0;
     for (int r = 1; r <= nr; r++) {
         s.round_start[r - 1] = (uint16_t)q;
@@ -1301,6 +1347,18 @@ static bool build_reduce_schedule(ReduceSchedule &s) {
     for (int r = 0; r < nr; r++)
         if ((s.round_start[r + 1] - s.round_start[r]) * kRedOutputs > kRedMaxPairs * kRedThreads) return false;
     return true;
+}
+
+// sum_b 2^b T_b + S from the Horner terms (mixed additions of affine slots)
+template <class Load>
+__device__ __forceinline__ G1J red_horner(Load load) {
+    G1J h = g1_identity();
+    for (int j = 6; j >= 0; j--) {
+        if (j < 6) h = g1_dbl(h);
+        for (int k = 0; k < c_red.term_n[j]; k++) h = g1_madd(h, load(c_red.term_slot[j][k]));
+    }
+    for (int k = 0; k < c_red.term_n[7]; k++) h = g1_madd(h, load(c_red.term_slot[7][k]));
+    return h;
 }
 
 __global__ void __launch_bounds__(kRedThreads, 2) k_reduce_hier(const G1A *__restrict__ bucket_aff, G1J *out,
@@ -1339,14 +1397,8 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_reduce_hier(const G1A *__res
         __syncthreads();
     }
     // Horner: H = sum_b 2^b T_b, then + S
-    for (int g = threadIdx.x; g < go; g += kRedThreads) {
-        G1J h = g1_from_affine(ld_vec(slot(g, c_red.t_slot[6])));
-        for (int j = 5; j >= 0; j--) {
-            h = g1_dbl(h);
-            h = g1_madd(h, ld_vec(slot(g, c_red.t_slot[j])));
-        }
-        st_vec(&out[o0 + g], g1_madd(h, ld_vec(slot(g, c_red.all_slot))));
-    }
+    for (int g = threadIdx.x; g < go; g += kRedThreads)
+        st_vec(&out[o0 + g], red_horner([&](int x) { return ld_vec(slot(g, x)); }));
 }
 
 cudaError_t configure_reduce_schedule() {
@@ -1440,12 +1492,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, in
 __global__ void __launch_bounds__(128) k_flatr_horner(FlatRArgs a, G1J *out) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= (uint32_t)a.n_out) return;
-    G1J h = g1_from_affine(ld_vec(red_slot(a, o, c_red.t_slot[6])));
-    for (int j = 5; j >= 0; j--) {
-        h = g1_dbl(h);
-        h = g1_madd(h, ld_vec(red_slot(a, o, c_red.t_slot[j])));
-    }
-    st_vec(&out[o], g1_madd(h, ld_vec(red_slot(a, o, c_red.all_slot))));
+    st_vec(&out[o], red_horner([&](int x) { return ld_vec(red_slot(a, o, x)); }));
 }
 
 // sum_k (k + 1) B_k of every output into out; returns the launches made
