@@ -48,9 +48,28 @@ PHASE_A_FP_MUL_PER_BLOB = 2.87e6     # ~261k madd-2007-bl (11 Fp mul) per blob
 PROOF_IMAD_PER_BLOB = 3.36e9         # 5.81M Fp mul + 74k Fr mul
 RECOVERY_IMAD_PER_BLOB = 118e6       # 0.46M Fr mul (4 NTT-8192 + pointwise + batch division)
 NOMINAL_IMAD_TPS = 148 * 64 * 1.965e9 / 1e12
+# this library's Fp product (one Karatsuba level + word-serial reduction) and square
+IMAD_FP_MUL_KS, IMAD_FP_SQR_KS = 516, 426
+PHASE_A_TAIL = 10  # lists of at most this many points finish in Jacobian form
+
+
+def phase_a_executed_imad_per_output(c):
+    """Multiply instructions plan 3's phase A executes per MSM output at window c:
+    affine additions (5 products + 1 square) in tree rounds down to lists of
+    PHASE_A_TAIL points, then mixed additions (7 + 4) on two chains and one
+    Jacobian addition (11 + 5)."""
+    m = 64 * ((256 + c - 1) // c)
+    adds = 0
+    while m > PHASE_A_TAIL:
+        adds += m // 2
+        m = (m + 1) // 2
+    madds = max(m - 2, 0)
+    muls = 5 * adds + 7 * madds + 11
+    sqrs = adds + 4 * madds + 5
+    return muls * IMAD_FP_MUL_KS + sqrs * IMAD_FP_SQR_KS
 # DRAM bytes of phase A per blob under plan 3 (13-bit digit table), from one
-# single-pass ncu capture of a 256-blob proof step (32.3 GB / 256)
-PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 = 32.3e9 / 256
+# single-pass ncu capture of a 256-blob proof step (30.9 GB / 256)
+PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 = 30.9e9 / 256
 
 
 # ------------------------------------------------------------------ inputs
@@ -441,9 +460,7 @@ def run_ours(args, rank, world, local_rank):
     plan = tuning.get(n, (None,))[0] if n in tuning else None
     executed = None
     if plan == 3 and digit:
-        # plan 3 executes 64 ceil(256 / c) - 1 affine additions (6 Fp multiplies each) per output
-        d_windows = (256 + digit[0] - 1) // digit[0]
-        executed = 128 * (64 * d_windows - 1) * 6 * IMAD_FP * n / (pa_ms / 1e3) / 1e12
+        executed = 128 * phase_a_executed_imad_per_output(digit[0]) * n / (pa_ms / 1e3) / 1e12
     stages = dict(stages_acc)
     p_ms = statistics.mean(proof_ms)
     rec_ms = statistics.mean(step_ms) - p_ms
@@ -494,7 +511,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic": f"{PHASE_A_FP_MUL_PER_BLOB:.3g} Fp mul x 576 IMAD per blob x {n} blobs: the "
                                     "reference algorithm's phase-A work (madd-2007-bl bucket accumulation); "
                                     "frac above 1 = fewer operations than the reference, frac_executed = the "
-                                    "Fp multiplies this kernel executes",
+                                    "multiply instructions this kernel executes (516 per Fp product, 426 per "
+                                    "square)",
                      "traffic": PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 * n if plan == 3 and digit and digit[0] == 13
                      else None,
                      "traffic_unit": "bytes per phase-A pass over the batch (ncu dram__bytes_read + write)"},
