@@ -185,7 +185,10 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
  * one Karatsuba level; 5: Fr multiplies through one Karatsuba level; 6: Fp
  * squares through one Karatsuba level; 7: Fp multiplies through two Karatsuba
  * levels (all giga-ops/s); 8: mad.wide.u32 (32x32+64-bit) issue rate and 9:
- * fma.rn.f64 issue rate, in tera-ops/s.  Best of three timed launches.
+ * fma.rn.f64 issue rate, in tera-ops/s; 10 and 11: the time in microseconds of
+ * one launch inverting 16 Fp values per SM, one per thread (the inversion
+ * between the passes of a batch-affine round), with variable-time and with
+ * fixed 30-divstep batches.  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
 

@@ -150,6 +150,11 @@ void shim_fp_inv_fast(const uint32_t *a, uint32_t *r) {
     memcpy(x.v, a, 48);
     memcpy(r, fp_inv_fast(x).v, 48);
 }
+void shim_fp_inv_var(const uint32_t *a, uint32_t *r) {
+    Fp x;
+    memcpy(x.v, a, 48);
+    memcpy(r, fp_inv_fast<true>(x).v, 48);
+}
 void shim_fr_inv_fast(const uint32_t *a, uint32_t *r) {
     Fr x;
     memcpy(x.v, a, 32);

@@ -100,18 +100,22 @@ def test_curve_ops(shim, oracle, mainnet_setup):
 
 @pytest.mark.parametrize("field", ["fp", "fr"])
 def test_divstep_inverse(shim, field):
-    """Batched-divstep inversion (Montgomery in, Montgomery out) equals x^-1."""
+    """Batched-divstep inversion (Montgomery in, Montgomery out) equals x^-1, with
+    fixed 30-divstep batches (the default) and, for Fp, in variable time."""
     mod, n, radix = (P_MOD, 12, 1 << 384) if field == "fp" else (R_MOD, 8, 1 << 256)
     rng = random.Random(11)
     vals = [1, 2, 3, mod - 1, mod - 2, (mod - 1) // 2, 1 << 200, (1 << 250) + 1, radix % mod]
     vals += [rng.randrange(1, mod) for _ in range(3000)]
     out = (ctypes.c_uint32 * n)()
-    fn = getattr(shim, f"shim_{field}_inv_fast")
-    for x in vals:
-        fn(words(x * radix % mod, n), out)
-        assert value(out, n) == pow(x, -1, mod) * radix % mod, hex(x)
-    fn(words(0, n), out)
-    assert value(out, n) == 0
+    fns = [getattr(shim, f"shim_{field}_inv_fast")]
+    if field == "fp":
+        fns.append(shim.shim_fp_inv_var)  # the variable-time divstep batches
+    for fn in fns:
+        for x in vals:
+            fn(words(x * radix % mod, n), out)
+            assert value(out, n) == pow(x, -1, mod) * radix % mod, hex(x)
+        fn(words(0, n), out)
+        assert value(out, n) == 0
 
 
 Z2 = 0xD201000000010000 ** 2
