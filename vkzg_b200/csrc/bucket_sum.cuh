@@ -55,6 +55,19 @@ __device__ __forceinline__ Fp pair_denominator_x(const Fp &ax, const Fp &bx, Loa
     return pair_denominator(a, b, pair_kind(a, b));
 }
 
+// INL: the products inlined instead of out-of-line calls
+template <bool INL>
+__device__ __forceinline__ Fp pmul(const Fp &a, const Fp &b) {
+    if constexpr (INL) return fp_mul_inl(a, b);
+    else return fp_mul(a, b);
+}
+template <bool INL>
+__device__ __forceinline__ Fp psqr(const Fp &a) {
+    if constexpr (INL) return fp_sqr_inl(a);
+    else return fp_sqr(a);
+}
+
+template <bool INL = false>
 __device__ __forceinline__ G1A pair_result(const G1A &a, const G1A &b, int kind, const Fp &inv_den) {
     if (kind == 2) return a;
     if (kind == 3) return b;
@@ -68,13 +81,13 @@ __device__ __forceinline__ G1A pair_result(const G1A &a, const G1A &b, int kind,
     if (kind == 0) {
         num = fp_sub(b.y, a.y);
     } else {
-        const Fp xx = fp_sqr(a.x);
+        const Fp xx = psqr<INL>(a.x);
         num = fp_add(fp_dbl(xx), xx);
     }
-    const Fp lam = fp_mul(num, inv_den);
+    const Fp lam = pmul<INL>(num, inv_den);
     G1A r;
-    r.x = fp_sub(fp_sub(fp_sqr(lam), a.x), b.x);
-    r.y = fp_sub(fp_mul(lam, fp_sub(a.x, r.x)), a.y);
+    r.x = fp_sub(fp_sub(psqr<INL>(lam), a.x), b.x);
+    r.y = fp_sub(pmul<INL>(lam, fp_sub(a.x, r.x)), a.y);
     return r;
 }
 
