@@ -68,6 +68,8 @@ struct FlatBPlan {
     uint32_t base[kFBMaxRounds + 1][kFBMaxParts][kBuckets + 1];
     uint32_t pscan[kFBMaxRounds][kFBMaxParts][kBuckets + 1];
     uint8_t odd[kFBMaxRounds][kFBMaxParts][kBuckets];
+    uint32_t n_empty[kFBMaxParts];              // buckets no tap digit reaches, per part
+    uint8_t empty[kFBMaxParts][kBuckets];
 };
 bool build_flatb_plan(const PartLayout &parts, const uint32_t offsets[][kBuckets + 1], FlatBPlan &plan);
 

@@ -851,15 +851,19 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
 // round: the round structure is a setup constant (FlatBPlan, built on the host)
 // and the pairs of all outputs are dealt to all lanes as in phase A.  Round r
 // keeps bucket k of output o (part q) at buf[o * stride[r] + base[r][q][k] ..];
-// the last round leaves one point or none per bucket, scattered into
-// bucket_aff for the reduction.
+// the last round writes each bucket's sum straight to bucket_aff[o][k] (at most
+// two elements are left per bucket then) and infinity to the buckets no digit
+// reaches, for the reduction.
 bool build_flatb_plan(const PartLayout &parts, const uint32_t offsets[][kBuckets + 1], FlatBPlan &pl) {
     memset(&pl, 0, sizeof pl);
     if (parts.n < 1 || parts.n > kFBMaxParts) return false;
     pl.parts = parts;
     uint32_t cnt[kFBMaxParts][kBuckets];
     for (int q = 0; q < parts.n; q++)
-        for (int k = 0; k < kBuckets; k++) cnt[q][k] = offsets[q][k + 1] - offsets[q][k];
+        for (int k = 0; k < kBuckets; k++) {
+            cnt[q][k] = offsets[q][k + 1] - offsets[q][k];
+            if (!cnt[q][k]) pl.empty[q][pl.n_empty[q]++] = (uint8_t)k;
+        }
     int r = 0;
     for (;; r++) {
         if (r > kFBMaxRounds) return false;
@@ -902,6 +906,7 @@ struct FlatBArgs {
     const uint32_t *offsets; // [kFBMaxParts][kBuckets + 1]
     const G1A *src;
     G1A *dst;
+    G1A *bucket_aff; // the last round's destination, [output][kBuckets]
     uint32_t *pre;
     Fp *others, *tot, *totinv;
     size_t slots;
@@ -1039,6 +1044,7 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
     const uint32_t wg = gl >> 5;
     const uint32_t P = sr.pair_end[sr.n_parts - 1];
     const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
+    const bool last = r + 1 == a.plan->rounds;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
     for (int t = S - 1; t >= 0; t--) {
@@ -1052,7 +1058,8 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
         const Fp den = pair_denominator(x, y, kind);
         const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
         inv = fp_mul(inv, den);
-        st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + i], pair_result(x, y, kind, inv_den));
+        G1A *d = last ? &a.bucket_aff[(size_t)o * kBuckets + k] : &a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + i];
+        st_vec(d, pair_result(x, y, kind, inv_den));
     }
     // odd last elements move up unchanged
     const FlatBPlan &pl = *a.plan;
@@ -1069,31 +1076,30 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
             const int k = pl.odd[r][q][j];
             const uint32_t o = (ol / m) * kCells + sr.off[q] + ol % m;
             const uint32_t c = sr.cnt[q][k];
-            st_vec(&a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + (c >> 1)],
-                   flatb_load<FIRST>(a, sr, items, offs, o, q, k, c - 1));
+            G1A *d = last ? &a.bucket_aff[(size_t)o * kBuckets + k]
+                          : &a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + (c >> 1)];
+            st_vec(d, flatb_load<FIRST>(a, sr, items, offs, o, q, k, c - 1));
         }
         odd_begin += odd_q;
     }
-}
-
-// bucket_aff[o][k] from the last round (infinity for empty buckets)
-__global__ void __launch_bounds__(128) k_flatb_finish(const FlatBPlan *__restrict__ plan, const G1A *__restrict__ last,
-                                                     G1A *bucket_aff, int n_out) {
-    const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= (size_t)n_out * kBuckets) return;
-    const uint32_t o = (uint32_t)(x / kBuckets), k = (uint32_t)(x % kBuckets);
-    const uint32_t slot = o % kCells;
-    int q = 0;
-    while (q + 1 < plan->parts.n && slot >= plan->parts.off[q + 1]) q++;
-    const int R = plan->rounds;
-    G1A v;
-    if (plan->cnt[R][q][k]) {
-        v = ld_vec(&last[(size_t)o * plan->stride[R] + plan->base[R][q][k]]);
-    } else {
-        v.x = fp_zero();
-        v.y = fp_zero();
+    if (last) { // infinity in the buckets of a part that no digit reaches
+        size_t e_begin = 0;
+        for (int q = 0; q < sr.n_parts; q++) {
+            const uint32_t ne = pl.n_empty[q], m = sr.size[q];
+            const size_t e_q = (size_t)a.n_blobs * m * ne;
+            const size_t first = e_begin + (gl + NL - e_begin % NL) % NL;
+            for (size_t x = first; x < e_begin + e_q; x += NL) {
+                const size_t xx = x - e_begin;
+                const uint32_t ol = (uint32_t)(xx / ne), j = (uint32_t)(xx - (size_t)ol * ne);
+                const uint32_t o = (ol / m) * kCells + sr.off[q] + ol % m;
+                G1A z;
+                z.x = fp_zero();
+                z.y = fp_zero();
+                st_vec(&a.bucket_aff[(size_t)o * kBuckets + pl.empty[q][j]], z);
+            }
+            e_begin += e_q;
+        }
     }
-    st_vec(&bucket_aff[x], v);
 }
 
 // Phase B of plan 3 into w.bucket_aff; returns the number of kernels launched.
@@ -1103,6 +1109,7 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
     a.ladder_aff = w.ladder_aff;
     a.items = t.part_items;
     a.offsets = t.part_offsets;
+    a.bucket_aff = w.bucket_aff;
     a.pre = w.flat_pre;
     a.others = w.flat_others;
     a.tot = w.flat_tot;
@@ -1125,8 +1132,7 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
         cur = bufs[out];
         out ^= 1;
     }
-    k_flatb_finish<<<(n * kCells * kBuckets + 127) / 128, 128, 0, s>>>(t.fb_plan, cur, w.bucket_aff, n * kCells);
-    return launched + 1;
+    return launched;
 }
 
 // Bases of the digit table: B[j][i][k] = 2^(c k) X[j][i], from the position
