@@ -619,19 +619,28 @@ __device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, uint32_t o, uint32_
 }
 
 // Signed c-bit digits of every scalar: scalar q = o 64 + i fills dig[q D ..].
+// A block's 128 scalars are recoded into shared memory and written out as one
+// contiguous run of 16-byte stores (a thread's own digits are D x 2 bytes apart
+// from its neighbour's: direct stores would scatter).  n_scalars is a multiple
+// of 128 (64 scalars per list, 128 lists per blob).
+constexpr int kDigitMaxWindows = 26; // c >= 10
 __global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, int c, int D,
                                                     int n_scalars) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n_scalars) return;
+    __shared__ __align__(16) int16_t sd[128 * kDigitMaxWindows];
+    const int q0 = blockIdx.x * 128, q = q0 + threadIdx.x;
+    if (q0 >= n_scalars) return;
     const Fr sc = ld_vec(&scalars[q]);
-    int16_t *d = dig + (size_t)q * D;
     const int H = 1 << (c - 1);
     int carry = 0;
     for (int k = 0; k < D; k++) {
         const int v = (int)scalar_window(sc, k * c, c) + carry;
         carry = v > H ? 1 : 0;
-        d[k] = (int16_t)(v - (carry << c));
+        sd[threadIdx.x * D + k] = (int16_t)(v - (carry << c));
     }
+    __syncthreads();
+    const uint4 *src = reinterpret_cast<const uint4 *>(sd);
+    uint4 *dst = reinterpret_cast<uint4 *>(dig + (size_t)q0 * D); // 256 D bytes per block: 16-byte aligned
+    for (int x = threadIdx.x; x < 16 * D; x += 128) dst[x] = src[x];
 }
 
 // Pair p = o h + i of a round (list o, pair i); a lane walks p = gl, gl + NL,
@@ -837,7 +846,7 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.slots = w.flat_slots;
     a.n_lists = lists;
     int launched = 1;
-    k_flat_digits<<<(lists * kCellElems + 127) / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
+    k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
     uint32_t m = (uint32_t)L;
     const G1A *res =
         run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s, &launched);
