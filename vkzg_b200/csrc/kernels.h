@@ -54,6 +54,20 @@ inline PartLayout part_layout(int levels) {
     return L;
 }
 
+// Pair sums shared by the buckets of a part (plans 3-4): when the same pair of
+// tap items -- rows a and b of the ladder, taps e and e + delta, relative sign
+// s -- falls into two or more buckets of a part, the part's outputs share
+//   M[x] = L_a[x] + s L~_b[x - delta],   x < n,
+// (L~ the ladder row extended cyclically or negacyclically like the part), and
+// each such pair becomes one tap item (e, digit slot 32 + t, sign of the first):
+// M~ obeys the same extension rule, so it is read like a ladder row.
+constexpr int kMaxPartTypes = 256 - kDigits; // digit slots 32..255
+struct DerivType {
+    uint8_t part, row_a, row_b, neg; // neg: s = -1
+    uint32_t delta;                  // 0 <= delta < n
+    uint32_t base;                   // first point of M in a blob's derived array
+};
+
 // Round structure of plan 3's phase B (see build_flatb_plan): per round r and
 // part q, each bucket's list length, element offsets, pair offsets and odd
 // buckets, identical for every output of a part.
@@ -86,6 +100,11 @@ struct DeviceTables {
     Fr *inv_blob_r2 = nullptr;      // [1] (1/4096) in Montgomery form
     uint32_t *part_items = nullptr;   // plans 3-4: tap items of the kPartLevels parts, part q from 32 * off[q]
     uint32_t *part_offsets = nullptr; // [kFBMaxParts][129]
+    DerivType *deriv = nullptr;       // plans 3-4: the shared pair sums
+    uint16_t *deriv_of = nullptr;     // [deriv_points] type of each derived point
+    uint32_t deriv_points = 0;        // derived points per blob
+    int deriv_types = 0;
+    uint32_t deriv_base[kFBMaxParts] = {}; // first derived point of part q (type t: + t n_q)
     FlatBPlan *fb_plan = nullptr;   // plan 3's phase-B rounds
     int fb_rounds = 0;              // 0: plan 3 uses the per-warp phase B
     uint32_t fb_stride[2] = {0, 0}; // elements per output after rounds 1 and 2
@@ -100,6 +119,7 @@ struct ProofWork {
     G1J *points = nullptr;      // [cap][128] reduce outputs
     G1J *ladder = nullptr;      // [cap][128][16] 2^(8d) v[j] of the folded parts
     G1A *ladder_aff = nullptr;  // [cap][128][32]: d < 16 the ladder, d >= 16 its phi images
+    G1A *deriv_buf = nullptr;   // plans 3-4: [cap][deriv_points] shared pair sums
     uint8_t *proofs = nullptr;  // [cap][128][48]
     uint32_t *err = nullptr;    // [cap]
     // batch-affine accumulation (plans 1, 2)

@@ -916,6 +916,9 @@ struct FlatBArgs {
     const G1A *src;
     G1A *dst;
     G1A *bucket_aff; // the last round's destination, [output][kBuckets]
+    const G1A *deriv_buf; // [blob][deriv_points] shared pair sums
+    uint32_t deriv_points;
+    uint32_t deriv_base[kFBMaxParts];
     uint32_t *pre;
     Fp *others, *tot, *totinv;
     size_t slots;
@@ -974,6 +977,13 @@ __device__ void flatb_stage(const FlatBArgs &a, int r, FlatBRound &sr, uint32_t 
     __syncthreads();
 }
 
+// point x (< n) of row d of part q of blob b: a ladder row (d < 32) or a shared pair sum
+__device__ __forceinline__ const G1A *flatb_src(const FlatBArgs &a, const FlatBRound &sr, uint32_t b, int q,
+                                                uint32_t x, int d) {
+    if (d < kDigits) return &a.ladder_aff[((size_t)b * kCells + sr.off[q] + x) * kDigits + d];
+    return &a.deriv_buf[(size_t)b * a.deriv_points + a.deriv_base[q] + (uint32_t)(d - kDigits) * sr.size[q] + x];
+}
+
 // element e of bucket k of output o (part q)
 template <bool FIRST>
 __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
@@ -982,8 +992,7 @@ __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &
         const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
         const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
         const uint32_t b = o / kCells, aa = o % kCells - sr.off[q];
-        const uint32_t slot = sr.off[q] + ((aa - (uint32_t)tap) & (sr.size[q] - 1));
-        G1A pt = ld_vec(&a.ladder_aff[((size_t)b * kCells + slot) * kDigits + d]);
+        G1A pt = ld_vec(flatb_src(a, sr, b, q, (aa - (uint32_t)tap) & (sr.size[q] - 1), d));
         if (((packed >> 16) & 1u) != (sr.nega[q] && tap > (int)aa)) pt.y = fp_neg(pt.y);
         return pt;
     }
@@ -998,8 +1007,7 @@ __device__ __forceinline__ Fp flatb_load_x(const FlatBArgs &a, const FlatBRound 
         const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
         const int tap = (int)(packed & 0xffu), d = (int)((packed >> 8) & 0xffu);
         const uint32_t b = o / kCells, aa = o % kCells - sr.off[q];
-        const uint32_t slot = sr.off[q] + ((aa - (uint32_t)tap) & (sr.size[q] - 1));
-        return ld_vec(&a.ladder_aff[((size_t)b * kCells + slot) * kDigits + d].x);
+        return ld_vec(&flatb_src(a, sr, b, q, (aa - (uint32_t)tap) & (sr.size[q] - 1), d)->x);
     }
     return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e].x);
 }
@@ -1111,6 +1119,102 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
     }
 }
 
+// The shared pair sums of phase B as one grid-wide round: point m of blob b is
+// x = m - base of its type; its pair is L_a[x] and s L~_b[x - delta].
+struct DerivArgs {
+    const DerivType *types;
+    const uint16_t *type_of;
+    const G1A *ladder_aff;
+    G1A *out;
+    PartLayout parts;
+    uint32_t points; // per blob
+    uint32_t *pre;
+    Fp *others, *tot, *totinv;
+    size_t slots_pre;
+    int n_blobs;
+};
+
+__device__ __forceinline__ void deriv_pair(const DerivArgs &a, uint32_t p, const G1A *&pa, const G1A *&pb,
+                                           bool &neg_b) {
+    const uint32_t b = p / a.points, m = p - b * a.points;
+    const DerivType ty = a.types[a.type_of[m]];
+    const uint32_t n = a.parts.size[ty.part], off = a.parts.off[ty.part];
+    const uint32_t x = m - ty.base;
+    const bool wrap = x < ty.delta;
+    const uint32_t xb = wrap ? x + n - ty.delta : x - ty.delta;
+    pa = &a.ladder_aff[((size_t)b * kCells + off + x) * kDigits + ty.row_a];
+    pb = &a.ladder_aff[((size_t)b * kCells + off + xb) * kDigits + ty.row_b];
+    neg_b = (ty.neg != 0) != (wrap && a.parts.nega[ty.part]);
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass1(DerivArgs a) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    const uint32_t P = (uint32_t)a.n_blobs * a.points;
+    uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
+    Fp acc = fp_one();
+    int s = 0;
+    for (uint32_t p = gl; p < P; p += NL, s++) {
+        const G1A *pa, *pb;
+        bool nb;
+        deriv_pair(a, p, pa, pb, nb);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator_x(ld_vec(&pa->x), ld_vec(&pb->x), [&] { return ld_vec(pa); },
+                                             [&] {
+                                                 G1A y = ld_vec(pb);
+                                                 if (nb) y.y = fp_neg(y.y);
+                                                 return y;
+                                             }));
+    }
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
+__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass2(DerivArgs a) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    const uint32_t wg = gl >> 5;
+    const uint32_t P = (uint32_t)a.n_blobs * a.points;
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    for (int t = S - 1; t >= 0; t--) {
+        const uint32_t p = gl + (uint32_t)t * NL;
+        const G1A *pa, *pb;
+        bool nb;
+        deriv_pair(a, p, pa, pb, nb);
+        const G1A x = ld_vec(pa);
+        G1A y = ld_vec(pb);
+        if (nb) y.y = fp_neg(y.y);
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
+        inv = fp_mul(inv, den);
+        st_vec(&a.out[p], pair_result(x, y, kind, inv_den));
+    }
+}
+
+// the shared pair sums into w.deriv_buf; returns the launches made (0 without any)
+int launch_deriv_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    if (!t.deriv_points) return 0;
+    DerivArgs a;
+    a.types = t.deriv;
+    a.type_of = t.deriv_of;
+    a.ladder_aff = w.ladder_aff;
+    a.out = w.deriv_buf;
+    a.parts = part_layout(kPartLevels);
+    a.points = t.deriv_points;
+    a.pre = w.flat_pre;
+    a.others = w.flat_others;
+    a.tot = w.flat_tot;
+    a.totinv = w.flat_totinv;
+    a.slots_pre = w.flat_slots;
+    a.n_blobs = n;
+    const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
+    k_deriv_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
+    k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
+    k_deriv_pass2<<<blocks, kFlatThreads, 0, s>>>(a);
+    return 3;
+}
+
 // Phase B of plan 3 into w.bucket_aff; returns the number of kernels launched.
 int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
     FlatBArgs a;
@@ -1119,6 +1223,9 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
     a.items = t.part_items;
     a.offsets = t.part_offsets;
     a.bucket_aff = w.bucket_aff;
+    a.deriv_buf = w.deriv_buf;
+    a.deriv_points = t.deriv_points;
+    for (int q = 0; q < kFBMaxParts; q++) a.deriv_base[q] = t.deriv_base[q];
     a.pre = w.flat_pre;
     a.others = w.flat_others;
     a.tot = w.flat_tot;
@@ -1676,6 +1783,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     else k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, w.ladder_aff, n_lad);
     mark();
     if (flatb) {
+        launched += launch_deriv_flat(t, w, n, s);
         launched += launch_phase_b_flat(t, w, n, s) - 1;
     } else if (affine) {
         k_phase_b_affine<<<ba_grid, kBAThreads, kPhaseBSmem, s>>>(w.ladder_aff, t.tap_items[0], t.tap_offsets[0],

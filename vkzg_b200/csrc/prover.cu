@@ -290,9 +290,13 @@ bool host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2],
 
 // Tap items of the parts of `levels` folds (part_layout), split for phi: the
 // taps fold like the points, t+-[e] = (t[e] +- t[e + m]) / 2.  items holds
-// 32 * 128 entries, part q's from 32 * off[q].
+// 32 * 128 entries, part q's from 32 * off[q].  Then, per part, pairs of items
+// that share a bucket are replaced by one item on a shared pair sum (DerivType)
+// wherever the same pair -- rows, tap distance, relative sign -- occurs in two
+// or more buckets: greedily, the most frequent pair first, each item used once.
+// A shared pair sum costs n additions per blob and saves n per extra use.
 bool host_part_tables(const std::vector<Fr> &fwd, int levels, std::vector<uint32_t> &items,
-                      uint32_t offsets[kFBMaxParts][kBuckets + 1]) {
+                      uint32_t offsets[kFBMaxParts][kBuckets + 1], std::vector<DerivType> &types) {
     const PartLayout L = part_layout(levels);
     Fr v[kCells];
     host_taps128(fwd, v);
@@ -310,12 +314,77 @@ bool host_part_tables(const std::vector<Fr> &fwd, int levels, std::vector<uint32
     taps[0].assign(v, v + (kCells >> levels));
     items.assign((size_t)kCells * kDigits, 0);
     memset(offsets, 0, sizeof(uint32_t) * kFBMaxParts * (kBuckets + 1));
+    types.clear();
+    struct Item {
+        int e, d, neg;
+    };
+    struct Occ {
+        int k, i, j;
+    };
     for (int q = 0; q < L.n; q++) {
-        std::vector<std::array<int, kDigits>> dig(L.size[q]);
-        for (uint32_t e = 0; e < L.size[q]; e++)
+        const int n = (int)L.size[q];
+        std::vector<std::array<int, kDigits>> dig(n);
+        for (int e = 0; e < n; e++)
             if (!tap_digits(taps[q][e], true, dig[e].data())) return false;
-        group_items(reinterpret_cast<const int(*)[kDigits]>(dig.data()), (int)L.size[q],
-                    items.data() + (size_t)kDigits * L.off[q], offsets[q], nullptr);
+        std::vector<std::vector<Item>> bk(kBuckets);
+        for (int e = 0; e < n; e++)
+            for (int d = 0; d < kDigits; d++)
+                if (dig[e][d]) bk[abs(dig[e][d]) - 1].push_back({e, d, dig[e][d] < 0 ? 1 : 0});
+        // every pair of items in a bucket, keyed by (row a, row b, delta, relative sign)
+        std::map<std::array<int, 4>, std::vector<Occ>> occ;
+        for (int k = 0; k < kBuckets; k++)
+            for (int i = 0; i < (int)bk[k].size(); i++)
+                for (int j = i + 1; j < (int)bk[k].size(); j++) {
+                    int ia = i, ib = j;
+                    const Item &x = bk[k][i], &y = bk[k][j];
+                    if (std::make_pair(y.d, y.e) < std::make_pair(x.d, x.e)) std::swap(ia, ib);
+                    const Item &A = bk[k][ia], &B = bk[k][ib];
+                    int delta = B.e - A.e, sgn = A.neg ^ B.neg;
+                    if (delta < 0) {
+                        delta += n;
+                        if (L.nega[q]) sgn ^= 1; // L~[y - n] = -L~[y]
+                    }
+                    occ[{A.d, B.d, delta, sgn}].push_back({k, ia, ib});
+                }
+        std::vector<std::pair<const std::array<int, 4> *, const std::vector<Occ> *>> order;
+        for (const auto &kv : occ)
+            if (kv.second.size() >= 2) order.push_back({&kv.first, &kv.second});
+        std::stable_sort(order.begin(), order.end(),
+                         [](const auto &x, const auto &y) { return x.second->size() > y.second->size(); });
+        std::vector<std::vector<char>> used(kBuckets);
+        for (int k = 0; k < kBuckets; k++) used[k].assign(bk[k].size(), 0);
+        std::vector<std::vector<Item>> extra(kBuckets);
+        int t = 0;
+        for (const auto &ty : order) {
+            if (t >= kMaxPartTypes) break;
+            std::vector<Occ> sel;
+            for (const Occ &o : *ty.second)
+                if (!used[o.k][o.i] && !used[o.k][o.j]) {
+                    sel.push_back(o);
+                    used[o.k][o.i] = used[o.k][o.j] = 1;
+                }
+            if (sel.size() < 2) {
+                for (const Occ &o : sel) used[o.k][o.i] = used[o.k][o.j] = 0;
+                continue;
+            }
+            const std::array<int, 4> &key = *ty.first;
+            types.push_back({(uint8_t)q, (uint8_t)key[0], (uint8_t)key[1], (uint8_t)key[3], (uint32_t)key[2], 0});
+            for (const Occ &o : sel) extra[o.k].push_back({bk[o.k][o.i].e, kDigits + t, bk[o.k][o.i].neg});
+            t++;
+        }
+        uint32_t *dst = items.data() + (size_t)kDigits * L.off[q];
+        uint32_t acc = 0;
+        for (int k = 0; k < kBuckets; k++) {
+            offsets[q][k] = acc;
+            auto put = [&](const Item &it) {
+                dst[acc++] = (uint32_t)it.e | ((uint32_t)it.d << 8) | ((uint32_t)it.neg << 16);
+            };
+            for (size_t i = 0; i < bk[k].size(); i++)
+                if (!used[k][i]) put(bk[k][i]);
+            for (const Item &it : extra[k]) put(it);
+        }
+        offsets[q][kBuckets] = acc;
+        if (acc > (uint32_t)(kDigits * n)) return false;
     }
     return true;
 }
@@ -411,11 +480,33 @@ vkzg_result upload_small_tables(vkzg_prover *p, const HostTables &h) {
     {
         std::vector<uint32_t> pitems;
         uint32_t poffs[kFBMaxParts][kBuckets + 1];
-        if (!host_part_tables(h.roots_fwd, kPartLevels, pitems, poffs)) return VKZG_ERR_SETUP;
+        std::vector<DerivType> types;
+        if (!host_part_tables(h.roots_fwd, kPartLevels, pitems, poffs, types)) return VKZG_ERR_SETUP;
         if (!p->alloc(t.part_items, pitems.size()) || !p->alloc(t.part_offsets, (size_t)kFBMaxParts * (kBuckets + 1)))
             return VKZG_ERR_MALLOC;
         CK(cudaMemcpy(t.part_items, pitems.data(), 4 * pitems.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(t.part_offsets, poffs, sizeof poffs, cudaMemcpyHostToDevice));
+        // shared pair sums: part q's types follow each other, n_q points each
+        const PartLayout PL = part_layout(kPartLevels);
+        uint32_t dp = 0;
+        for (int q = 0; q < PL.n; q++) {
+            t.deriv_base[q] = dp;
+            for (auto &ty : types)
+                if (ty.part == q) {
+                    ty.base = dp;
+                    dp += PL.size[q];
+                }
+        }
+        t.deriv_points = dp;
+        t.deriv_types = (int)types.size();
+        if (dp) {
+            std::vector<uint16_t> of(dp);
+            for (size_t i = 0; i < types.size(); i++)
+                for (uint32_t x = 0; x < PL.size[types[i].part]; x++) of[types[i].base + x] = (uint16_t)i;
+            if (!p->alloc(t.deriv, types.size()) || !p->alloc(t.deriv_of, dp)) return VKZG_ERR_MALLOC;
+            CK(cudaMemcpy(t.deriv, types.data(), sizeof(DerivType) * types.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(t.deriv_of, of.data(), 2 * (size_t)dp, cudaMemcpyHostToDevice));
+        }
         std::unique_ptr<FlatBPlan> pl(new FlatBPlan);
         if (build_flatb_plan(part_layout(kPartLevels), poffs, *pl) && pl->rounds > 0) {
             if (!p->alloc(t.fb_plan, 1)) return VKZG_ERR_MALLOC;
@@ -665,6 +756,7 @@ void take_comb(ProofWork &w, const ProofWork &from) {
     w.flat_blocks = from.flat_blocks;
     w.flatb_buf[0] = from.flatb_buf[0];
     w.flatb_buf[1] = from.flatb_buf[1];
+    w.deriv_buf = from.deriv_buf;
 }
 
 // The proof pipeline of one chunk on the prover's own working set (p->pw with
@@ -730,7 +822,8 @@ bool ensure_flat_b(vkzg_prover *p) {
     if (!p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
         !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
         !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
-        !p->alloc(w.flatb_buf[1], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[1]))) {
+        !p->alloc(w.flatb_buf[1], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[1])) ||
+        !p->alloc(w.deriv_buf, (size_t)p->cap * std::max<uint32_t>(1, p->t.deriv_points))) {
         cudaGetLastError();
         w.flat_pre = nullptr;
         p->flat_failed = true;
