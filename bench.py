@@ -253,17 +253,35 @@ def plain_rates(prover, h_blobs, h_cells, h_present, sample):
             "recovery_blobs_per_s": rr, "sample": f"{sample} proof + {sample} recovery calls of 1 blob"}
 
 
-def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions, seconds, seed=99, args_warm=0.6):
+def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions, seconds, seed=99, args_warm=0.6,
+                batch=128, lanes=3):
     """Served mixed stream (continuous batching, vkzg_b200_server_*): Poisson arrivals,
     request sizes geometric with mean 6 in 1..64 blobs, 70% proof requests and 30%
     recovery requests (64..127 cells present).  One segment per offered load
-    (fraction x capacity blobs/s); latency is submit-to-completion inside the server."""
+    (fraction x capacity blobs/s); latency is submit-to-completion inside the server.
+    Outputs land in reused pinned rings, as a serving caller's would, not in fresh
+    pageable arrays (whose first-touch page faults would be charged to the lanes)."""
     import queue
+    import torch
     import vkzg_b200
     rng = np.random.default_rng(seed)
     results, checks = [], []
     warming = True
-    with vkzg_b200.Server(max_blobs_per_batch=128, lanes=3, hbm_budget_bytes=8 << 30) as srv:
+    # the rings wrap after ~0.5 s of output at the highest load, far beyond any request's latency
+    ring = {"proofs": torch.empty(64 << 20, dtype=torch.uint8).pin_memory().numpy(),
+            "recovery": torch.empty(768 << 20, dtype=torch.uint8).pin_memory().numpy()}
+    ring_off = {"proofs": 0, "recovery": 0}
+
+    def ring_take(kind, size):
+        off = ring_off[kind]
+        if off + size > len(ring[kind]):
+            off = 0
+        ring_off[kind] = off + size
+        return ring[kind][off:off + size]
+
+    t_setup = time.perf_counter()
+    with vkzg_b200.Server(max_blobs_per_batch=batch, lanes=lanes, hbm_budget_bytes=8 << 30) as srv:
+        setup_s = time.perf_counter() - t_setup
         # warm-up segment (not reported): the lanes capture the pipelines of the batch
         # sizes they meet, so the measured segments mostly replay captured graphs
         fractions = [args_warm] + list(fractions)
@@ -280,8 +298,10 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
                         return
                     statuses.append(srv.wait(item[0]))
                     # every 40th request of every segment, up to 64, checked after the sweep
+                    # (copied out of the ring now that the request is complete)
                     if len(statuses) % 40 == 1 and len(checks) < 64 and item[1] is not None:
-                        checks.append(item[1])
+                        kind, first, n, out = item[1]
+                        checks.append((kind, first, n, out.copy()))
 
             th = threading.Thread(target=waiter, daemon=True)
             th.start()
@@ -298,11 +318,11 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
                 n = int(min(64, rng.geometric(1.0 / 6.0)))
                 first = int(rng.integers(0, n_pool - n + 1))
                 if rng.random() < 0.7:
-                    out = np.empty(n * PROOFS, np.uint8)
+                    out = ring_take("proofs", n * PROOFS)
                     t = srv.submit_proofs(out, h_blobs.data_ptr() + first * BLOB, n)
                     tickets.put((t, ("proofs", first, n, out)))
                 else:
-                    out = np.empty(n * EXT, np.uint8)
+                    out = ring_take("recovery", n * EXT)
                     t = srv.submit_recovery(out, h_cells.data_ptr() + first * EXT,
                                             h_present.data_ptr() + first * 128, n)
                     tickets.put((t, ("recovery", first, n, out)))
@@ -329,7 +349,7 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
             assert prover.recover_cells_raw(ref, h_cells.data_ptr() + first * EXT,
                                             h_present.data_ptr() + first * 128, n) == 0
         assert np.array_equal(ref, out), f"served {kind} request differs from a direct call"
-    return results, len(checks)
+    return results, len(checks), setup_s
 
 
 def run_ours(args, rank, world, local_rank):
@@ -442,12 +462,13 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the plain form (one call per blob) and the served form, one replica each
     plain = plain_rates(prover, h_blobs, h_cells, h_present, args.plain_sample) if not args.no_plain else None
-    serving, checked = None, 0
+    serving, checked, serve_setup_s = None, 0, None
     if args.serve_seconds > 0:
         capacity = 1.0 / (0.7 / e2e_proof_rate + 0.3 / e2e_rec_rate)
         fractions = [float(x) for x in args.serve_loads.split(",")]
-        serving, checked = serve_sweep(prover, h_blobs, h_cells, h_present, n, capacity, fractions,
-                                       args.serve_seconds)
+        serving, checked, serve_setup_s = serve_sweep(prover, h_blobs, h_cells, h_present, n, capacity, fractions,
+                                                      args.serve_seconds, batch=args.serve_batch,
+                                                      lanes=args.serve_lanes)
     replicas.barrier(dev)
     if rank != 0:
         return
@@ -497,7 +518,9 @@ def run_ours(args, rank, world, local_rank):
                 "proof_blobs_per_s": world * e2e_proof_rate, "recovery_blobs_per_s": world * e2e_rec_rate},
         "plain_per_blob": plain,
         "batched_over_plain": (e2e_value / world) / plain["value"] if plain else None,
-        "serving": {"sweep": serving, "lanes": 3, "max_blobs_per_batch": 128, "hbm_budget_bytes": 8 << 30,
+        "serving": {"sweep": serving, "lanes": args.serve_lanes, "max_blobs_per_batch": args.serve_batch,
+                    "hbm_budget_bytes": 8 << 30, "outputs": "reused pinned rings",
+                    "setup_s": round(serve_setup_s, 2),
                     "seconds_per_load": args.serve_seconds, "bit_exact_checked_requests": checked,
                     "mix": "Poisson arrivals; 1-64 blobs per request (geometric, mean 6); 70% proofs, "
                            "30% recovery with 64-127 cells present"} if serving else None,
@@ -540,6 +563,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="per offered load; 0 skips serving")
     ap.add_argument("--serve-loads", default="0.3,0.6,0.9", help="offered loads as fractions of batched capacity")
+    ap.add_argument("--serve-batch", type=int, default=128, help="the server's max_blobs_per_batch")
+    ap.add_argument("--serve-lanes", type=int, default=3, help="the server's lanes")
     args = ap.parse_args()
 
     if args.profile_case:

@@ -189,6 +189,7 @@ cudaError_t configure_kernels();
 struct vkzg_prover;
 namespace vkzg {
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src);
+void precapture_graphs(vkzg_prover *p, uint32_t max_n);
 
 // process-wide count of kernels launched by the launchers above
 void count_launches(int k);

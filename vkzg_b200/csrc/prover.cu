@@ -765,13 +765,15 @@ void take_comb(ProofWork &w, const ProofWork &from) {
 // timing is on, for sizes beyond the cache (kMaxGraphs), or when $VKZG_GRAPHS=0.
 constexpr size_t kMaxGraphs = 160; // every chunk size of a 128-blob serving lane, and then some
 
-cudaError_t run_proofs(vkzg_prover *p, const ProofWork &w, uint32_t n) {
-    cudaStream_t s = p->stream;
+// the captured pipeline of (n, w.plan), captured now if it is not yet; *rec is
+// null when graphs are off or the cache is full
+cudaError_t proof_graph(vkzg_prover *p, const ProofWork &w, uint32_t n, const vkzg_prover::GraphRec **rec) {
+    *rec = nullptr;
     const uint64_t key = ((uint64_t)n << 8) | (uint64_t)w.plan;
     auto it = p->graphs.find(key);
-    if (p->timing || !p->use_graphs || (it == p->graphs.end() && p->graphs.size() >= kMaxGraphs))
-        return launch_proofs_timed(p->t, w, (int)n, s, p->timing ? p->ev : nullptr);
+    if (p->timing || !p->use_graphs || (it == p->graphs.end() && p->graphs.size() >= kMaxGraphs)) return cudaSuccess;
     if (it == p->graphs.end()) {
+        cudaStream_t s = p->stream;
         const uint64_t before = t_launches;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -787,8 +789,17 @@ cudaError_t run_proofs(vkzg_prover *p, const ProofWork &w, uint32_t n) {
         if (e != cudaSuccess) return e;
         it = p->graphs.emplace(key, vkzg_prover::GraphRec{ex, k}).first;
     }
-    count_launches((int)it->second.launches);
-    return cudaGraphLaunch(it->second.exec, s);
+    *rec = &it->second;
+    return cudaSuccess;
+}
+
+cudaError_t run_proofs(vkzg_prover *p, const ProofWork &w, uint32_t n) {
+    const vkzg_prover::GraphRec *rec = nullptr;
+    const cudaError_t e = proof_graph(p, w, n, &rec);
+    if (e != cudaSuccess) return e;
+    if (!rec) return launch_proofs_timed(p->t, w, (int)n, p->stream, p->timing ? p->ev : nullptr);
+    count_launches((int)rec->launches);
+    return cudaGraphLaunch(rec->exec, p->stream);
 }
 constexpr uint32_t kCombMinBlobs = 16; // smaller chunks never pay for the digit table
 
@@ -1341,6 +1352,21 @@ namespace vkzg {
 // dst takes src's tuned plans (provers of one serving loop share their
 // decisions) and allocates what those plans need now, so that no later call
 // stops for a device allocation
+// Captures the pipeline of every chunk size 1..max_n (with its tuned plan)
+// ahead of use, so that no call waits for a capture (a serving lane meets
+// every batch size up to its maximum).
+void precapture_graphs(vkzg_prover *p, uint32_t max_n) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (cudaSetDevice(p->device) != cudaSuccess) return;
+    for (uint32_t n = 1; n <= std::min(max_n, p->cap); n++) {
+        ProofWork w = p->pw;
+        w.plan = plan_for(p, n);
+        const vkzg_prover::GraphRec *rec = nullptr;
+        if (proof_graph(p, w, n, &rec) != cudaSuccess || !rec) return;
+    }
+}
+
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src) {
     if (!dst || !src) return;
     std::lock_guard<std::mutex> lock(dst->mutex);

@@ -260,6 +260,9 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
         return VKZG_ERR_GPU;
     }
     for (auto &l : s->lanes) vkzg::adopt_tuning(l->p, s->lanes[0]->p);
+    // and capture every batch size's proof pipeline on every lane: a capture on
+    // first use would hold up the request that meets it
+    for (auto &l : s->lanes) vkzg::precapture_graphs(l->p, cap);
     for (auto &l : s->lanes) {
         Lane *lp = l.get();
         l->worker = std::thread([s, lp] { s->lane_loop(lp); });
