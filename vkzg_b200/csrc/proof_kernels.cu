@@ -1726,8 +1726,24 @@ int launch_normalize_flat(const ProofWork &w, int n, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- launcher
+// Stages 1-2 (per blob) for blobs [off, off + cnt) of the working set: a host
+// upload in pieces runs them on each piece as it lands.
+cudaError_t launch_proofs_front(const DeviceTables &t, const ProofWork &w, int off, int cnt, cudaStream_t s) {
+    if (cnt <= 0) return cudaSuccess;
+    const size_t smem_ntt = (size_t)kBlobElems * sizeof(Fr);
+    k_blob_to_coeffs<<<cnt, kNttThreads, smem_ntt, s>>>(w.blobs + (size_t)off * kBlobBytes,
+                                                        w.coeffs + (size_t)off * kBlobElems, t.roots_inv,
+                                                        t.inv_blob_r2, w.err + off);
+    k_circulant<<<dim3(kCellElems / kCircCols, cnt), kCircCols * 64, 0, s>>>(
+        w.coeffs + (size_t)off * kBlobElems, w.scalars + (size_t)off * kCells * kCellElems, t.roots_fwd);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
 // ev (nullable): kProofStages + 1 events recorded around the stages.
-cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev) {
+// skip_front: stages 1-2 already ran (launch_proofs_front).
+cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s, cudaEvent_t *ev,
+                                bool skip_front) {
     if (n <= 0) return cudaSuccess;
     int k = 0;
     auto mark = [&]() {
@@ -1738,9 +1754,11 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     const int red_blocks = (n_out * kReduceLanes + kReduceThreads - 1) / kReduceThreads;
     const int n_lad = n * kCells * kLadderDigits;
     mark();
-    k_blob_to_coeffs<<<n, kNttThreads, smem_ntt, s>>>(w.blobs, w.coeffs, t.roots_inv, t.inv_blob_r2, w.err);
+    if (!skip_front)
+        k_blob_to_coeffs<<<n, kNttThreads, smem_ntt, s>>>(w.blobs, w.coeffs, t.roots_inv, t.inv_blob_r2, w.err);
     mark();
-    k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
+    if (!skip_front)
+        k_circulant<<<dim3(kCellElems / kCircCols, n), kCircCols * 64, 0, s>>>(w.coeffs, w.scalars, t.roots_fwd);
     mark();
     // plan: 0 serial Jacobian buckets + serial reduction; 1 batch-affine buckets
     // per warp + binary-split reduction; 2 as 1 with the serial reduction; 3 phase A
@@ -1750,7 +1768,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     const bool comb = w.plan == 3 && w.comb != nullptr && w.flat_dig != nullptr && w.ba_blocks > 0;
     const bool flatb = (w.plan == 3 || w.plan == 4) && w.flat_pre != nullptr && t.fb_rounds > 0 && w.ba_blocks > 0;
     const bool hier = w.plan == 1 || w.plan == 3 || w.plan == 4;
-    int launched = 10;
+    int launched = skip_front ? 8 : 10;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
     auto reduce = [&]() {
         if (flatb) launched += launch_reduce_flat(w, w.bucket_aff, w.points, n_out, s) - 1;
@@ -1804,7 +1822,7 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
 }
 
 cudaError_t launch_proofs(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
-    return launch_proofs_timed(t, w, n, s, nullptr);
+    return launch_proofs_timed(t, w, n, s, nullptr, false);
 }
 
 // Resident blocks per SM of the batch-affine kernels (sizes their persistent grid).

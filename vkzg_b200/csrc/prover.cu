@@ -35,7 +35,8 @@ cudaError_t configure_recover_kernels();
 int batch_affine_blocks_per_sm();
 size_t reduce_scratch_points(int cap_blobs);
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s,
-                                cudaEvent_t *ev);
+                                cudaEvent_t *ev, bool skip_front = false);
+cudaError_t launch_proofs_front(const DeviceTables &t, const ProofWork &w, int off, int cnt, cudaStream_t s);
 cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
                                  cudaEvent_t *ev);
 
@@ -767,9 +768,11 @@ constexpr size_t kMaxGraphs = 160; // every chunk size of a 128-blob serving lan
 
 // the captured pipeline of (n, w.plan), captured now if it is not yet; *rec is
 // null when graphs are off or the cache is full
-cudaError_t proof_graph(vkzg_prover *p, const ProofWork &w, uint32_t n, const vkzg_prover::GraphRec **rec) {
+// rest_only: the pipeline without stages 1-2 (launched per upload piece)
+cudaError_t proof_graph(vkzg_prover *p, const ProofWork &w, uint32_t n, const vkzg_prover::GraphRec **rec,
+                        bool rest_only = false) {
     *rec = nullptr;
-    const uint64_t key = ((uint64_t)n << 8) | (uint64_t)w.plan;
+    const uint64_t key = ((uint64_t)n << 8) | (uint64_t)w.plan | (rest_only ? 0x80u : 0u);
     auto it = p->graphs.find(key);
     if (p->timing || !p->use_graphs || (it == p->graphs.end() && p->graphs.size() >= kMaxGraphs)) return cudaSuccess;
     if (it == p->graphs.end()) {
@@ -778,7 +781,7 @@ cudaError_t proof_graph(vkzg_prover *p, const ProofWork &w, uint32_t n, const vk
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
-        e = launch_proofs_timed(p->t, w, (int)n, s, nullptr);
+        e = launch_proofs_timed(p->t, w, (int)n, s, nullptr, rest_only);
         const cudaError_t e2 = cudaStreamEndCapture(s, &g);
         const uint64_t k = t_launches - before;
         count_launches(-(int)k); // captured, not run
@@ -992,16 +995,48 @@ bool tuned(const vkzg_prover *p, uint32_t n) {
     return p->plan_forced >= 0 || p->plan_of.count(size_class(n)) != 0;
 }
 
+// Host blobs of a tuned chunk of >= 64 blobs go up in kSides pieces on the side
+// streams, and the per-blob front of the pipeline (stages 1-2) runs on each piece
+// as it lands, so the upload overlaps that work; the rest replays its own graph.
+static bool upload_in_pieces(vkzg_prover *p, uint32_t n) {
+    return n >= 64 && p->side[0] && p->use_graphs && !p->timing && tuned(p, n);
+}
+
 vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
-    CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
-    if (!tuned(p, n)) {
-        const vkzg_result rc = tune_chunk(p, p->pw, n);
-        if (rc != VKZG_OK) return rc;
+    if (upload_in_pieces(p, n)) {
+        p->pw.plan = plan_for(p, n);
+        const vkzg_prover::GraphRec *rec = nullptr;
+        CK(proof_graph(p, p->pw, n, &rec, true));
+        CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+        // the pieces' copies start after the stream's earlier work (which may still read the blobs)
+        CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
+        const uint32_t part = (n + vkzg_prover::kSides - 1) / vkzg_prover::kSides;
+        for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
+            const uint32_t cnt = std::min(part, n - off);
+            CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
+            CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, blobs + (size_t)off * kBlobBytes,
+                               (size_t)cnt * kBlobBytes, cudaMemcpyHostToDevice, p->side[k]));
+            CK(cudaEventRecord(p->side_ev[k], p->side[k]));
+            CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
+            CK(launch_proofs_front(p->t, p->pw, (int)off, (int)cnt, s));
+        }
+        if (rec) {
+            count_launches((int)rec->launches);
+            CK(cudaGraphLaunch(rec->exec, s));
+        } else {
+            CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr, true));
+        }
+    } else {
+        CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+        if (!tuned(p, n)) {
+            const vkzg_result rc = tune_chunk(p, p->pw, n);
+            if (rc != VKZG_OK) return rc;
+        }
+        p->pw.plan = plan_for(p, n);
+        CK(run_proofs(p, p->pw, n));
     }
-    p->pw.plan = plan_for(p, n);
-    CK(run_proofs(p, p->pw, n));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (p->timing) collect_times(p->ev, kProofStages, p->last_proof_ms);
