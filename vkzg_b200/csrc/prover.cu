@@ -300,8 +300,9 @@ bool host_tap_tables(const std::vector<Fr> &fwd, std::vector<uint32_t> items[2],
 // taps fold like the points, t+-[e] = (t[e] +- t[e + m]) / 2.  items holds
 // 32 * 128 entries, part q's from 32 * off[q].  Then, per part, pairs of items
 // that share a bucket are replaced by one item on a shared pair sum (DerivType)
-// wherever the same pair -- rows, tap distance, relative sign -- occurs in two
-// or more buckets: greedily, the most frequent pair first, each item used once.
+// wherever the same pair -- rows, tap distance, relative sign -- occurs twice or
+// more (in one bucket or several): greedily, the most frequent pair first, each
+// item used once.
 // A shared pair sum costs n additions per blob and saves n per extra use.
 bool host_part_tables(const std::vector<Fr> &fwd, int levels, std::vector<uint32_t> &items,
                       uint32_t offsets[kFBMaxParts][kBuckets + 1], std::vector<DerivType> &types) {
