@@ -61,8 +61,8 @@ vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out,
  * fail), latency-critical loops that cannot absorb the device-wide
  * synchronisation a cudaMalloc/cudaFree can imply, and code that enqueues work
  * on a stream it does not own.  This call allocates nothing and frees nothing:
- * its scratch is a fixed array compiled into the library's device code (4.125
- * MiB, resident on every GPU that loads the library until the process exits).
+ * its scratch is a fixed array compiled into the library's device code (128
+ * KiB, resident on every GPU that loads the library until the process exits).
  * Inputs and outputs are the caller's device buffers, laid out as for
  * vkzg_b200_recover_cells_device; the work is enqueued on `stream` (a
  * cudaStream_t, NULL = legacy default stream) and the call returns after

@@ -1065,7 +1065,13 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
     }
     cudaStream_t s = p->stream;
     const size_t ext = (size_t)kExtElems * 32;
-    const uint32_t parts = std::min<uint32_t>(vkzg_prover::kSides, n / 16);
+#ifndef VKZG_REC_PART_BLOBS
+#define VKZG_REC_PART_BLOBS 16
+#endif
+#ifndef VKZG_REC_MAX_PARTS
+#define VKZG_REC_MAX_PARTS 16
+#endif
+    const uint32_t parts = std::min<uint32_t>(VKZG_REC_MAX_PARTS, n / VKZG_REC_PART_BLOBS);
     const uint32_t part = n >= 64 && p->side[0] ? (n + parts - 1) / parts : n;
     if (p->timing || part == n) {
         CK(cudaMemcpyAsync(p->rw.cells, cells, n * ext, cudaMemcpyHostToDevice, s));

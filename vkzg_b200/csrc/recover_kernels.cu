@@ -11,22 +11,19 @@
 // coset ones), which replaces two of the reference's six 8192-point NTTs and
 // its per-element Fermat division with exactly the same field values.
 //
-// k_recover_main then runs the remaining four transforms for one blob per
-// block.  The wire order of cells is the bit-reversed order of the evaluation
-// domain, so a DIT inverse (bit-reversed in, natural out) and a DIF forward
-// (natural in, bit-reversed out) chain with no permutation pass.  An 8192-point
-// transform is split at its outermost radix-2 stage: the inner 12 stages run on
-// one 4096-element half at a time in shared memory (128 KB), and the stage
-// that pairs k with k+4096 runs as a streaming pass over global scratch,
-// fused with the pointwise coset shift and the next transform's first stage.
+// k_recover_cluster then runs the remaining four transforms for one blob per
+// cluster of four blocks.  The wire order of cells is the bit-reversed order of
+// the evaluation domain, so a DIT inverse (bit-reversed in, natural out) and a
+// DIF forward (natural in, bit-reversed out) chain with no permutation pass.
 #include "device_util.cuh"
 #include "kernels.h"
 
+#include <cooperative_groups.h>
 #include <mutex>
 
 namespace vkzg {
 
-constexpr int kRecThreads = 512;
+namespace cg = cooperative_groups;
 
 // zv[c] = Zs(w_128^brev7(c)) * R   (R folded in so raw cell words need no
 //                                    separate Montgomery conversion)
@@ -59,86 +56,129 @@ __global__ void __launch_bounds__(kCells) k_recover_prep(const uint8_t *__restri
     st_vec(&inv_zc[(size_t)b * kCells + c], inv);
 }
 
-// Outermost DIT stage of an inverse 8192 transform, pointwise scale by
-// shift[k], then outermost DIF stage of a forward transform, in place on g.
-__device__ void stream_dit_scale_dif(Fr *g, const Fr *__restrict__ roots_fwd, const Fr *__restrict__ roots_inv,
-                                     const Fr *__restrict__ shift) {
-    for (int j = threadIdx.x; j < kBlobElems; j += kRecThreads) {
-        const Fr u = ld_vec(&g[j]);
-        const Fr v = fr_mul(ld_vec(&g[j + kBlobElems]), ldg_vec(&roots_inv[j]));
-        const Fr c0 = fr_mul(fr_add(u, v), ldg_vec(&shift[j]));
-        const Fr c1 = fr_mul(fr_sub(u, v), ldg_vec(&shift[j + kBlobElems]));
-        st_vec(&g[j], fr_add(c0, c1));
-        st_vec(&g[j + kBlobElems], fr_mul(fr_sub(c0, c1), ldg_vec(&roots_fwd[j])));
+// ------------------------------------------------ transforms
+// One blob is spread over a cluster of four blocks, each holding a quarter
+// (2048 elements, 64 KB) of the blob in its own shared memory.  The inner 11
+// stages of every transform run per quarter; the two outermost stages (the
+// pairs k, k+2048 and k, k+4096), fused with the pointwise coset shift and the
+// first two stages of the next transform, run as a radix-4 step on the groups
+// {k, k+2048, k+4096, k+6144}, one element from each block's shared memory over
+// the cluster's distributed shared memory.  No global scratch is used, and a
+// block is a quarter of the per-blob work (three fit on an SM), so a batch's
+// last blobs finish sooner than with one 128 KB block per blob, which ran two
+// 4096-point halves in turn with the outer stage streamed through global
+// memory (130 k against 143 k blobs/s at 256 blobs).
+constexpr int kRecQuarter = kExtElems / 4;
+constexpr int kRecQThreads = 256;
+
+__device__ void cluster_dit_scale_dif(cg::cluster_group &cl, Fr *s, const Fr *__restrict__ roots_fwd,
+                                      const Fr *__restrict__ roots_inv, const Fr *__restrict__ shift) {
+    Fr *q0 = cl.map_shared_rank(s, 0), *q1 = cl.map_shared_rank(s, 1);
+    Fr *q2 = cl.map_shared_rank(s, 2), *q3 = cl.map_shared_rank(s, 3);
+    const int first = (int)cl.block_rank() * (kRecQuarter / 4);
+    for (int i = threadIdx.x; i < kRecQuarter / 4; i += kRecQThreads) {
+        const int k = first + i;
+        Fr a0 = ld_vec(&q0[k]), a1 = ld_vec(&q1[k]), a2 = ld_vec(&q2[k]), a3 = ld_vec(&q3[k]);
+        // inverse DIT, length 4096: (k, k+2048) and (k+4096, k+6144), twiddle w^(2k)
+        const Fr w4 = ldg_vec(&roots_inv[2 * k]);
+        Fr t = fr_mul(a1, w4);
+        a1 = fr_sub(a0, t);
+        a0 = fr_add(a0, t);
+        t = fr_mul(a3, w4);
+        a3 = fr_sub(a2, t);
+        a2 = fr_add(a2, t);
+        // inverse DIT, length 8192: (k, k+4096) twiddle w^k, (k+2048, k+6144) twiddle w^(k+2048)
+        t = fr_mul(a2, ldg_vec(&roots_inv[k]));
+        a2 = fr_sub(a0, t);
+        a0 = fr_add(a0, t);
+        t = fr_mul(a3, ldg_vec(&roots_inv[k + kRecQuarter]));
+        a3 = fr_sub(a1, t);
+        a1 = fr_add(a1, t);
+        // pointwise shift
+        a0 = fr_mul(a0, ldg_vec(&shift[k]));
+        a1 = fr_mul(a1, ldg_vec(&shift[k + kRecQuarter]));
+        a2 = fr_mul(a2, ldg_vec(&shift[k + 2 * kRecQuarter]));
+        a3 = fr_mul(a3, ldg_vec(&shift[k + 3 * kRecQuarter]));
+        // forward DIF, length 8192: (k, k+4096) twiddle w^k, (k+2048, k+6144) twiddle w^(k+2048)
+        t = fr_sub(a0, a2);
+        a0 = fr_add(a0, a2);
+        a2 = fr_mul(t, ldg_vec(&roots_fwd[k]));
+        t = fr_sub(a1, a3);
+        a1 = fr_add(a1, a3);
+        a3 = fr_mul(t, ldg_vec(&roots_fwd[k + kRecQuarter]));
+        // forward DIF, length 4096: (k, k+2048) and (k+4096, k+6144), twiddle w^(2k)
+        const Fr v4 = ldg_vec(&roots_fwd[2 * k]);
+        t = fr_sub(a0, a1);
+        a0 = fr_add(a0, a1);
+        a1 = fr_mul(t, v4);
+        t = fr_sub(a2, a3);
+        a2 = fr_add(a2, a3);
+        a3 = fr_mul(t, v4);
+        st_vec(&q0[k], a0);
+        st_vec(&q1[k], a1);
+        st_vec(&q2[k], a2);
+        st_vec(&q3[k], a3);
     }
 }
 
-__global__ void __launch_bounds__(kRecThreads, 1) k_recover_main(const uint8_t *__restrict__ cells, uint8_t *out,
-                                                                 Fr *scratch, const Fr *__restrict__ zv,
-                                                                 const Fr *__restrict__ inv_zc,
-                                                                 const Fr *__restrict__ roots_fwd,
-                                                                 const Fr *__restrict__ roots_inv,
-                                                                 const Fr *__restrict__ shift_fwd,
-                                                                 const Fr *__restrict__ shift_inv) {
+#ifndef VKZG_REC_BLOCKS_PER_SM
+#define VKZG_REC_BLOCKS_PER_SM 3
+#endif
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_REC_BLOCKS_PER_SM)
+    k_recover_cluster(const uint8_t *__restrict__ cells, uint8_t *out, const Fr *__restrict__ zv,
+                      const Fr *__restrict__ inv_zc, const Fr *__restrict__ roots_fwd,
+                      const Fr *__restrict__ roots_inv, const Fr *__restrict__ shift_fwd,
+                      const Fr *__restrict__ shift_inv) {
     extern __shared__ uint4 smem_raw[];
     Fr *s = reinterpret_cast<Fr *>(smem_raw);
-    const int b = blockIdx.x;
-    Fr *g = scratch + (size_t)b * kExtElems;
-    const uint8_t *src = cells + (size_t)b * kExtElems * 32;
+    cg::cluster_group cl = cg::this_cluster();
+    const int b = blockIdx.x >> 2;
+    const int first = (int)cl.block_rank() * kRecQuarter; // this block's positions
+    const uint8_t *src = cells + ((size_t)b * kExtElems + first) * 32;
     const Fr *zvb = zv + (size_t)b * kCells;
     const Fr *izb = inv_zc + (size_t)b * kCells;
 
     // A: X = E . Z on the domain (bit-reversed), inverse DIT inner stages
-    for (int h = 0; h < 2; h++) {
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) {
-            const int p = h * kBlobElems + q;
-            const uint4 *w = reinterpret_cast<const uint4 *>(src + 32 * (size_t)p);
-            const uint4 lo = w[0], hi = w[1];
-            Fr v;
-            v.v[7] = bswap32(lo.x); v.v[6] = bswap32(lo.y); v.v[5] = bswap32(lo.z); v.v[4] = bswap32(lo.w);
-            v.v[3] = bswap32(hi.x); v.v[2] = bswap32(hi.y); v.v[1] = bswap32(hi.z); v.v[0] = bswap32(hi.w);
-            st_vec(&s[q], fr_mul(ld_vec(&zvb[p >> 6]), v)); // raw word second
-        }
-        __syncthreads();
-        smem_dit<kRecThreads>(s, 12, 1, 2, 4096, roots_inv);
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) st_vec(&g[h * kBlobElems + q], ld_vec(&s[q]));
-        __syncthreads();
+    for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads) {
+        const uint4 *w = reinterpret_cast<const uint4 *>(src + 32 * (size_t)q);
+        const uint4 lo = w[0], hi = w[1];
+        Fr v;
+        v.v[7] = bswap32(lo.x); v.v[6] = bswap32(lo.y); v.v[5] = bswap32(lo.z); v.v[4] = bswap32(lo.w);
+        v.v[3] = bswap32(hi.x); v.v[2] = bswap32(hi.y); v.v[1] = bswap32(hi.z); v.v[0] = bswap32(hi.w);
+        st_vec(&s[q], fr_mul(ld_vec(&zvb[(first + q) >> 6]), v)); // raw word second
     }
-    // B: finish IFFT, x 7^k / N, first stage of the coset FFT
-    stream_dit_scale_dif(g, roots_fwd, roots_inv, shift_fwd);
     __syncthreads();
+    smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
+    cl.sync();
+    // B: finish the IFFT, x 7^k / N, first two stages of the coset FFT
+    cluster_dit_scale_dif(cl, s, roots_fwd, roots_inv, shift_fwd);
+    cl.sync();
     // C: coset FFT inner stages, divide by Z on the coset, inverse DIT inner stages
-    for (int h = 0; h < 2; h++) {
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) st_vec(&s[q], ld_vec(&g[h * kBlobElems + q]));
-        __syncthreads();
-        smem_dif<kRecThreads>(s, 12, 1, 4096, 2, roots_fwd);
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) {
-            const int p = h * kBlobElems + q;
-            st_vec(&s[q], fr_mul(ld_vec(&s[q]), ld_vec(&izb[p >> 6])));
-        }
-        __syncthreads();
-        smem_dit<kRecThreads>(s, 12, 1, 2, 4096, roots_inv);
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) st_vec(&g[h * kBlobElems + q], ld_vec(&s[q]));
-        __syncthreads();
-    }
-    // D: finish the coset IFFT, x 7^-k / N / R, first stage of the final FFT
-    stream_dit_scale_dif(g, roots_fwd, roots_inv, shift_inv);
+    smem_dif<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
+    for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads)
+        st_vec(&s[q], fr_mul(ld_vec(&s[q]), ld_vec(&izb[(first + q) >> 6])));
     __syncthreads();
-    // E: final FFT inner stages; bit-reversed output = wire order.  The 1/R in
-    // shift_inv leaves each value's canonical form in its limbs.
-    uint8_t *dst = out + (size_t)b * kExtElems * 32;
-    for (int h = 0; h < 2; h++) {
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) st_vec(&s[q], ld_vec(&g[h * kBlobElems + q]));
-        __syncthreads();
-        smem_dif<kRecThreads>(s, 12, 1, 4096, 2, roots_fwd);
-        for (int q = threadIdx.x; q < kBlobElems; q += kRecThreads) {
-            const Fr v = ld_vec(&s[q]);
-            uint4 *w = reinterpret_cast<uint4 *>(dst + 32 * (size_t)(h * kBlobElems + q));
-            w[0] = make_uint4(bswap32(v.v[7]), bswap32(v.v[6]), bswap32(v.v[5]), bswap32(v.v[4]));
-            w[1] = make_uint4(bswap32(v.v[3]), bswap32(v.v[2]), bswap32(v.v[1]), bswap32(v.v[0]));
-        }
-        __syncthreads();
+    smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
+    cl.sync();
+    // D: finish the coset IFFT, x 7^-k / N / R, first two stages of the final FFT
+    cluster_dit_scale_dif(cl, s, roots_fwd, roots_inv, shift_inv);
+    cl.sync();
+    // E: final FFT inner stages; bit-reversed output = wire order (no shared
+    // memory of another block is touched after the last cluster barrier)
+    smem_dif<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
+    uint8_t *dst = out + ((size_t)b * kExtElems + first) * 32;
+    for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads) {
+        const Fr v = ld_vec(&s[q]);
+        uint4 *w = reinterpret_cast<uint4 *>(dst + 32 * (size_t)q);
+        w[0] = make_uint4(bswap32(v.v[7]), bswap32(v.v[6]), bswap32(v.v[5]), bswap32(v.v[4]));
+        w[1] = make_uint4(bswap32(v.v[3]), bswap32(v.v[2]), bswap32(v.v[1]), bswap32(v.v[0]));
     }
+}
+
+static void launch_recover_transforms(const DeviceTables &t, const uint8_t *cells, uint8_t *out, const Fr *zv,
+                                      const Fr *inv_zc, int n, cudaStream_t s) {
+    k_recover_cluster<<<4 * n, kRecQThreads, kRecQuarter * sizeof(Fr), s>>>(cells, out, zv, inv_zc, t.roots_fwd,
+                                                                            t.roots_inv, t.shift_fwd, t.shift_inv);
 }
 
 static Fr host_seven64() {
@@ -154,9 +194,7 @@ cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, in
     if (ev) cudaEventRecord(ev[0], s);
     k_recover_prep<<<n, kCells, 0, s>>>(w.present, t.roots_fwd, seven64, w.zv, w.inv_zc, w.err);
     if (ev) cudaEventRecord(ev[1], s);
-    k_recover_main<<<n, kRecThreads, kBlobElems * sizeof(Fr), s>>>(w.cells, w.out, w.scratch, w.zv, w.inv_zc,
-                                                                   t.roots_fwd, t.roots_inv, t.shift_fwd,
-                                                                   t.shift_inv);
+    launch_recover_transforms(t, w.cells, w.out, w.zv, w.inv_zc, n, s);
     if (ev) cudaEventRecord(ev[2], s);
     count_launches(2);
     return cudaGetLastError();
@@ -167,18 +205,18 @@ cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, c
 }
 
 cudaError_t configure_recover_kernels() {
-    return cudaFuncSetAttribute(k_recover_main, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kBlobElems * sizeof(Fr)));
+    return cudaFuncSetAttribute(k_recover_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kRecQuarter * sizeof(Fr)));
 }
 
 // ------------------------------------------ allocation-free recovery variant
 // Scratch for vkzg_b200_recover_cells_device_noalloc: a fixed array in the
 // module's device memory instead of the prover's cudaMalloc'd working set.
-// Per blob: the 8192-element transform buffer, then Z on the domain and
-// 1/Z on the coset (128 elements each).  Every GPU that loads this library
-// holds it (4.125 MiB) until the process exits; all calls share it.
+// Per blob: Z on the domain and 1/Z on the coset (128 elements each; the
+// transforms work in shared memory).  Every GPU that loads this library holds
+// it (128 KiB) until the process exits; all calls share it.
 constexpr int kNoAllocMaxBlobs = 16;
-constexpr size_t kNoAllocPerBlob = kExtElems + 2 * kCells;
+constexpr size_t kNoAllocPerBlob = 2 * kCells;
 static __device__ __align__(256) Fr g_noalloc_scratch[kNoAllocMaxBlobs * kNoAllocPerBlob];
 
 namespace {
@@ -206,10 +244,9 @@ static cudaError_t noalloc_scratch_address(Fr **out) {
 
 int noalloc_max_blobs() { return kNoAllocMaxBlobs; }
 
-// Same two kernels as launch_recover, with the per-blob scratch carved out of
+// Same two kernels as launch_recover, with the Z tables carved out of
 // g_noalloc_scratch.  Nothing in the scratch needs to start at zero: the prep
-// kernel writes zv / inv_zc and the main kernel writes each transform buffer
-// before reading it.
+// kernel writes zv / inv_zc before the transforms read them.
 cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, const uint8_t *present, uint8_t *out,
                                    uint32_t *err, int n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
@@ -217,13 +254,11 @@ cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, 
     Fr *base = nullptr;
     cudaError_t e = noalloc_scratch_address(&base);
     if (e != cudaSuccess) return e;
-    Fr *work = base;
-    Fr *zv = base + (size_t)kNoAllocMaxBlobs * kExtElems;
+    Fr *zv = base;
     Fr *inv_zc = zv + (size_t)kNoAllocMaxBlobs * kCells;
     static const Fr seven64 = host_seven64();
     k_recover_prep<<<n, kCells, 0, s>>>(present, t.roots_fwd, seven64, zv, inv_zc, err);
-    k_recover_main<<<n, kRecThreads, kBlobElems * sizeof(Fr), s>>>(cells, out, work, zv, inv_zc, t.roots_fwd,
-                                                                   t.roots_inv, t.shift_fwd, t.shift_inv);
+    launch_recover_transforms(t, cells, out, zv, inv_zc, n, s);
     count_launches(2);
     return cudaGetLastError();
 }

@@ -86,6 +86,9 @@ struct vkzg_server {
     std::map<uint64_t, std::shared_ptr<Request>> requests;
     uint64_t next_id = 1;
     uint64_t bytes_in_flight = 0;
+    // the head request does not fit the HBM budget beside the batches in
+    // flight: the dispatcher sleeps until one of them completes
+    bool over_budget = false;
     bool stopping = false;
     std::thread dispatcher;
     // completed-request statistics since the last reset
@@ -103,7 +106,7 @@ void vkzg_server::dispatch_loop() {
     for (;;) {
         cv_dispatch.wait(lk, [&] {
             if (stopping) return true;
-            if (pending.empty()) return false;
+            if (pending.empty() || over_budget) return false;
             for (auto &l : lanes)
                 if (!l->busy) return true;
             return false;
@@ -128,7 +131,10 @@ void vkzg_server::dispatch_loop() {
                 b.parts.push_back(*it);
                 it = pending.erase(it);
             }
-            if (b.parts.empty()) break; // budget exhausted until something completes
+            if (b.parts.empty()) { // budget exhausted until something completes
+                over_budget = true;
+                break;
+            }
             bytes_in_flight += b.bytes;
             l->batch = std::move(b);
             l->busy = true;
@@ -194,6 +200,7 @@ void vkzg_server::run_batch(Lane *lane) {
         }
     }
     bytes_in_flight -= b.bytes;
+    over_budget = false;
     lane->busy = false;
     b.parts.clear();
     cv_done.notify_all();
