@@ -60,21 +60,17 @@ vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out,
  * where a framework's pool owns nearly all of HBM (an extra cudaMalloc would
  * fail), latency-critical loops that cannot absorb the device-wide
  * synchronisation a cudaMalloc/cudaFree can imply, and code that enqueues work
- * on a stream it does not own.  This call allocates nothing and frees nothing:
- * its scratch is a fixed array compiled into the library's device code (128
- * KiB, resident on every GPU that loads the library until the process exits).
- * Inputs and outputs are the caller's device buffers, laid out as for
- * vkzg_b200_recover_cells_device; the work is enqueued on `stream` (a
- * cudaStream_t, NULL = legacy default stream) and the call returns after
- * enqueueing.  The prover's device must be current.
+ * on a stream it does not own.  This call allocates nothing and frees nothing,
+ * and uses no scratch: one cluster of four blocks per blob keeps its working
+ * state in shared memory.  Inputs and outputs are the caller's device buffers,
+ * laid out as for vkzg_b200_recover_cells_device; the work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call returns
+ * after enqueueing.  The prover's device must be current.  Calls on different
+ * streams or threads may overlap on the GPU: they share nothing but the
+ * prover's read-only tables.
  *
  * Limits: at most VKZG_B200_NOALLOC_MAX_BLOBS blobs per call; more returns
- * VKZG_ERR_BADARGS without enqueueing anything.  The first call on a device
- * looks up the scratch array's device address (cudaGetSymbolAddress) and caches
- * it; make that first call before any stream capture.  Every call uses the same
- * scratch, so calls whose work overlaps on the GPU (different streams with no
- * ordering between them, or several threads) race and corrupt each other's
- * results; order them on one stream.
+ * VKZG_ERR_BADARGS without enqueueing anything.
  */
 #define VKZG_B200_NOALLOC_MAX_BLOBS 16
 vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,

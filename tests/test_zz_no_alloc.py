@@ -4,7 +4,8 @@ Some callers cannot allocate device memory when they call in: a framework's
 memory pool may already own nearly all of HBM, a latency-critical loop cannot
 absorb the synchronisation a cudaMalloc/cudaFree implies, and code enqueueing on
 a stream it does not own must not add allocations to it.  This entry point runs
-recovery with its scratch in a fixed array in the library's device memory.
+recovery with no scratch: each blob's cluster of four blocks keeps its working
+state in shared memory.
 
 The test calls it through the C ABI twice in a row, on different inputs, and
 checks each output byte for byte against the existing device entry point

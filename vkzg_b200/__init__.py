@@ -262,7 +262,7 @@ class Prover:
 
     def recover_cells_device_noalloc(self, d_out, d_cells, d_present, d_err, n, stream=None):
         """Allocation-free recovery on caller-owned device buffers (at most NOALLOC_MAX_BLOBS blobs);
-        scratch is a fixed array in the library's device memory shared by every call."""
+        the kernel keeps its working state in shared memory and uses no scratch."""
         return self._lib.vkzg_b200_recover_cells_device_noalloc(self._h, d_out, d_cells, d_present, d_err, n,
                                                                 stream)
 

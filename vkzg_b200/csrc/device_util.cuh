@@ -87,8 +87,10 @@ __device__ Fp block_batch_inverse_fp(const Fp &z, Fp *tree) {
 
 template <int NT>
 __device__ Fr block_batch_inverse_fr(const Fr &z, Fr *tree) {
+    // the first NT threads of the block hold the values; every thread of the
+    // block must call (the barriers), and threads from NT on get their z back
     const int t = threadIdx.x;
-    st_vec(&tree[NT + t], z);
+    if (t < NT) st_vec(&tree[NT + t], z);
     __syncthreads();
     for (int width = NT / 2; width >= 1; width >>= 1) {
         if (t < width) {
@@ -109,7 +111,7 @@ __device__ Fr block_batch_inverse_fr(const Fr &z, Fr *tree) {
         }
         __syncthreads();
     }
-    const Fr res = ld_vec(&tree[NT + t]);
+    const Fr res = t < NT ? ld_vec(&tree[NT + t]) : z;
     __syncthreads();
     return res;
 }

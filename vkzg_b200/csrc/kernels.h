@@ -161,8 +161,6 @@ struct RecoverWork {
     uint8_t *present = nullptr;   // [cap][128]
     uint8_t *out = nullptr;       // [cap][8192*32]
     Fr *scratch = nullptr;        // [cap][8192]
-    Fr *zv = nullptr;             // [cap][128]  Z on the domain (x R)
-    Fr *inv_zc = nullptr;         // [cap][128]  1 / Z on the coset
     uint32_t *err = nullptr;      // [cap] more than 64 cells missing
 };
 

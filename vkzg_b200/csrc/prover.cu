@@ -50,11 +50,11 @@ uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 } // namespace vkzg
 
 static constexpr int kProofStages = 10;
-static constexpr int kRecoverStages = 2;
+static constexpr int kRecoverStages = 1;
 static const char *kProofStageNames[kProofStages] = {"blob_to_coeffs", "circulant", "phase_a",  "reduce_a",
                                                      "fold",           "ladder",    "normalize", "phase_b",
                                                      "reduce_b",       "finish"};
-static const char *kRecoverStageNames[kRecoverStages] = {"recover_prep", "recover_main"};
+static const char *kRecoverStageNames[kRecoverStages] = {"recover"};
 
 // Plan 3's digit table (proof_kernels.cu, k_phase_a_comb): tens of GB, built
 // on first use and shared by every prover of the process on the same device
@@ -111,15 +111,15 @@ struct vkzg_prover {
     };
     std::map<uint64_t, GraphRec> graphs;
     bool use_graphs = true;
-    // recovery from host buffers runs in parts on these streams so that copies
-    // in, transforms and copies out of different parts overlap
-    // side streams for host-buffer chunks: a recovery chunk runs as parts of at
-    // least 16 blobs (16 parts at 256 blobs: 91 k blobs/s through the C ABI
-    // against 88 k with 4 and 81 k with 2), each copying in, computing and copying
-    // out on its own stream; a proof chunk uploads in kUploadPieces pieces (2 beat
-    // 4, 8 and 16: each piece adds a launch of the per-blob front that fills only
-    // part of the GPU)
+    // side streams for host-buffer chunks, so that copies in, kernels and copies
+    // out overlap: a recovery chunk of 64 blobs or more runs as parts of at least
+    // kRecPartBlobs blobs (32 parts at 256 blobs: 116 k blobs/s through the C ABI;
+    // 8-blob parts beat 16- and 32-blob parts by 4-6 %), each copying in,
+    // computing and copying out on side stream (part mod kSides); a proof chunk
+    // uploads in kUploadPieces pieces (2 beat 4, 8 and 16: each piece adds a
+    // launch of the per-blob front that fills only part of the GPU)
     static constexpr int kSides = 16;
+    static constexpr uint32_t kRecPartBlobs = 8, kRecMaxParts = 32;
     static constexpr int kUploadPieces = 2;
     cudaStream_t side[kSides] = {};
     cudaEvent_t side_ev[kSides + 1] = {};
@@ -589,7 +589,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
               p->alloc(w.proofs, B * kCells * kProofBytes) && p->alloc(w.err, B) &&
               p->alloc(r.cells, B * kExtElems * 32) && p->alloc(r.present, B * kCells) &&
               p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.scratch, B * kExtElems) &&
-              p->alloc(r.zv, B * kCells) && p->alloc(r.inv_zc, B * kCells) && p->alloc(r.err, B);
+              p->alloc(r.err, B);
     if (!ok) return VKZG_ERR_MALLOC;
     if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
     // batch-affine bucket accumulation: one scratch slot per resident block
@@ -1065,13 +1065,7 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
     }
     cudaStream_t s = p->stream;
     const size_t ext = (size_t)kExtElems * 32;
-#ifndef VKZG_REC_PART_BLOBS
-#define VKZG_REC_PART_BLOBS 16
-#endif
-#ifndef VKZG_REC_MAX_PARTS
-#define VKZG_REC_MAX_PARTS 16
-#endif
-    const uint32_t parts = std::min<uint32_t>(VKZG_REC_MAX_PARTS, n / VKZG_REC_PART_BLOBS);
+    const uint32_t parts = std::min<uint32_t>(vkzg_prover::kRecMaxParts, n / vkzg_prover::kRecPartBlobs);
     const uint32_t part = n >= 64 && p->side[0] ? (n + parts - 1) / parts : n;
     if (p->timing || part == n) {
         CK(cudaMemcpyAsync(p->rw.cells, cells, n * ext, cudaMemcpyHostToDevice, s));
@@ -1093,8 +1087,6 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         w.present += (size_t)off * kCells;
         w.out += off * ext;
         w.scratch += (size_t)off * kExtElems;
-        w.zv += (size_t)off * kCells;
-        w.inv_zc += (size_t)off * kCells;
         w.err += off;
         CK(cudaMemcpyAsync(w.cells, cells + off * ext, cnt * ext, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(w.present, present + (size_t)off * kCells, (size_t)cnt * kCells, cudaMemcpyHostToDevice, st));

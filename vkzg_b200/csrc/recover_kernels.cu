@@ -7,54 +7,22 @@
 // Because Z(x) = Zs(x^64), its values on the 8192-point domain and on the
 // coset 7.domain take only 128 distinct values each:
 //   Z(w^k)   = Zs(w_128^(k mod 128)),   Z(7 w^k) = Zs(7^64 w_128^(k mod 128)).
-// k_recover_prep evaluates those 2 x 128 values directly (and batch-inverts the
-// coset ones), which replaces two of the reference's six 8192-point NTTs and
-// its per-element Fermat division with exactly the same field values.
-//
-// k_recover_cluster then runs the remaining four transforms for one blob per
-// cluster of four blocks.  The wire order of cells is the bit-reversed order of
-// the evaluation domain, so a DIT inverse (bit-reversed in, natural out) and a
-// DIF forward (natural in, bit-reversed out) chain with no permutation pass.
+// Each cluster evaluates those values directly (the coset inverses as products
+// over the present cells' roots), which replaces two of the reference's six
+// 8192-point NTTs and its per-element Fermat division with exactly the same
+// field values, and then
+// runs the remaining four transforms.  The wire order of cells is the
+// bit-reversed order of the evaluation domain, so a DIT inverse (bit-reversed
+// in, natural out) and a DIF forward (natural in, bit-reversed out) chain with
+// no permutation pass.
 #include "device_util.cuh"
 #include "kernels.h"
 
 #include <cooperative_groups.h>
-#include <mutex>
 
 namespace vkzg {
 
 namespace cg = cooperative_groups;
-
-// zv[c] = Zs(w_128^brev7(c)) * R   (R folded in so raw cell words need no
-//                                    separate Montgomery conversion)
-// inv_zc[c] = 1 / Zs(7^64 w_128^brev7(c))
-__global__ void __launch_bounds__(kCells) k_recover_prep(const uint8_t *__restrict__ present,
-                                                        const Fr *__restrict__ roots_fwd, Fr seven64, Fr *zv,
-                                                        Fr *inv_zc, uint32_t *err) {
-    __shared__ uint8_t miss_root[kCells];
-    __shared__ int n_miss;
-    __shared__ Fr tree[2 * kCells];
-    const int b = blockIdx.x, c = threadIdx.x;
-    if (c == 0) {
-        int n = 0;
-        for (int i = 0; i < kCells; i++)
-            if (!present[(size_t)b * kCells + i]) miss_root[n++] = (uint8_t)brev_bits((uint32_t)i, 7);
-        n_miss = n;
-        if (err) err[b] = n > kCellElems ? 1u : 0u;
-    }
-    __syncthreads();
-    const Fr x = ldg_vec(&roots_fwd[brev_bits((uint32_t)c, 7) * 64]);
-    const Fr xc = fr_mul(x, seven64);
-    Fr pv = fr_one(), pc = fr_one();
-    for (int m = 0; m < n_miss; m++) {
-        const Fr r = ldg_vec(&roots_fwd[(int)miss_root[m] * 64]);
-        pv = fr_mul(pv, fr_sub(x, r));
-        pc = fr_mul(pc, fr_sub(xc, r));
-    }
-    st_vec(&zv[(size_t)b * kCells + c], fr_mul(pv, Fr{VK_FR_R2}));
-    const Fr inv = block_batch_inverse_fr<kCells>(pc, tree);
-    st_vec(&inv_zc[(size_t)b * kCells + c], inv);
-}
 
 // ------------------------------------------------ transforms
 // One blob is spread over a cluster of four blocks, each holding a quarter
@@ -67,9 +35,12 @@ __global__ void __launch_bounds__(kCells) k_recover_prep(const uint8_t *__restri
 // block is a quarter of the per-blob work (three fit on an SM), so a batch's
 // last blobs finish sooner than with one 128 KB block per blob, which ran two
 // 4096-point halves in turn with the outer stage streamed through global
-// memory (130 k against 143 k blobs/s at 256 blobs).
+// memory (130 k blobs/s at 256 blobs, against 143 k for this form).
 constexpr int kRecQuarter = kExtElems / 4;
+constexpr int kQCells = kCells / 4; // cells per quarter
 constexpr int kRecQThreads = 256;
+constexpr int kZSlice = kCells / (kRecQThreads / kQCells); // list entries per thread
+static_assert(kZSlice * kRecQThreads == kCells * kQCells, "Z partial products: whole slices");
 
 __device__ void cluster_dit_scale_dif(cg::cluster_group &cl, Fr *s, const Fr *__restrict__ roots_fwd,
                                       const Fr *__restrict__ roots_inv, const Fr *__restrict__ shift) {
@@ -121,22 +92,78 @@ __device__ void cluster_dit_scale_dif(cg::cluster_group &cl, Fr *s, const Fr *__
     }
 }
 
-#ifndef VKZG_REC_BLOCKS_PER_SM
-#define VKZG_REC_BLOCKS_PER_SM 3
-#endif
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_REC_BLOCKS_PER_SM)
-    k_recover_cluster(const uint8_t *__restrict__ cells, uint8_t *out, const Fr *__restrict__ zv,
-                      const Fr *__restrict__ inv_zc, const Fr *__restrict__ roots_fwd,
-                      const Fr *__restrict__ roots_inv, const Fr *__restrict__ shift_fwd,
-                      const Fr *__restrict__ shift_inv) {
+// three blocks per SM (80 registers; 64 KB of shared memory each) measured
+// faster than two with more registers: 143 k against 138 k blobs/s
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, 3)
+    k_recover_cluster(const uint8_t *__restrict__ cells, const uint8_t *__restrict__ present, uint8_t *out,
+                      const Fr *__restrict__ roots_fwd, const Fr *__restrict__ roots_inv,
+                      const Fr *__restrict__ shift_fwd, const Fr *__restrict__ shift_inv, Fr seven64,
+                      Fr coset_scale, uint32_t *err) {
     extern __shared__ uint4 smem_raw[];
     Fr *s = reinterpret_cast<Fr *>(smem_raw);
+    __shared__ uint8_t root_of[kCells];
+    __shared__ int warp_miss[kCells / 32];
+    __shared__ Fr zq[kQCells], izq[kQCells];
     cg::cluster_group cl = cg::this_cluster();
     const int b = blockIdx.x >> 2;
-    const int first = (int)cl.block_rank() * kRecQuarter; // this block's positions
+    const int rank = (int)cl.block_rank();
+    const int first = rank * kRecQuarter; // this block's positions: cells 32 rank .. 32 rank + 31
     const uint8_t *src = cells + ((size_t)b * kExtElems + first) * 32;
-    const Fr *zvb = zv + (size_t)b * kCells;
-    const Fr *izb = inv_zc + (size_t)b * kCells;
+
+    // Z on the domain needs the roots w_128^brev7(m) of the missing cells m; its
+    // inverse on the coset needs no inversion: the 128 roots are all the 128th
+    // roots of unity, so for y = 7^64 x (x one of them)
+    //   prod over all m of (y - root_m) = y^128 - 1 = 7^8192 - 1,
+    //   1 / Zs(y) = prod over present m of (y - root_m) / (7^8192 - 1).
+    // root_of lists the missing cells' roots first, then the present ones.
+    int before_m = 0, before_p = 0;
+    bool missing = false;
+    if (threadIdx.x < kCells) { // warps 0-3, whole warps
+        missing = present[(size_t)b * kCells + threadIdx.x] == 0;
+        const unsigned ball = __ballot_sync(0xffffffffu, missing);
+        const unsigned lower = (1u << (threadIdx.x & 31)) - 1u;
+        before_m = __popc(ball & lower);
+        before_p = __popc(~ball & lower);
+        if ((threadIdx.x & 31) == 0) warp_miss[threadIdx.x >> 5] = __popc(ball);
+    }
+    __syncthreads();
+    int n_miss = 0;
+    for (int w = 0; w < kCells / 32; w++) {
+        if (w < (int)(threadIdx.x >> 5)) {
+            before_m += warp_miss[w];
+            before_p += 32 - warp_miss[w];
+        }
+        n_miss += warp_miss[w];
+    }
+    if (threadIdx.x < kCells)
+        root_of[missing ? before_m : n_miss + before_p] = (uint8_t)brev_bits(threadIdx.x, 7);
+    if (err && rank == 0 && threadIdx.x == 0) err[b] = n_miss > kCellElems ? 1u : 0u;
+    __syncthreads();
+    // this block's 32 cells: thread (sub, j) multiplies list entries 16 sub ..
+    // 16 sub + 15 into a domain and a coset partial product, kept in the (not yet
+    // used) shared buffer as [sub][domain / coset][j]
+    {
+        const int j = threadIdx.x & 31, sub = threadIdx.x >> 5;
+        const Fr x = ldg_vec(&roots_fwd[brev_bits((uint32_t)(rank * kQCells + j), 7) * 64]);
+        const Fr xc = fr_mul(x, seven64);
+        Fr dom = fr_one(), cos = fr_one();
+        for (int i = sub * kZSlice; i < (sub + 1) * kZSlice; i++) {
+            const Fr r = ldg_vec(&roots_fwd[(int)root_of[i] * 64]);
+            if (i < n_miss) dom = fr_mul(dom, fr_sub(x, r));
+            else cos = fr_mul(cos, fr_sub(xc, r));
+        }
+        st_vec(&s[(2 * sub) * kQCells + j], dom);
+        st_vec(&s[(2 * sub + 1) * kQCells + j], cos);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * kQCells) {
+        const int j = threadIdx.x & 31, kind = threadIdx.x >> 5;
+        Fr v = ld_vec(&s[kind * kQCells + j]);
+        for (int sub = 1; sub < kRecQThreads / kQCells; sub++) v = fr_mul(v, ld_vec(&s[(2 * sub + kind) * kQCells + j]));
+        if (kind == 0) st_vec(&zq[j], fr_mul(v, Fr{VK_FR_R2})); // R folded in: cell words are raw
+        else st_vec(&izq[j], fr_mul(v, coset_scale));
+    }
+    __syncthreads();
 
     // A: X = E . Z on the domain (bit-reversed), inverse DIT inner stages
     for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads) {
@@ -145,7 +172,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_R
         Fr v;
         v.v[7] = bswap32(lo.x); v.v[6] = bswap32(lo.y); v.v[5] = bswap32(lo.z); v.v[4] = bswap32(lo.w);
         v.v[3] = bswap32(hi.x); v.v[2] = bswap32(hi.y); v.v[1] = bswap32(hi.z); v.v[0] = bswap32(hi.w);
-        st_vec(&s[q], fr_mul(ld_vec(&zvb[(first + q) >> 6]), v)); // raw word second
+        st_vec(&s[q], fr_mul(ld_vec(&zq[q >> 6]), v)); // raw word second
     }
     __syncthreads();
     smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
@@ -156,7 +183,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_R
     // C: coset FFT inner stages, divide by Z on the coset, inverse DIT inner stages
     smem_dif<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
     for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads)
-        st_vec(&s[q], fr_mul(ld_vec(&s[q]), ld_vec(&izb[(first + q) >> 6])));
+        st_vec(&s[q], fr_mul(ld_vec(&s[q]), ld_vec(&izq[q >> 6])));
     __syncthreads();
     smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
     cl.sync();
@@ -175,29 +202,37 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_R
     }
 }
 
-static void launch_recover_transforms(const DeviceTables &t, const uint8_t *cells, uint8_t *out, const Fr *zv,
-                                      const Fr *inv_zc, int n, cudaStream_t s) {
-    k_recover_cluster<<<4 * n, kRecQThreads, kRecQuarter * sizeof(Fr), s>>>(cells, out, zv, inv_zc, t.roots_fwd,
-                                                                            t.roots_inv, t.shift_fwd, t.shift_inv);
-}
-
 static Fr host_seven64() {
     Fr seven = fr_from_u32(7), acc = seven;
     for (int i = 0; i < 6; i++) acc = fr_mul(acc, acc); // 7^64
     return acc;
 }
 
+// 1 / (7^8192 - 1): the product of y - w over all 128th roots of unity w is
+// y^128 - 1, and y^128 = 7^8192 for every y on the coset 7^64 w_128^j
+static Fr host_coset_scale() {
+    Fr acc = fr_from_u32(7);
+    for (int i = 0; i < 13; i++) acc = fr_mul(acc, acc); // 7^8192
+    return fr_inv(fr_sub(acc, fr_one()));
+}
+
+static cudaError_t launch_recover_cluster(const DeviceTables &t, const uint8_t *cells, const uint8_t *present,
+                                          uint8_t *out, uint32_t *err, int n, cudaStream_t s) {
+    static const Fr seven64 = host_seven64();
+    static const Fr coset_scale = host_coset_scale();
+    k_recover_cluster<<<4 * n, kRecQThreads, kRecQuarter * sizeof(Fr), s>>>(
+        cells, present, out, t.roots_fwd, t.roots_inv, t.shift_fwd, t.shift_inv, seven64, coset_scale, err);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_recover_timed(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s,
                                  cudaEvent_t *ev) {
     if (n <= 0) return cudaSuccess;
-    static const Fr seven64 = host_seven64();
     if (ev) cudaEventRecord(ev[0], s);
-    k_recover_prep<<<n, kCells, 0, s>>>(w.present, t.roots_fwd, seven64, w.zv, w.inv_zc, w.err);
+    const cudaError_t e = launch_recover_cluster(t, w.cells, w.present, w.out, w.err, n, s);
     if (ev) cudaEventRecord(ev[1], s);
-    launch_recover_transforms(t, w.cells, w.out, w.zv, w.inv_zc, n, s);
-    if (ev) cudaEventRecord(ev[2], s);
-    count_launches(2);
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, cudaStream_t s) {
@@ -210,57 +245,18 @@ cudaError_t configure_recover_kernels() {
 }
 
 // ------------------------------------------ allocation-free recovery variant
-// Scratch for vkzg_b200_recover_cells_device_noalloc: a fixed array in the
-// module's device memory instead of the prover's cudaMalloc'd working set.
-// Per blob: Z on the domain and 1/Z on the coset (128 elements each; the
-// transforms work in shared memory).  Every GPU that loads this library holds
-// it (128 KiB) until the process exits; all calls share it.
+// vkzg_b200_recover_cells_device_noalloc: the same kernel, which keeps all of
+// its working state in shared memory and needs no scratch, on the caller's
+// buffers; the 16-blob limit is part of that entry point's contract.
 constexpr int kNoAllocMaxBlobs = 16;
-constexpr size_t kNoAllocPerBlob = 2 * kCells;
-static __device__ __align__(256) Fr g_noalloc_scratch[kNoAllocMaxBlobs * kNoAllocPerBlob];
-
-namespace {
-std::mutex g_noalloc_mutex;
-Fr *g_noalloc_addr[64] = {};
-} // namespace
-
-// Device address of g_noalloc_scratch on the current device.  The host-side
-// symbol is only a stand-in; the address is fetched once per device.
-static cudaError_t noalloc_scratch_address(Fr **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_addr[dev] = reinterpret_cast<Fr *>(ptr);
-    }
-    *out = g_noalloc_addr[dev];
-    return cudaSuccess;
-}
 
 int noalloc_max_blobs() { return kNoAllocMaxBlobs; }
 
-// Same two kernels as launch_recover, with the Z tables carved out of
-// g_noalloc_scratch.  Nothing in the scratch needs to start at zero: the prep
-// kernel writes zv / inv_zc before the transforms read them.
 cudaError_t launch_recover_noalloc(const DeviceTables &t, const uint8_t *cells, const uint8_t *present, uint8_t *out,
                                    uint32_t *err, int n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     if (n > kNoAllocMaxBlobs) return cudaErrorInvalidValue;
-    Fr *base = nullptr;
-    cudaError_t e = noalloc_scratch_address(&base);
-    if (e != cudaSuccess) return e;
-    Fr *zv = base;
-    Fr *inv_zc = zv + (size_t)kNoAllocMaxBlobs * kCells;
-    static const Fr seven64 = host_seven64();
-    k_recover_prep<<<n, kCells, 0, s>>>(present, t.roots_fwd, seven64, zv, inv_zc, err);
-    launch_recover_transforms(t, cells, out, zv, inv_zc, n, s);
-    count_launches(2);
-    return cudaGetLastError();
+    return launch_recover_cluster(t, cells, present, out, err, n, s);
 }
 
 } // namespace vkzg
