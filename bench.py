@@ -466,6 +466,33 @@ def run_ours(args, rank, world, local_rank):
     e2e_proof_rate = n * args.steps / sum(e2e_p)
     e2e_rec_rate = n * args.steps / sum(e2e_r)
 
+    # ---- the next rows through the C ABI (host buffers, copies in the timed
+    # region): cells from blobs, cells + proofs from one upload, recovered
+    # cells + the proofs of the recovered blobs; median of 3 calls each
+    next_rows = None
+    if not args.no_next:
+        L, hp = prover._lib, prover.handle
+        h_cells_out = torch.empty(n * EXT, dtype=torch.uint8).pin_memory()
+        calls = {
+            "cells_blobs_per_s": lambda: L.vkzg_b200_compute_cells_batch(
+                hp, h_cells_out.data_ptr(), h_blobs.data_ptr(), n),
+            "cells_and_proofs_blobs_per_s": lambda: L.vkzg_b200_compute_cells_and_proofs_batch(
+                hp, h_cells_out.data_ptr(), h_proofs.data_ptr(), h_blobs.data_ptr(), n),
+            "recovered_cells_and_proofs_blobs_per_s": lambda: L.vkzg_b200_recover_cells_and_proofs_batch(
+                hp, h_cells_out.data_ptr(), h_proofs.data_ptr(), h_cells.data_ptr(), h_present.data_ptr(), n),
+        }
+        next_rows = {"blobs": n, "timing": "per GPU; wall clock around each synchronous call, L2 flushed before each"}
+        for key, call in calls.items():
+            assert call() == 0
+            ts = []
+            for _ in range(3):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                assert call() == 0
+                ts.append(time.perf_counter() - t0)
+            next_rows[key] = n / statistics.median(ts)
+
     # ---- the plain form (one call per blob) and the served form, one replica each
     plain = plain_rates(prover, h_blobs, h_cells, h_present, args.plain_sample) if not args.no_plain else None
     serving, checked, serve_setup_s = None, 0, None
@@ -522,6 +549,7 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": n * BLOB + n * EXT + n * 128,
                 "d2h_bytes_per_step": n * PROOFS + n * EXT,
                 "proof_blobs_per_s": world * e2e_proof_rate, "recovery_blobs_per_s": world * e2e_rec_rate},
+        "next_rows": next_rows,
         "plain_per_blob": plain,
         "batched_over_plain": (e2e_value / world) / plain["value"] if plain else None,
         "serving": {"sweep": serving, "lanes": args.serve_lanes, "max_blobs_per_batch": args.serve_batch,
@@ -564,6 +592,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the cells / cells+proofs / recovered+proofs rates")
     ap.add_argument("--profile-case", nargs="?", const="proofs", choices=["proofs", "recovery"],
                     help="small untimed case for ncu captures")
     ap.add_argument("--plain-sample", type=int, default=16)

@@ -4,14 +4,16 @@
 // reference's test vectors (tests/vectors/compute_cells_and_kzg_proofs_*,
 // spans 1..128, which tests/vectors.h:88-95 skips).
 //
-// Per blob, one block: inverse NTT-4096 of the blob (bit-reversed evaluations
-// -> natural coefficients f, as in the proof path), then the forward NTT-8192
-// of f zero-padded, whose bit-reversed output order is the cells' wire order.
-// The outermost DIF stage of that transform pairs k with k+4096, where the
-// upper input half is zero: it reduces to (f[k], f[k] w_8192^k).  So the block
-// keeps f in shared memory for the lower half and parks f . w^k in global
-// scratch for the upper half.  The 1/4096 scale carries an extra 1/R, so the
-// Montgomery limbs of every output are its canonical value.
+// Per blob, one block.  The wire order of the 8192 extended evaluations is
+// bit-reversed: position p holds the value at w_8192^brev13(p), and for p < 4096
+// brev13(p) = 2 brev12(p), so the first 64 cells are the blob itself (its
+// element p is the value at w_4096^brev12(p)); those bytes are copied.  The
+// other 64 cells are the values on the coset w_8192 D_4096: the forward NTT-4096
+// of f_k w_8192^k, f the blob's coefficients from an inverse NTT-4096
+// (bit-reversed evaluations -> natural coefficients, as in the proof path), and
+// that DIF transform's bit-reversed output is the cells' wire order.  The
+// 1/4096 scale carries an extra 1/R, so the Montgomery limbs of every output
+// are its canonical value.
 #include "device_util.cuh"
 #include "kernels.h"
 
@@ -20,18 +22,21 @@ namespace vkzg {
 constexpr int kCellsThreads = 512;
 
 __global__ void __launch_bounds__(kCellsThreads, 1) k_blob_to_cells(const uint8_t *__restrict__ blobs, uint8_t *cells,
-                                                                   Fr *scratch, const Fr *__restrict__ roots_fwd,
+                                                                   const Fr *__restrict__ roots_fwd,
                                                                    const Fr *__restrict__ roots_inv, Fr scale,
                                                                    uint32_t *err) {
     extern __shared__ uint4 smem_raw[];
     Fr *s = reinterpret_cast<Fr *>(smem_raw);
     const int b = blockIdx.x;
     const uint8_t *src = blobs + (size_t)b * kBlobBytes;
-    Fr *g = scratch + (size_t)b * kExtElems;
+    uint8_t *dst = cells + (size_t)b * kExtElems * 32;
     bool bad = false;
     for (int i = threadIdx.x; i < kBlobElems; i += kCellsThreads) {
         const uint4 *p = reinterpret_cast<const uint4 *>(src + 32 * (size_t)i);
         const uint4 lo = p[0], hi = p[1];
+        uint4 *w = reinterpret_cast<uint4 *>(dst + 32 * (size_t)i); // first half of the cells: the blob
+        w[0] = lo;
+        w[1] = hi;
         Fr v;
         v.v[7] = bswap32(lo.x); v.v[6] = bswap32(lo.y); v.v[5] = bswap32(lo.z); v.v[4] = bswap32(lo.w);
         v.v[3] = bswap32(hi.x); v.v[2] = bswap32(hi.y); v.v[1] = bswap32(hi.z); v.v[0] = bswap32(hi.w);
@@ -41,37 +46,26 @@ __global__ void __launch_bounds__(kCellsThreads, 1) k_blob_to_cells(const uint8_
     if (bad) atomicOr(&err[b], 1u);
     __syncthreads();
     smem_dit<kCellsThreads>(s, 12, 1, 2, 4096, roots_inv);
-    // f (scaled by 1/(4096 R)); upper half of the first DIF stage to scratch
-    for (int k = threadIdx.x; k < kBlobElems; k += kCellsThreads) {
-        const Fr f = fr_mul(ld_vec(&s[k]), scale);
-        st_vec(&s[k], f);
-        st_vec(&g[k], fr_mul(f, ldg_vec(&roots_fwd[k])));
-    }
+    // f_k w_8192^k, f scaled by 1/(4096 R)
+    for (int k = threadIdx.x; k < kBlobElems; k += kCellsThreads)
+        st_vec(&s[k], fr_mul(fr_mul(ld_vec(&s[k]), scale), ldg_vec(&roots_fwd[k])));
     __syncthreads();
-    uint8_t *dst = cells + (size_t)b * kExtElems * 32;
-    for (int h = 0; h < 2; h++) {
-        if (h == 1) {
-            for (int q = threadIdx.x; q < kBlobElems; q += kCellsThreads) st_vec(&s[q], ld_vec(&g[q]));
-            __syncthreads();
-        }
-        smem_dif<kCellsThreads>(s, 12, 1, 4096, 2, roots_fwd);
-        for (int q = threadIdx.x; q < kBlobElems; q += kCellsThreads) {
-            const Fr v = ld_vec(&s[q]);
-            uint4 *w = reinterpret_cast<uint4 *>(dst + 32 * (size_t)(h * kBlobElems + q));
-            w[0] = make_uint4(bswap32(v.v[7]), bswap32(v.v[6]), bswap32(v.v[5]), bswap32(v.v[4]));
-            w[1] = make_uint4(bswap32(v.v[3]), bswap32(v.v[2]), bswap32(v.v[1]), bswap32(v.v[0]));
-        }
-        __syncthreads();
+    smem_dif<kCellsThreads>(s, 12, 1, 4096, 2, roots_fwd);
+    for (int q = threadIdx.x; q < kBlobElems; q += kCellsThreads) {
+        const Fr v = ld_vec(&s[q]);
+        uint4 *w = reinterpret_cast<uint4 *>(dst + 32 * (size_t)(kBlobElems + q));
+        w[0] = make_uint4(bswap32(v.v[7]), bswap32(v.v[6]), bswap32(v.v[5]), bswap32(v.v[4]));
+        w[1] = make_uint4(bswap32(v.v[3]), bswap32(v.v[2]), bswap32(v.v[1]), bswap32(v.v[0]));
     }
 }
 
-cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, Fr *scratch, uint32_t *err,
-                         int n, cudaStream_t s) {
+cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, uint32_t *err, int n,
+                         cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     // (1/4096) / R: the canonical integer of the Montgomery constant 1/4096
     static const Fr scale = fr_to_canonical(fr_inv(fr_from_u32(kBlobElems)));
-    k_blob_to_cells<<<n, kCellsThreads, kBlobElems * sizeof(Fr), s>>>(blobs, cells, scratch, t.roots_fwd,
-                                                                      t.roots_inv, scale, err);
+    k_blob_to_cells<<<n, kCellsThreads, kBlobElems * sizeof(Fr), s>>>(blobs, cells, t.roots_fwd, t.roots_inv, scale,
+                                                                      err);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -160,7 +160,6 @@ struct RecoverWork {
     uint8_t *cells = nullptr;     // [cap][8192*32]
     uint8_t *present = nullptr;   // [cap][128]
     uint8_t *out = nullptr;       // [cap][8192*32]
-    Fr *scratch = nullptr;        // [cap][8192]
     uint32_t *err = nullptr;      // [cap] more than 64 cells missing
 };
 

@@ -588,8 +588,7 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
               p->alloc(w.ladder_aff, B * kCells * kDigits) &&
               p->alloc(w.proofs, B * kCells * kProofBytes) && p->alloc(w.err, B) &&
               p->alloc(r.cells, B * kExtElems * 32) && p->alloc(r.present, B * kCells) &&
-              p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.scratch, B * kExtElems) &&
-              p->alloc(r.err, B);
+              p->alloc(r.out, B * kExtElems * 32) && p->alloc(r.err, B);
     if (!ok) return VKZG_ERR_MALLOC;
     if (cudaMallocHost(&p->h_err, B * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
     // batch-affine bucket accumulation: one scratch slot per resident block
@@ -1086,7 +1085,6 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         w.cells += off * ext;
         w.present += (size_t)off * kCells;
         w.out += off * ext;
-        w.scratch += (size_t)off * kExtElems;
         w.err += off;
         CK(cudaMemcpyAsync(w.cells, cells + off * ext, cnt * ext, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(w.present, present + (size_t)off * kCells, (size_t)cnt * kCells, cudaMemcpyHostToDevice, st));
@@ -1305,8 +1303,8 @@ vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_ce
 // ------------------------------------------------- cells (2x RS extension)
 
 namespace vkzg {
-cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, Fr *scratch, uint32_t *err,
-                         int n, cudaStream_t s);
+cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, uint32_t *err, int n,
+                         cudaStream_t s);
 cudaError_t configure_cells_kernels();
 } // namespace vkzg
 
@@ -1321,7 +1319,7 @@ vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const u
     cudaStream_t s = p->stream;
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
-    CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->rw.scratch, p->pw.err, (int)n, s));
+    CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->pw.err, (int)n, s));
     p->pw.plan = plan_for(p, n);
     if (proofs) CK(run_proofs(p, p->pw, n));
     CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
