@@ -471,15 +471,13 @@ def run_ours(args, rank, world, local_rank):
     # cells + the proofs of the recovered blobs; median of 3 calls each
     next_rows = None
     if not args.no_next:
-        L, hp = prover._lib, prover.handle
         h_cells_out = torch.empty(n * EXT, dtype=torch.uint8).pin_memory()
         calls = {
-            "cells_blobs_per_s": lambda: L.vkzg_b200_compute_cells_batch(
-                hp, h_cells_out.data_ptr(), h_blobs.data_ptr(), n),
-            "cells_and_proofs_blobs_per_s": lambda: L.vkzg_b200_compute_cells_and_proofs_batch(
-                hp, h_cells_out.data_ptr(), h_proofs.data_ptr(), h_blobs.data_ptr(), n),
-            "recovered_cells_and_proofs_blobs_per_s": lambda: L.vkzg_b200_recover_cells_and_proofs_batch(
-                hp, h_cells_out.data_ptr(), h_proofs.data_ptr(), h_cells.data_ptr(), h_present.data_ptr(), n),
+            "cells_blobs_per_s": lambda: prover.compute_cells_raw(h_cells_out.data_ptr(), h_blobs.data_ptr(), n),
+            "cells_and_proofs_blobs_per_s": lambda: prover.compute_cells_and_proofs_raw(
+                h_cells_out.data_ptr(), h_proofs.data_ptr(), h_blobs.data_ptr(), n),
+            "recovered_cells_and_proofs_blobs_per_s": lambda: prover.recover_cells_and_proofs_raw(
+                h_cells_out.data_ptr(), h_proofs.data_ptr(), h_cells.data_ptr(), h_present.data_ptr(), n),
         }
         next_rows = {"blobs": n, "timing": "per GPU; wall clock around each synchronous call, L2 flushed before each"}
         for key, call in calls.items():

@@ -116,7 +116,7 @@ def test_server_wait_timeout_keeps_ticket(golden_proofs):
     with vkzg_b200.Server(max_blobs_per_batch=64) as s:
         out = np.zeros(len(blobs) * 6144, np.uint8)
         t = s.submit_proofs(out, blobs, len(blobs))
-        rc = s._lib.vkzg_b200_server_wait(s._h, t, 0)
+        rc = s.wait(t, 0)
         assert rc in (vkzg_b200.ERR_GPU, vkzg_b200.OK)
         if rc == vkzg_b200.ERR_GPU:
             assert s.wait(t) == vkzg_b200.OK

@@ -232,6 +232,18 @@ class Prover:
     def recover_cells_raw(self, cells_out, cells, present, n):
         return self._lib.vkzg_recover_cells_batch(self._h, _ptr(cells_out), _ptr(cells), _ptr(present), n)
 
+    def compute_cells_raw(self, cells_out, blobs, n):
+        """vkzg_b200_compute_cells_batch on caller-owned buffers; returns the status."""
+        return self._lib.vkzg_b200_compute_cells_batch(self._h, _ptr(cells_out), _ptr(blobs), n)
+
+    def compute_cells_and_proofs_raw(self, cells_out, proofs_out, blobs, n):
+        return self._lib.vkzg_b200_compute_cells_and_proofs_batch(self._h, _ptr(cells_out), _ptr(proofs_out),
+                                                                  _ptr(blobs), n)
+
+    def recover_cells_and_proofs_raw(self, cells_out, proofs_out, cells, present, n):
+        return self._lib.vkzg_b200_recover_cells_and_proofs_batch(self._h, _ptr(cells_out), _ptr(proofs_out),
+                                                                  _ptr(cells), _ptr(present), n)
+
     def compute_cell_kzg_proofs_batch(self, blobs, blob_count):
         """Vkzg.computeCellKzgProofsBatch (Vkzg.java:204-229)."""
         if len(blobs) != blob_count * BYTES_PER_BLOB:
@@ -372,9 +384,12 @@ class Server:
         return t.value
 
     def wait(self, ticket, timeout_ms=-1):
-        """Returns the request's status code (0 = ok)."""
+        """Returns the request's status code (0 = ok); ERR_GPU when timeout_ms ran
+        out first, in which case the request is still in flight, its ticket stays
+        valid and its buffers stay referenced here."""
         rc = self._lib.vkzg_b200_server_wait(self._h, ticket, int(timeout_ms))
-        self._keep.pop(ticket, None)
+        if rc != ERR_GPU or timeout_ms < 0:
+            self._keep.pop(ticket, None)
         return rc
 
     def stats(self, reset=False):
