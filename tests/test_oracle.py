@@ -33,6 +33,34 @@ def test_cells_vectors(oracle, golden_proofs):
     for k in range(len(golden_proofs["valid_names"])):
         digest = hashlib.sha256(cells[k * 262144:(k + 1) * 262144].tobytes()).digest()
         assert digest == golden_proofs["valid_cells_sha256"][k].tobytes()
+        # the first 64 cells are the blob's own bytes (wire position p < 4096 is
+        # the value at w_8192^(2 brev12(p))): the device kernel copies them
+        assert np.array_equal(cells[k * 262144:k * 262144 + 131072], golden_proofs["valid_blobs"][k])
+
+
+def test_coset_inverse_of_vanishing_polynomial_without_inversion():
+    """The identity the device recovery uses for 1/Z on the 7-coset: the roots
+    w_128^brev7(m) of the 128 cells are all the 128th roots of unity, so for
+    y = 7^64 w_128^j, prod over all m of (y - root_m) = y^128 - 1 = 7^8192 - 1 and
+    1/Zs(y) = prod over present m of (y - root_m) / (7^8192 - 1)."""
+    w128 = pow(7, (R_MOD - 1) // 128, R_MOD)
+    roots = [pow(w128, int(f"{m:07b}"[::-1], 2), R_MOD) for m in range(128)]
+    assert sorted(roots) == sorted(pow(w128, k, R_MOD) for k in range(128))
+    scale = pow((pow(7, 8192, R_MOD) - 1) % R_MOD, R_MOD - 2, R_MOD)
+    seven64 = pow(7, 64, R_MOD)
+    rng = np.random.default_rng(7)
+    for trial in range(12):
+        missing = set(rng.choice(128, int(rng.integers(0, 65)), replace=False).tolist())
+        for c in rng.choice(128, 4, replace=False):
+            y = seven64 * roots[int(c)] % R_MOD
+            zs = 1
+            for m in missing:
+                zs = zs * (y - roots[m]) % R_MOD
+            prod_present = 1
+            for m in range(128):
+                if m not in missing:
+                    prod_present = prod_present * (y - roots[m]) % R_MOD
+            assert pow(zs, R_MOD - 2, R_MOD) == prod_present * scale % R_MOD
 
 
 def test_invalid_blobs(oracle, mainnet_tables, golden_proofs):
