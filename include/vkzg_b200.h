@@ -138,13 +138,15 @@ uint64_t vkzg_b200_kernel_launches(void);
  *
  * Requests of any blob count are submitted without blocking and identified by
  * a ticket; their buffers must stay valid until vkzg_b200_server_wait returns
- * for the ticket.  A dispatcher cuts pending requests into batches (one kind
+ * the ticket's final status (not its timeout).  A dispatcher cuts pending requests into batches (one kind
  * per batch, first come first served, at most max_blobs_per_batch blobs;
  * larger requests are split) and hands each batch to a free lane: a prover with
  * its own CUDA stream and buffers, so batches on different lanes run
  * concurrently on the GPU and requests that arrive while lanes are busy join
  * the next batch.  A batch is admitted only while the device working set of
- * all batches in flight stays within hbm_budget_bytes.  Each blob is computed
+ * all batches in flight stays within hbm_budget_bytes (a batch is always admitted
+ * when none is in flight, so a budget below one batch serialises batches; the
+ * dispatcher sleeps until a batch completes).  Each blob is computed
  * independently, so a request's output is the same alone and in any mix.
  * vkzg_b200_server_new tunes the proof plan of every batch size class up to
  * max_blobs_per_batch on one lane and gives the choices to all lanes, so that
