@@ -150,11 +150,15 @@ uint64_t vkzg_b200_kernel_launches(void);
  * independently, so a request's output is the same alone and in any mix.
  * vkzg_b200_server_new tunes the proof plan of every batch size class up to
  * max_blobs_per_batch on one lane and gives the choices to all lanes, so that
- * no request waits for a tuning run.  vkzg_b200_server_wait returns the request's status (VKZG_ERR_INVALID_BLOB /
- * VKZG_ERR_BADARGS as the batch calls would; VKZG_ERR_GPU on timeout, with the
- * ticket still valid).  Stats cover requests completed since the last reset:
- * latency from submit to completion.
+ * no request waits for a tuning run.  vkzg_b200_server_wait returns the request's final status
+ * (VKZG_ERR_INVALID_BLOB / VKZG_ERR_BADARGS / VKZG_ERR_GPU as the batch calls would), after
+ * which the ticket is spent; or VKZG_B200_PENDING when timeout_ms ran out first, in which case
+ * the request is still in flight, its buffers are still in use and the ticket stays valid.
+ * Stats cover requests completed since the last reset: latency from submit to completion.
  */
+/* Status of vkzg_b200_server_wait only: the wait timed out before the request
+ * finished.  Outside the reference's vkzg_result values 0..6. */
+#define VKZG_B200_PENDING ((vkzg_result)7)
 typedef struct vkzg_server vkzg_server;
 typedef struct {
     uint32_t max_blobs_per_batch; /* 0 = 128 */

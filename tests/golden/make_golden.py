@@ -1,8 +1,9 @@
 """Converts the consensus-spec vectors that jtraglia/vkzg ships (tests/vectors/*/data.yaml)
 into compact binary fixtures for this repository's tests.
 
-Run from the repository root, in a container where the reference checkout exists:
-    python tests/golden/make_golden.py /root/reference/tests/vectors
+Run from the repository root, where a reference checkout exists:
+    python tests/golden/make_golden.py <reference checkout>/tests/vectors
+(or with $VKZG_REFERENCE_DIR set and no argument).
 
 compute_cells_and_kzg_proofs.npz
     valid_names, valid_blobs [7,131072] u8, valid_proofs [7,6144] u8 (wire order, as in
@@ -73,5 +74,10 @@ def main(vec_dir, out_dir):
 
 
 if __name__ == "__main__":
-    vec_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/vectors"
+    if len(sys.argv) > 1:
+        vec_dir = sys.argv[1]
+    elif os.environ.get("VKZG_REFERENCE_DIR"):
+        vec_dir = os.path.join(os.environ["VKZG_REFERENCE_DIR"], "tests", "vectors")
+    else:
+        sys.exit("usage: make_golden.py <reference checkout>/tests/vectors (or set VKZG_REFERENCE_DIR)")
     main(vec_dir, os.path.dirname(os.path.abspath(__file__)))

@@ -110,16 +110,19 @@ def test_server_one_byte_budget_still_serves_every_request(golden_proofs, golden
 
 
 def test_server_wait_timeout_keeps_ticket(golden_proofs):
-    """wait() with a zero timeout on a request still in flight returns ERR_GPU and
-    the ticket stays valid; an unknown ticket is BADARGS."""
+    """wait() with a zero timeout on a request still in flight returns PENDING and
+    the ticket stays valid; a spent or unknown ticket is BADARGS."""
     blobs = np.tile(golden_proofs["valid_blobs"], (10, 1))
     with vkzg_b200.Server(max_blobs_per_batch=64) as s:
         out = np.zeros(len(blobs) * 6144, np.uint8)
         t = s.submit_proofs(out, blobs, len(blobs))
         rc = s.wait(t, 0)
-        assert rc in (vkzg_b200.ERR_GPU, vkzg_b200.OK)
-        if rc == vkzg_b200.ERR_GPU:
+        assert rc in (vkzg_b200.PENDING, vkzg_b200.OK)
+        if rc == vkzg_b200.PENDING:
+            assert t in s._keep
             assert s.wait(t) == vkzg_b200.OK
+        assert t not in s._keep
+        assert s.wait(t) == vkzg_b200.ERR_BADARGS
         assert s.wait(t + 1000) == vkzg_b200.ERR_BADARGS
         want = np.tile(golden_proofs["valid_proofs"], (10, 1)).reshape(-1)
         assert np.array_equal(out, want)

@@ -1,6 +1,7 @@
 """The CPU oracle against the consensus-spec vectors the reference ships, and
 against independent forms of the same math (CPU only)."""
 import hashlib
+import os
 
 import numpy as np
 import pytest
@@ -149,3 +150,22 @@ def test_g1_kats(oracle, mainnet_setup):
     assert inf == bytes([0xC0]) + bytes(47)
     # G1 generator x-coordinate (compressed form of the first setup point)
     assert g[:4].hex() == "97f1d3a7"
+
+
+def test_spec_vectors_dir_round_trips(tmp_path, golden_proofs, golden_recover, oracle):
+    """The vectors directory written for the reference's test program holds the
+    fixtures' bytes, laid out as tests/vectors.h:68-136 parses them."""
+    import yaml
+    from spec_vectors import write_vectors_dir
+    root = write_vectors_dir(str(tmp_path), golden_proofs, golden_recover, oracle)
+    names = sorted(os.listdir(root))
+    assert len(names) == 17
+    for k, name in enumerate(golden_proofs["valid_names"]):
+        y = yaml.safe_load(open(os.path.join(root, str(name), "data.yaml")))
+        assert bytes.fromhex(y["input"]["blob"][2:]) == golden_proofs["valid_blobs"][k].tobytes()
+        assert len(y["output"][0]) == 128
+        assert b"".join(bytes.fromhex(x[2:]) for x in y["output"][1]) == golden_proofs["valid_proofs"][k].tobytes()
+    for name in golden_recover["names"]:
+        y = yaml.safe_load(open(os.path.join(root, str(name), "data.yaml")))
+        assert y["input"]["cell_indices"] == [int(i) for i in golden_recover[str(name) + "__indices"]]
+        assert (y["output"] is None) == (str(name) + "__expected" not in golden_recover)

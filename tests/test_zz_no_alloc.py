@@ -8,11 +8,13 @@ recovery with no scratch: each blob's cluster of four blocks keeps its working
 state in shared memory.
 
 The test calls it through the C ABI twice in a row, on different inputs, and
-checks each output byte for byte against the existing device entry point
-(vkzg_b200_recover_cells_device, which uses the prover's cudaMalloc'd working
-set).  Recovery is exact integer work, so the tolerance is zero.  It builds its
-own prover and inputs, so it passes alone in a fresh process as well as after
-the other tests.
+checks each output byte for byte against the CPU oracle's recovery of the same
+inputs (an independent restatement: per-element Fermat division, separate
+transforms), and against the existing device entry point.  Recovery is exact
+integer work, so the tolerance is zero.  A blob with more than 64 cells missing
+must get a nonzero error word while the others in the same call still recover.
+The test builds its own prover and inputs, so it passes alone in a fresh process
+as well as after the other tests.
 """
 import numpy as np
 import pytest
@@ -42,35 +44,57 @@ def _inputs(n, seed):
     return cells.reshape(n, EXT), present
 
 
-def test_noalloc_recovery_matches_device_entry_point():
-    torch = pytest.importorskip("torch")
+def _device_call(torch, prover, fn, cells_np, present_np, fill):
     dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
-    prover = vkzg_b200.Prover(max_batch_size=vkzg_b200.NOALLOC_MAX_BLOBS)
+    n = len(present_np)
+    cells = torch.from_numpy(np.ascontiguousarray(cells_np)).to(dev)
+    present = torch.from_numpy(np.ascontiguousarray(present_np)).to(dev)
+    out = torch.full((n * EXT,), fill, dtype=torch.uint8, device=dev)
+    err = torch.full((n,), 7, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = fn(out.data_ptr(), cells.data_ptr(), present.data_ptr(), err.data_ptr(), n, stream)
+    torch.cuda.synchronize()
+    return rc, out.cpu().numpy(), err.cpu().numpy()
+
+
+def test_noalloc_recovery_matches_oracle(oracle):
+    torch = pytest.importorskip("torch")
+    torch.cuda.set_device(0)
+    prover = vkzg_b200.Prover(max_batch_size=vkzg_b200.NOALLOC_MAX_BLOBS)
     try:
         for call, (n, seed) in enumerate([(5, 11), (vkzg_b200.NOALLOC_MAX_BLOBS, 12)]):
-            cells_np, present_np = _inputs(n, seed)
-            cells = torch.from_numpy(cells_np).to(dev)
-            present = torch.from_numpy(present_np).to(dev)
-            out_ref = torch.zeros(n * EXT, dtype=torch.uint8, device=dev)
-            out_new = torch.full((n * EXT,), 0xEE, dtype=torch.uint8, device=dev)
-            err_ref = torch.full((n,), 7, dtype=torch.int32, device=dev)
-            err_new = torch.full((n,), 7, dtype=torch.int32, device=dev)
-            rc = prover.recover_cells_device(out_ref.data_ptr(), cells.data_ptr(), present.data_ptr(),
-                                             err_ref.data_ptr(), n, stream)
-            assert rc == 0
-            rc = prover.recover_cells_device_noalloc(out_new.data_ptr(), cells.data_ptr(), present.data_ptr(),
-                                                     err_new.data_ptr(), n, stream)
+            cells, present = _inputs(n, seed)
+            orc, want = oracle.recover_cells(cells, present)
+            assert orc == 0
+            rc, got, err = _device_call(torch, prover, prover.recover_cells_device_noalloc, cells, present, 0xEE)
             assert rc == 0, f"call {call}: status {rc}"
-            torch.cuda.synchronize()
-            assert int(err_new.count_nonzero()) == 0 and int(err_ref.count_nonzero()) == 0
-            assert torch.equal(out_new, out_ref), f"call {call}: outputs differ"
+            assert not err.any(), f"call {call}: error words {err}"
+            assert np.array_equal(got, want), f"call {call}: output differs from the oracle"
+            rc, via_device, _ = _device_call(torch, prover, prover.recover_cells_device, cells, present, 0)
+            assert rc == 0 and np.array_equal(via_device, got)
     finally:
         prover.close()
 
 
-def test_noalloc_rejects_more_than_its_scratch_holds():
+def test_noalloc_flags_blob_with_too_few_cells(oracle):
+    torch = pytest.importorskip("torch")
+    torch.cuda.set_device(0)
+    prover = vkzg_b200.Prover(max_batch_size=4)
+    try:
+        cells, present = _inputs(3, 13)
+        present[1] = 0
+        present[1, 3::2] = 1  # 63 present, 65 missing
+        rc, got, err = _device_call(torch, prover, prover.recover_cells_device_noalloc, cells, present, 0)
+        assert rc == 0
+        assert err[1] != 0 and err[0] == 0 and err[2] == 0
+        for b in (0, 2):
+            orc, want = oracle.recover_cells(cells[b], present[b])
+            assert orc == 0 and np.array_equal(got[b * EXT:(b + 1) * EXT], want)
+    finally:
+        prover.close()
+
+
+def test_noalloc_rejects_more_blobs_than_its_limit():
     torch = pytest.importorskip("torch")
     dev = torch.device("cuda", 0)
     prover = vkzg_b200.Prover(max_batch_size=2)

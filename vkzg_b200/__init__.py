@@ -27,6 +27,7 @@ BYTES_PER_CELL = FIELD_ELEMENTS_PER_CELL * BYTES_PER_FIELD_ELEMENT
 BYTES_PER_EXT_BLOB = CELL_PROOFS_PER_BLOB * BYTES_PER_CELL
 
 OK, ERR_BADARGS, ERR_MALLOC, ERR_IO, ERR_SETUP, ERR_GPU, ERR_INVALID_BLOB = range(7)
+PENDING = 7  # VKZG_B200_PENDING: a server wait timed out, the request is still in flight
 
 # every symbol declared in include/vkzg.h and include/vkzg_b200.h
 PLANS = 5  # VKZG_B200_PLANS
@@ -384,11 +385,12 @@ class Server:
         return t.value
 
     def wait(self, ticket, timeout_ms=-1):
-        """Returns the request's status code (0 = ok); ERR_GPU when timeout_ms ran
+        """Returns the request's final status code (0 = ok), after which the ticket
+        is spent and its buffers are released here; or PENDING when timeout_ms ran
         out first, in which case the request is still in flight, its ticket stays
         valid and its buffers stay referenced here."""
         rc = self._lib.vkzg_b200_server_wait(self._h, ticket, int(timeout_ms))
-        if rc != ERR_GPU or timeout_ms < 0:
+        if rc != PENDING:
             self._keep.pop(ticket, None)
         return rc
 

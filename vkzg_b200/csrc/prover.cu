@@ -32,6 +32,7 @@ using namespace vkzg;
 namespace vkzg {
 cudaError_t configure_proof_kernels();
 cudaError_t configure_recover_kernels();
+cudaError_t configure_cells_kernels();
 int batch_affine_blocks_per_sm();
 size_t reduce_scratch_points(int cap_blobs);
 cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s,
@@ -167,6 +168,7 @@ const char *vkzg_error_string(vkzg_result r) {
     case VKZG_ERR_GPU: return "gpu error";
     case VKZG_ERR_INVALID_BLOB: return "blob contains a non-canonical field element";
     }
+    if (r == VKZG_B200_PENDING) return "request still in flight (wait timed out)";
     return "unknown error";
 }
 
@@ -644,7 +646,10 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
     if (cudaGetDevice(&dev) != cudaSuccess) return VKZG_ERR_GPU;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return VKZG_ERR_GPU;
-    if (configure_proof_kernels() != cudaSuccess || configure_recover_kernels() != cudaSuccess) return VKZG_ERR_GPU;
+    // Kernel attributes are per device: set them on the device this prover uses.
+    if (configure_proof_kernels() != cudaSuccess || configure_recover_kernels() != cudaSuccess ||
+        configure_cells_kernels() != cudaSuccess)
+        return VKZG_ERR_GPU;
 
     vkzg_prover *p = new (std::nothrow) vkzg_prover();
     if (!p) return VKZG_ERR_MALLOC;
@@ -1305,7 +1310,6 @@ vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_ce
 namespace vkzg {
 cudaError_t launch_cells(const DeviceTables &t, const uint8_t *blobs, uint8_t *cells, uint32_t *err, int n,
                          cudaStream_t s);
-cudaError_t configure_cells_kernels();
 } // namespace vkzg
 
 namespace {
@@ -1314,8 +1318,6 @@ namespace {
 // pipelines on the same device copy of the blobs, outputs written only when
 // every blob of the chunk is canonical (the proofs path's rule).
 vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
-    static const cudaError_t configured = configure_cells_kernels();
-    if (configured != cudaSuccess) return VKZG_ERR_GPU;
     cudaStream_t s = p->stream;
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));

@@ -362,7 +362,7 @@ vkzg_result vkzg_b200_server_wait(vkzg_server *s, uint64_t ticket, int64_t timeo
     if (timeout_ms < 0) {
         s->cv_done.wait(lk, ready);
     } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
-        return VKZG_ERR_GPU; // still running: the ticket stays valid
+        return VKZG_B200_PENDING; // still running: the ticket stays valid
     }
     s->requests.erase(ticket);
     return r->status;

@@ -5,7 +5,9 @@ trusted_setup_g1_monomial.bin, checking the sha256 that src/setup_data.h:13 reco
 This is protocol data (the public ceremony output), not code: the bytes must be the
 same in every EIP-7594 implementation.
 
-    python vkzg_b200/data/make_setup.py /root/reference/src/setup_data.cpp
+    python vkzg_b200/data/make_setup.py <reference checkout>/src/setup_data.cpp
+
+(or with $VKZG_REFERENCE_DIR set and no argument).
 """
 import hashlib
 import os
@@ -27,4 +29,9 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/setup_data.cpp")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("VKZG_REFERENCE_DIR"):
+        main(os.path.join(os.environ["VKZG_REFERENCE_DIR"], "src", "setup_data.cpp"))
+    else:
+        sys.exit("usage: make_setup.py <reference checkout>/src/setup_data.cpp (or set VKZG_REFERENCE_DIR)")
