@@ -190,7 +190,9 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
  * fma.rn.f64 issue rate, in tera-ops/s; 10 and 11: the time in microseconds of
  * one launch inverting 16 Fp values per SM, one per thread (the inversion
  * between the passes of a batch-affine round), with variable-time and with
- * fixed 30-divstep batches.  Best of three timed launches.
+ * fixed 30-divstep batches; 12: Fp multiplies with the partial products on the
+ * FP64 pipe, 13: Fp squares on the FP64 pipe, 14: Fp multiplies with half the
+ * warps on each pipe (giga-ops/s).  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
 

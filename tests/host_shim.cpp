@@ -161,3 +161,19 @@ void shim_fr_inv_fast(const uint32_t *a, uint32_t *r) {
     memcpy(r, fr_inv_fast(x).v, 32);
 }
 }
+
+extern "C" {
+// Fp products on the FP64 pipe (field_f64.cuh), host build with std::fma
+void shim_fp_mul_f64(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    Fp x, y;
+    memcpy(x.v, a, 48);
+    memcpy(y.v, b, 48);
+    memcpy(r, f64::mont_mul(x, y).v, 48);
+}
+void shim_fp_sqr_f64(const uint32_t *a, const uint32_t *b, uint32_t *r) {
+    (void)b;
+    Fp x;
+    memcpy(x.v, a, 48);
+    memcpy(r, f64::mont_sqr(x).v, 48);
+}
+}

@@ -70,6 +70,27 @@ def test_field_ops(shim, field):
         assert value(out, n) == pow(a, -1, mod) * radix % mod
 
 
+def test_fp_products_on_the_fp64_pipe(shim):
+    """field_f64.cuh's products (50-bit limbs, exact FMA splits) equal a b / 2^384 mod p,
+    including limbs at their extremes (all-ones 50-bit limbs, zero limbs, p - 1)."""
+    rng = random.Random(11)
+    mask50 = (1 << 50) - 1
+    edge = [0, 1, P_MOD - 1, P_MOD - 2, (1 << 380) - 1, P_MOD >> 1, (1 << 384) % P_MOD]
+    edge += [sum(mask50 << (50 * i) for i in range(k)) % P_MOD for k in range(1, 9)]
+    edge += [(mask50 << (50 * i)) % P_MOD for i in range(8)]
+    edge += [P_MOD - 1 - (mask50 << (50 * i)) for i in range(7)]
+    edge += [P_MOD - 1 - rng.randrange(1 << 64) for _ in range(20)]
+    vals = edge + [rng.randrange(P_MOD) for _ in range(3000)]
+    rinv = pow(1 << 384, -1, P_MOD)
+    out = (ctypes.c_uint32 * 12)()
+    for k, a in enumerate(vals):
+        for b in (vals[(7 * k + 3) % len(vals)], a, P_MOD - 1, vals[-1 - k % len(vals)]):
+            shim.shim_fp_mul_f64(words(a, 12), words(b, 12), out)
+            assert value(out, 12) == a * b * rinv % P_MOD, (hex(a), hex(b))
+        shim.shim_fp_sqr_f64(words(a, 12), words(a, 12), out)
+        assert value(out, 12) == a * a * rinv % P_MOD, hex(a)
+
+
 def test_fr_from_raw_noncanonical(shim):
     """Raw 256-bit words (cells are not canonicity-checked) reduce mod r."""
     rng = random.Random(3)

@@ -99,16 +99,31 @@ __device__ __noinline__ Fp fp_sqr_ks_call(Fp a) {
     return r;
 }
 
+__device__ __noinline__ Fp fp_mul_f64_call(Fp a, Fp b) { return f64::mont_mul(a, b); }
+__device__ __noinline__ Fp fp_sqr_f64_call(Fp a) { return f64::mont_sqr(a); }
+
 // independent Fp products per thread (2 chains); OP 0: fp_mul, 1: fp_sqr, 2: the
-// one-level Karatsuba product, 3: the Karatsuba square, 4: the two-level product
+// one-level Karatsuba product, 3: the Karatsuba square, 4: the two-level product,
+// 5: the FP64-pipe product, 6: the FP64-pipe square, 7: even warps the
+// Karatsuba product and odd warps the FP64-pipe product (both pipes at once)
 template <int OP>
 __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint32_t *sink) {
     Fp a = fp_one(), b = fp_one();
     a.v[0] ^= seed + threadIdx.x;
     b.v[1] ^= seed * 3u + blockIdx.x;
     const Fp c = a;
+    const bool odd_warp = (threadIdx.x >> 5) & 1;
     for (int i = 0; i < iters; i++) {
-        if (OP == 0) {
+        if (OP == 5 || (OP == 7 && odd_warp)) {
+            a = fp_mul_f64_call(a, c);
+            b = fp_mul_f64_call(b, c);
+        } else if (OP == 6) {
+            a = fp_sqr_f64_call(a);
+            b = fp_sqr_f64_call(b);
+        } else if (OP == 7) {
+            a = fp_mul_ks_call(a, c);
+            b = fp_mul_ks_call(b, c);
+        } else if (OP == 0) {
             a = fp_mul(a, c);
             b = fp_mul(b, c);
         } else if (OP == 1) {
@@ -272,7 +287,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 11) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 14) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -304,7 +319,10 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
             else if (which == 3) k_probe_fp<1><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 4) k_probe_fp<2><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 6) k_probe_fp<3><<<blocks, 128>>>(rep + 1, fp_iters, sink);
-            else k_probe_fp<4><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 7) k_probe_fp<4><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 12) k_probe_fp<5><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 13) k_probe_fp<6><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else k_probe_fp<7><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             ops = (double)blocks * 128 * 2 * fp_iters;
         } else {
             const int blocks = sms * 8;
@@ -319,12 +337,12 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (which >= 10) { // launch time in microseconds, the smallest
+        if (which == 10 || which == 11) { // launch time in microseconds, the smallest
             const double us = ms * 1e3;
             if (rep > 0 && (best == 0.0 || us < best)) best = us;
             continue;
         }
-        const double rate = ops / (ms * 1e-3) / ((which == 0 || which >= 8) ? 1e12 : 1e9);
+        const double rate = ops / (ms * 1e-3) / ((which == 0 || which == 8 || which == 9) ? 1e12 : 1e9);
         if (rep > 0 && rate > best) best = rate;
     }
     cudaEventDestroy(e0);

@@ -144,6 +144,12 @@ VK_HD constexpr uint32_t mod_n0() {
     } while (0)
 #endif
 
+} // namespace vkzg
+
+#include "field_f64.cuh"
+
+namespace vkzg {
+
 // ------------------------------------------------------- generic n-limb ops
 // r = a + b mod m (a, b < m; m < 2^(32n-1) so the raw sum fits in n words).
 template <int N>
@@ -538,8 +544,16 @@ VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
 #ifndef VKZG_FP_KARATSUBA
 #define VKZG_FP_KARATSUBA 1
 #endif
+// VKZG_FP_F64=1 computes Fp products and squares with the partial products on
+// the FP64 pipe (field_f64.cuh); the results are the same bits.
+#ifndef VKZG_FP_F64
+#define VKZG_FP_F64 0
+#endif
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_mul_call(Fp a, Fp b) {
+#if VKZG_FP_F64
+    return f64::mont_mul(a, b);
+#endif
     Fp r;
 #if VKZG_FP_KARATSUBA
     mont_mul_ks<12, VKZG_FP_KARATSUBA>(r.v, a.v, b.v);
@@ -564,6 +578,9 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
 }
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_sqr_call(Fp a) {
+#if VKZG_FP_F64
+    return f64::mont_sqr(a);
+#endif
     Fp r;
 #if VKZG_FP_KARATSUBA
     mont_sqr_ks<12>(r.v, a.v);
