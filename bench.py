@@ -53,6 +53,17 @@ IMAD_FP_MUL_KS, IMAD_FP_SQR_KS = 516, 426
 PHASE_A_TAIL = 10  # lists of at most this many points finish in Jacobian form
 
 
+def phase_a_executed_products_per_output(c):
+    """Fp products and squares plan 3's phase A executes per MSM output at window c."""
+    m = 64 * ((256 + c - 1) // c)
+    adds = 0
+    while m > PHASE_A_TAIL:
+        adds += m // 2
+        m = (m + 1) // 2
+    madds = max(m - 2, 0)
+    return 6 * adds + 11 * madds + 16
+
+
 def phase_a_executed_imad_per_output(c):
     """Multiply instructions plan 3's phase A executes per MSM output at window c:
     affine additions (5 products + 1 square) in tree rounds down to lists of
@@ -67,9 +78,10 @@ def phase_a_executed_imad_per_output(c):
     muls = 5 * adds + 7 * madds + 11
     sqrs = adds + 4 * madds + 5
     return muls * IMAD_FP_MUL_KS + sqrs * IMAD_FP_SQR_KS
-# DRAM bytes of phase A per blob under plan 3 (13-bit digit table), from one
-# single-pass ncu capture of a 256-blob proof step (30.9 GB / 256)
-PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 = 30.9e9 / 256
+# DRAM bytes of phase A per blob under plan 3, by window: ncu dram__bytes_read +
+# dram__bytes_write of every phase-A kernel of a 16-blob proof call (one kernel
+# per capture, profiles/phase_a_dram_traffic_16blobs.md), divided by 16
+PHASE_A_DRAM_BYTES_PER_BLOB = {}
 
 
 # ------------------------------------------------------------------ inputs
@@ -259,19 +271,24 @@ def plain_rates(prover, h_blobs, h_cells, h_present, sample):
             "recovery_blobs_per_s": rr, "sample": f"{sample} proof + {sample} recovery calls of 1 blob"}
 
 
-def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions, seconds, seed=99, args_warm=0.6,
-                batch=128, lanes=3):
+def serve_sweep(want_proofs, want_cells, h_blobs, h_cells, h_present, n_pool, capacity, fractions, seconds,
+                seed=99, args_warm=0.6, batch=128, lanes=3, hbm_budget=8 << 30, table_budget=0):
     """Served mixed stream (continuous batching, vkzg_b200_server_*): Poisson arrivals,
     request sizes geometric with mean 6 in 1..64 blobs, 70% proof requests and 30%
     recovery requests (64..127 cells present).  One segment per offered load
-    (fraction x capacity blobs/s); latency is submit-to-completion inside the server.
-    Outputs land in reused pinned rings, as a serving caller's would, not in fresh
-    pageable arrays (whose first-touch page faults would be charged to the lanes)."""
+    (fraction x capacity blobs/s), after an unreported warm-up segment; latency is
+    submit-to-completion inside the server.  Outputs land in reused pinned rings, as
+    a serving caller's would, not in fresh pageable arrays (whose first-touch page
+    faults would be charged to the lanes).  Every served request's output is
+    compared with the direct call's output for the same blobs (want_proofs /
+    want_cells, one row per pool blob) as soon as it completes."""
     import queue
     import torch
     import vkzg_b200
     rng = np.random.default_rng(seed)
-    results, checks = [], []
+    results = []
+    checked = [0]
+    mismatches = []
     warming = True
     # the rings wrap after ~0.5 s of output at the highest load, far beyond any request's latency
     ring = {"proofs": torch.empty(64 << 20, dtype=torch.uint8).pin_memory().numpy(),
@@ -286,8 +303,10 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
         return ring[kind][off:off + size]
 
     t_setup = time.perf_counter()
-    with vkzg_b200.Server(max_blobs_per_batch=batch, lanes=lanes, hbm_budget_bytes=8 << 30) as srv:
+    with vkzg_b200.Server(max_blobs_per_batch=batch, lanes=lanes, hbm_budget_bytes=hbm_budget,
+                          table_budget_bytes=table_budget) as srv:
         setup_s = time.perf_counter() - t_setup
+        charges = srv.stats()
         # warm-up segment (not reported): the lanes capture the pipelines of the batch
         # sizes they meet, so the measured segments mostly replay captured graphs
         fractions = [args_warm] + list(fractions)
@@ -303,11 +322,11 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
                     if item is None:
                         return
                     statuses.append(srv.wait(item[0]))
-                    # every 40th request of every segment, up to 64, checked after the sweep
-                    # (copied out of the ring now that the request is complete)
-                    if len(statuses) % 40 == 1 and len(checks) < 64 and item[1] is not None:
-                        kind, first, n, out = item[1]
-                        checks.append((kind, first, n, out.copy()))
+                    kind, first, n, out = item[1]
+                    want = want_proofs if kind == "proofs" else want_cells
+                    if not np.array_equal(out.reshape(n, -1), want[first:first + n]):
+                        mismatches.append((kind, first, n))
+                    checked[0] += 1
 
             th = threading.Thread(target=waiter, daemon=True)
             th.start()
@@ -342,20 +361,20 @@ def serve_sweep(prover, h_blobs, h_cells, h_present, n_pool, capacity, fractions
                 continue
             results.append({"offered_blobs_per_s": round(offered, 1),
                             "served_blobs_per_s": round(st["blobs"] / st["seconds"], 1),
+                            "seconds": round(st["seconds"], 1),
                             "requests": int(st["requests"]), "blobs": int(st["blobs"]),
                             "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
-                            "p999_ms": round(st["p999_ms"], 3), "max_ms": round(st["max_ms"], 3)})
+                            "p999_ms": round(st["p999_ms"], 3), "max_ms": round(st["max_ms"], 3),
+                            "admission_deferrals": int(st["deferrals"]),
+                            "peak_in_flight_bytes": int(st["peak_in_flight_bytes"])})
     results = [r for r in results if r is not None]
-    # bit-exactness in the mix: sampled requests against direct calls on the same inputs
-    for kind, first, n, out in checks:
-        ref = np.empty_like(out)
-        if kind == "proofs":
-            assert prover.compute_proofs_raw(ref, h_blobs.data_ptr() + first * BLOB, n) == 0
-        else:
-            assert prover.recover_cells_raw(ref, h_cells.data_ptr() + first * EXT,
-                                            h_present.data_ptr() + first * 128, n) == 0
-        assert np.array_equal(ref, out), f"served {kind} request differs from a direct call"
-    return results, len(checks), setup_s
+    assert not mismatches, f"served requests differ from direct calls: {mismatches[:4]}"
+    info = {"setup_s": round(setup_s, 2), "hbm_budget_bytes": hbm_budget, "lanes": lanes, "max_blobs_per_batch": batch,
+            "resident_bytes": int(charges["resident_bytes"]),
+            "proof_bytes_per_blob": int(charges["proof_bytes_per_blob"]),
+            "recover_bytes_per_blob": int(charges["recover_bytes_per_blob"]),
+            "bit_exact_checked_requests": checked[0]}
+    return results, info
 
 
 def run_ours(args, rank, world, local_rank):
@@ -370,6 +389,10 @@ def run_ours(args, rank, world, local_rank):
     # the autotuner's decisions are shared with the serving lanes' provers through this file
     tune_dir = tempfile.mkdtemp(prefix="vkzg_tune_")
     os.environ["VKZG_TUNE_CACHE"] = os.path.join(tune_dir, "plans.txt")
+    # digit-table budget: opted in above the library's 20 GiB default, so the
+    # tuner may pick windows up to 13 bits (64.4 GB)
+    os.environ.setdefault("VKZG_COMB_BUDGET_GB", str(args.table_budget_gb))
+    table_budget = int(float(os.environ["VKZG_COMB_BUDGET_GB"]) * (1 << 30))
     prover = vkzg_b200.Prover(max_batch_size=n)
 
     blobs_np = make_blobs(n, 1234 + rank)
@@ -420,6 +443,78 @@ def run_ours(args, rank, world, local_rank):
     total_ms = replicas.max_over_ranks(sum(step_ms), dev)
     value = world * n * args.steps / (total_ms / 1e3)
     assert int(d_err.count_nonzero()) == 0
+
+    # ---- the timed outputs checked: every proof against a plan-0 pass (serial
+    # Jacobian buckets: an independent kernel path), a seeded sample of proofs
+    # and recovered blobs against the CPU oracle
+    got_proofs = d_proofs.cpu().numpy().reshape(n, PROOFS)
+    got_cells = d_out.cpu().numpy().reshape(n, EXT)
+    saved_plan = os.environ.get("VKZG_PLAN")
+    os.environ["VKZG_PLAN"] = "0"
+    with vkzg_b200.Prover(max_batch_size=n) as plain0:
+        plan0 = np.zeros(n * PROOFS, np.uint8)
+        assert plain0.compute_proofs_raw(plan0, blobs_np, n) == 0
+    if saved_plan is None:
+        del os.environ["VKZG_PLAN"]
+    else:
+        os.environ["VKZG_PLAN"] = saved_plan
+    assert np.array_equal(plan0.reshape(n, PROOFS), got_proofs), "timed proofs differ from the plan-0 pass"
+    verified = {"proofs_vs_plan0": n}
+    if not args.no_cpu:
+        from oracle import Oracle, build
+        build()
+        orc = Oracle()
+        with open(os.path.join(ROOT, "vkzg_b200", "data", "trusted_setup_g1_monomial.bin"), "rb") as f:
+            orc_tables = orc.tables_from_setup(f.read())
+        pick = np.random.default_rng(2024 + rank).choice(n, 4, replace=False)
+        pick_p = sorted(set(pick.tolist()) | {n - 4, n - 1})  # two of the adversarial blobs too
+        rc, want = orc.compute_proofs(orc_tables, np.ascontiguousarray(blobs_np[pick_p]))
+        assert rc == 0 and np.array_equal(want.reshape(-1, PROOFS), got_proofs[pick_p]), "proofs differ from the oracle"
+        pick_r = sorted(np.random.default_rng(4048 + rank).choice(n, 8, replace=False).tolist())
+        rc, want = orc.recover_cells(np.ascontiguousarray(cells_np[pick_r]), np.ascontiguousarray(present_np[pick_r]))
+        assert rc == 0 and np.array_equal(want.reshape(-1, EXT), got_cells[pick_r]), "recovery differs from the oracle"
+        verified.update({"proofs_vs_oracle": len(pick_p), "recovered_blobs_vs_oracle": len(pick_r)})
+
+    # ---- recovery of 16 blobs keeping exactly 64 of 128 cells,
+    # seeded uniform subsets; device-resident and through the C ABI (pinned buffers)
+    c1 = None
+    if n >= 16:
+        rng1 = np.random.default_rng(0x7594)
+        c1_present = np.zeros((16, 128), np.uint8)
+        for b in range(16):
+            c1_present[b, rng1.choice(128, 64, replace=False)] = 1
+        c1_cells = np.ascontiguousarray(cells_np[:16])
+        d_c1_cells = torch.from_numpy(c1_cells).to(dev)
+        d_c1_present = torch.from_numpy(c1_present).to(dev)
+        for _ in range(3):
+            prover.recover_cells_device(d_out.data_ptr(), d_c1_cells.data_ptr(), d_c1_present.data_ptr(),
+                                        d_err.data_ptr(), 16, sp)
+        c1_ms = []
+        for _ in range(20):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prover.recover_cells_device(d_out.data_ptr(), d_c1_cells.data_ptr(), d_c1_present.data_ptr(),
+                                        d_err.data_ptr(), 16, sp)
+            e1.record(stream)
+            e1.synchronize()
+            c1_ms.append(e0.elapsed_time(e1))
+        h_c1_cells = torch.from_numpy(c1_cells).pin_memory()
+        h_c1_present = torch.from_numpy(c1_present).pin_memory()
+        h_c1_out = torch.empty(16 * EXT, dtype=torch.uint8).pin_memory()
+        c1_e2e = []
+        for i in range(23):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            assert prover.recover_cells_raw(h_c1_out.data_ptr(), h_c1_cells.data_ptr(), h_c1_present.data_ptr(), 16) == 0
+            if i >= 3:
+                c1_e2e.append(time.perf_counter() - t0)
+        if not args.no_cpu:
+            rc, want = orc.recover_cells(c1_cells[:4], c1_present[:4])
+            assert rc == 0 and np.array_equal(want.reshape(-1), h_c1_out.numpy()[:4 * EXT]), "C1 differs from the oracle"
+        c1 = {"blobs": 16, "present_per_blob": 64, "device_blobs_per_s": 16 / (statistics.median(c1_ms) / 1e3),
+              "e2e_blobs_per_s": 16 / statistics.median(c1_e2e)}
 
     # ---- per-stage breakdown from untimed steps with stage events (the timed steps
     # above replay the captured pipeline; these launch it stage by stage)
@@ -493,26 +588,42 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the plain form (one call per blob) and the served form, one replica each
     plain = plain_rates(prover, h_blobs, h_cells, h_present, args.plain_sample) if not args.no_plain else None
-    serving, checked, serve_setup_s = None, 0, None
+    serving = None
     if args.serve_seconds > 0:
         capacity = 1.0 / (0.7 / e2e_proof_rate + 0.3 / e2e_rec_rate)
         fractions = [float(x) for x in args.serve_loads.split(",")]
-        serving, checked, serve_setup_s = serve_sweep(prover, h_blobs, h_cells, h_present, n, capacity, fractions,
-                                                      args.serve_seconds, batch=args.serve_batch,
-                                                      lanes=args.serve_lanes)
+        want_cells = np.frombuffer(prover.recover_cells_batch(cells_np.tobytes(), present_np.tobytes(), n),
+                                   np.uint8).reshape(n, EXT)
+        sweep, info = serve_sweep(got_proofs, want_cells, h_blobs, h_cells, h_present, n, capacity, fractions,
+                                  args.serve_seconds, batch=args.serve_batch, lanes=args.serve_lanes,
+                                  hbm_budget=64 << 30, table_budget=table_budget)
+        serving = {"sweep": sweep, **info, "seconds_per_load": args.serve_seconds, "outputs": "reused pinned rings",
+                   "mix": "Poisson arrivals; 1-64 blobs per request (geometric, mean 6); 70% proofs, "
+                          "30% recovery with 64-127 cells present"}
+        if args.c4_seconds > 0:
+            # BASELINE config 4 as stated: 60 s at the top offered load with the
+            # admission budget at 8 GiB of working set, which binds (3 lanes x 128
+            # blobs of proof work in flight would need more)
+            top = [max(fractions)]
+            c4, c4_info = serve_sweep(got_proofs, want_cells, h_blobs, h_cells, h_present, n, capacity, top,
+                                      args.c4_seconds, seed=4242, batch=args.serve_batch, lanes=args.serve_lanes,
+                                      hbm_budget=8 << 30, table_budget=table_budget)
+            serving["c4_8gib_budget"] = {**c4[0], **c4_info, "seconds_per_load": args.c4_seconds}
     replicas.barrier(dev)
     if rank != 0:
         return
 
     # ---- roofline of the dominant kernel (phase A), integer-multiply bound
     imad_peak = vkzg_b200.microbench(0)
+    product_rate = vkzg_b200.microbench(4)  # this library's Fp product alone, G/s
     pa_ms = statistics.mean(phase_a_ms)
-    achieved = PHASE_A_FP_MUL_PER_BLOB * IMAD_FP * n / (pa_ms / 1e3) / 1e12
+    reference_work = PHASE_A_FP_MUL_PER_BLOB * IMAD_FP * n / (pa_ms / 1e3) / 1e12
     digit = prover.digit_table()
     plan = tuning.get(n, (None,))[0] if n in tuning else None
-    executed = None
+    executed = products = None
     if plan == 3 and digit:
         executed = 128 * phase_a_executed_imad_per_output(digit[0]) * n / (pa_ms / 1e3) / 1e12
+        products = 128 * phase_a_executed_products_per_output(digit[0]) * n / (pa_ms / 1e3) / 1e9
     stages = dict(stages_acc)
     p_ms = statistics.mean(proof_ms)
     rec_ms = statistics.mean(step_ms) - p_ms
@@ -550,28 +661,33 @@ def run_ours(args, rank, world, local_rank):
         "next_rows": next_rows,
         "plain_per_blob": plain,
         "batched_over_plain": (e2e_value / world) / plain["value"] if plain else None,
-        "serving": {"sweep": serving, "lanes": args.serve_lanes, "max_blobs_per_batch": args.serve_batch,
-                    "hbm_budget_bytes": 8 << 30, "outputs": "reused pinned rings",
-                    "setup_s": round(serve_setup_s, 2),
-                    "seconds_per_load": args.serve_seconds, "bit_exact_checked_requests": checked,
-                    "mix": "Poisson arrivals; 1-64 blobs per request (geometric, mean 6); 70% proofs, "
-                           "30% recovery with 64-127 cells present"} if serving else None,
+        "serving": serving,
         "roofline": {"kernel": "phase A (plan %s: %s)" % (plan, "k_flat_* rounds over the digit table" if plan == 3
                                                             else "k_phase_a_affine + k_reduce_hier"),
-                     "bound": "int", "achieved": achieved, "peak": imad_peak,
-                     "unit": "TIMAD/s", "frac": achieved / imad_peak,
-                     "frac_executed": executed / imad_peak if executed else None,
-                     "peak_source": "measured in-process (vkzg_b200_microbench IMAD probe); "
-                                    f"nominal 148 SM x 64/clk x 1.965 GHz = {NOMINAL_IMAD_TPS:.1f}",
-                     "algorithmic": f"{PHASE_A_FP_MUL_PER_BLOB:.3g} Fp mul x 576 IMAD per blob x {n} blobs: the "
-                                    "reference algorithm's phase-A work (madd-2007-bl bucket accumulation); "
-                                    "frac above 1 = fewer operations than the reference, frac_executed = the "
-                                    "multiply instructions this kernel executes (516 per Fp product, 426 per "
-                                    "square)",
-                     "traffic": PHASE_A_DRAM_BYTES_PER_BLOB_PLAN3 * n if plan == 3 and digit and digit[0] == 13
-                     else None,
-                     "traffic_unit": "bytes per phase-A pass over the batch (ncu dram__bytes_read + write)"},
-        "digit_table": {"window_bits": digit[0], "build_ms": round(digit[1], 1), "bytes": digit[2]} if digit else None,
+                     "bound": "int", "achieved": executed, "peak": imad_peak, "unit": "TIMAD/s",
+                     "frac": executed / imad_peak if executed else None,
+                     "peak_source": "measured in-process (vkzg_b200_microbench(0): mad.lo.u32 issue rate; "
+                                    "MEASURED_PEAKS.json has no integer figure); nominal 148 SM x 64/clk x "
+                                    f"1.965 GHz = {NOMINAL_IMAD_TPS:.1f}",
+                     "algorithmic": "multiply instructions phase A executes: per MSM output 64 ceil(256/c) - 1 "
+                                    "digit-table points summed by affine additions (5 products + 1 square, "
+                                    "516 / 426 multiply instructions each) down to lists of 10, then mixed "
+                                    "Jacobian additions",
+                     "products_g_per_s": products, "product_rate_alone_g_per_s": product_rate,
+                     "frac_of_product_rate": products / product_rate if products else None,
+                     "reference_algorithm_tera_imad_per_s": reference_work,
+                     "work_saved": reference_work / executed if executed else None,
+                     "traffic": PHASE_A_DRAM_BYTES_PER_BLOB[digit[0]] * n
+                     if plan == 3 and digit and digit[0] in PHASE_A_DRAM_BYTES_PER_BLOB else None,
+                     "traffic_unit": "DRAM bytes per phase-A pass over the batch (ncu dram__bytes_read + write "
+                                     "of a 16-blob capture per kernel, scaled by blobs)"},
+        "digit_table": {"window_bits": digit[0], "build_ms": round(digit[1], 1), "bytes": digit[2],
+                        "budget_bytes": table_budget,
+                        "window_trials": [{"window_bits": c, "bytes": b, "build_ms": round(bm, 1), "proof_ms": round(t, 3)}
+                                          for c, b, bm, t in prover.window_trials(n)]} if digit else None,
+        "device_bytes": prover.device_bytes(),
+        "verified": verified,
+        "c1_recovery_16_blobs": c1,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
         "gpu_launches": launches,
@@ -591,13 +707,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the cells / cells+proofs / recovered+proofs rates")
-    ap.add_argument("--profile-case", nargs="?", const="proofs", choices=["proofs", "recovery"],
+    ap.add_argument("--profile-case", nargs="?", const="proofs", choices=["proofs", "recovery", "cells"],
                     help="small untimed case for ncu captures")
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="per offered load; 0 skips serving")
     ap.add_argument("--serve-loads", default="0.3,0.6,0.9", help="offered loads as fractions of batched capacity")
     ap.add_argument("--serve-batch", type=int, default=128, help="the server's max_blobs_per_batch")
     ap.add_argument("--serve-lanes", type=int, default=3, help="the server's lanes")
+    ap.add_argument("--c4-seconds", type=float, default=60.0,
+                    help="BASELINE config 4 at the top load with an 8 GiB budget; 0 skips it")
+    ap.add_argument("--table-budget-gb", type=float, default=100.0,
+                    help="digit-table budget (GiB) unless $VKZG_COMB_BUDGET_GB is set")
     args = ap.parse_args()
 
     if args.profile_case:
@@ -611,6 +731,11 @@ def main():
             out = np.zeros(args.blobs * PROOFS, np.uint8)
             for _ in range(args.steps):
                 assert prover.compute_proofs_raw(out, blobs, args.blobs) == 0
+        elif args.profile_case == "cells":
+            blobs = make_blobs(args.blobs, 5, adversarial=False)
+            out = np.zeros(args.blobs * EXT, np.uint8)
+            for _ in range(args.steps):
+                assert prover.compute_cells_raw(out, blobs, args.blobs) == 0
         else:
             cells, present = make_recovery(args.blobs, 6)
             out = np.zeros(args.blobs * EXT, np.uint8)

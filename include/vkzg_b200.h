@@ -119,11 +119,28 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * where a plan was not timed) and returns how many classes are tuned.
  * vkzg_b200_digit_table returns the digit table's window c (0 = none built),
  * its build time and size.
+ *
+ * Plan 3's digit table holds m 2^(c k) X[j][i] for every window k of c bits:
+ * 128 x 64 x ceil(256/c) x 2^(c-1) points of 96 bytes (c = 8: 3.2 GB, 10: 10.5,
+ * 11: 19.3, 12: 35.4, 13: 64.4, 14: 122 GB); wider windows mean fewer
+ * additions per output (64 ceil(256/c) - 1).  Its size is bounded by a budget:
+ * $VKZG_COMB_BUDGET_GB (GiB, default 20, so c <= 11 unless raised); a serving
+ * loop uses its table_budget_bytes.  When plan 3 is tuned, the widest window
+ * that fits the budget and the two below it are each built and timed, and the
+ * fastest is kept (and remembered in $VKZG_TUNE_CACHE); $VKZG_COMB_BITS pins
+ * the window (0: no digit table).  vkzg_b200_window_trials reports those
+ * trials for a size class (window, table bytes, build ms, proof-chunk ms) and
+ * returns their count.  vkzg_b200_prover_device_bytes reports the device
+ * memory a prover holds: its working set, its setup tables, and the digit
+ * table it uses (shared by all provers of the process with the same setup).
  */
 #define VKZG_B200_PLANS 5
 vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms, int cap);
 int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes);
+int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *window_bits, uint64_t *table_bytes,
+                            double *build_ms, double *ms, int cap);
+void vkzg_b200_prover_device_bytes(const vkzg_prover *p, uint64_t *working, uint64_t *tables, uint64_t *digit_table);
 
 /*
  * Number of CUDA kernels this library has launched in this process (proof,
@@ -146,7 +163,13 @@ uint64_t vkzg_b200_kernel_launches(void);
  * the next batch.  A batch is admitted only while the device working set of
  * all batches in flight stays within hbm_budget_bytes (a batch is always admitted
  * when none is in flight, so a budget below one batch serialises batches; the
- * dispatcher sleeps until a batch completes).  Each blob is computed
+ * dispatcher sleeps until a batch completes).  A batch is charged its blobs
+ * times the device working set per blob that the lanes hold (measured from
+ * their allocations at creation: a lane prover's working set over its
+ * capacity, plus the lane's I/O buffers); the setup tables and the shared
+ * digit table are resident and reported apart (resident_bytes).  The lanes'
+ * digit table is bounded by table_budget_bytes (0 = 20 GiB).  Stats also count
+ * the batches admission deferred and the peak in-flight charge.  Each blob is computed
  * independently, so a request's output is the same alone and in any mix.
  * vkzg_b200_server_new tunes the proof plan of every batch size class up to
  * max_blobs_per_batch on one lane and gives the choices to all lanes, so that
@@ -164,10 +187,15 @@ typedef struct {
     uint32_t max_blobs_per_batch; /* 0 = 128 */
     uint32_t lanes;               /* concurrent device batches; 0 = 3 */
     uint64_t hbm_budget_bytes;    /* admission cap on the in-flight working set; 0 = 8 GiB */
+    uint64_t table_budget_bytes;  /* cap on the lanes' digit table; 0 = 20 GiB */
 } vkzg_server_options;
 typedef struct {
     uint64_t requests, blobs;
     double p50_ms, p99_ms, p999_ms, mean_ms, max_ms, seconds;
+    uint64_t deferrals;            /* times admission held a batch back for the budget */
+    uint64_t peak_in_flight_bytes; /* largest in-flight charge */
+    uint64_t resident_bytes;       /* setup tables of the lanes + the shared digit table */
+    uint64_t proof_bytes_per_blob, recover_bytes_per_blob; /* admission charges */
 } vkzg_server_stats;
 void vkzg_b200_server_options_default(vkzg_server_options *opts);
 vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *opts);

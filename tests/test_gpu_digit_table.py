@@ -9,7 +9,7 @@ from conftest import adversarial_blobs, random_blobs
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("bits", [10, 11])
+@pytest.mark.parametrize("bits", [8, 9, 10, 11])
 def test_plan3_mainnet_vectors(golden_proofs, monkeypatch, bits):
     """Every valid vector, batched, with the window forced to `bits`."""
     monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
@@ -37,7 +37,7 @@ def test_plan3_synthetic_vs_oracle(synthetic, oracle, tmp_path, monkeypatch):
     with vkzg_b200.Prover(max_batch_size=len(blobs)) as p:
         assert p.compute_proofs_raw(out, blobs, len(blobs)) == 0
         c, build_ms, nbytes = p.digit_table()
-        assert 10 <= c <= 13 and nbytes > 0
+        assert 9 <= c <= 11 and 0 < nbytes <= 20 << 30  # the default budget
     rc, want = oracle.compute_proofs(tables, blobs)
     assert rc == 0
     for b in range(len(blobs)):
@@ -82,3 +82,51 @@ def test_plan3_without_digit_table_falls_back(golden_proofs, monkeypatch):
         out = p.compute_cell_kzg_proofs_batch(golden_proofs["valid_blobs"].tobytes(), n)
         assert p.digit_table() is None
     assert out == golden_proofs["valid_proofs"].tobytes()
+
+
+def comb_bytes(c):
+    return 128 * 64 * -(-256 // c) * (1 << (c - 1)) * 96
+
+
+def test_tuner_times_windows_within_budget(monkeypatch):
+    """With a 12 GiB budget the tuner builds and times windows 10, 9 and 8 (the
+    widest that fits and the two below), keeps the fastest, and reports each
+    trial's table size; the proofs equal those of plan 0."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.delenv("VKZG_PLAN", raising=False)
+    monkeypatch.delenv("VKZG_COMB_BITS", raising=False)
+    monkeypatch.setenv("VKZG_COMB_BUDGET_GB", "12")
+    blobs = random_blobs(32, 505)
+    with vkzg_b200.Prover(max_batch_size=32) as p:
+        table = p.autotune(32)  # largest size class first: the window is chosen at 32 blobs
+        trials = p.window_trials(32)
+        assert [t[0] for t in trials] == [10, 9, 8]
+        for c, nbytes, build_ms, ms in trials:
+            assert nbytes == comb_bytes(c) and build_ms > 0 and ms > 0
+        best = min(trials, key=lambda t: t[3])
+        assert p.digit_table()[0] == best[0]
+        assert abs(table[32][1][3] - best[3]) < 1e-9
+        assert [t[0] for t in p.window_trials(16)] == [best[0]]  # smaller classes keep it
+        out = np.zeros(32 * 6144, np.uint8)
+        assert p.compute_proofs_raw(out, blobs, 32) == 0
+        mem = p.device_bytes()
+        assert mem["digit_table"] == comb_bytes(best[0]) <= 12 << 30
+    monkeypatch.setenv("VKZG_PLAN", "0")
+    with vkzg_b200.Prover(max_batch_size=32) as q:
+        want = np.zeros(32 * 6144, np.uint8)
+        assert q.compute_proofs_raw(want, blobs, 32) == 0
+    assert np.array_equal(out, want)
+
+
+def test_default_prover_is_small(monkeypatch):
+    """A prover with the default options batches 4 blobs per launch, as the
+    reference's does, and holds well under 8 GB of device memory."""
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    with vkzg_b200.Prover() as p:
+        mem = p.device_bytes()
+        assert mem["digit_table"] == 0
+        assert mem["working"] + mem["tables"] < 1 << 30
+        blobs = random_blobs(9, 606)  # three chunks of 4, 4 and 1
+        out = np.zeros(9 * 6144, np.uint8)
+        assert p.compute_proofs_raw(out, blobs, 9) == 0
+        assert p.device_bytes()["digit_table"] == 0

@@ -106,7 +106,36 @@ def test_server_one_byte_budget_still_serves_every_request(golden_proofs, golden
         for t, out, want in jobs:
             assert s.wait(t) == vkzg_b200.OK
             assert np.array_equal(out, want)
-        assert s.stats()["requests"] == len(jobs)
+        st = s.stats()
+        assert st["requests"] == len(jobs)
+        assert st["proof_bytes_per_blob"] > st["recover_bytes_per_blob"] > 0
+        assert st["resident_bytes"] > 0
+
+
+def test_server_budget_binding_partway(golden_proofs):
+    """A budget of one and a half full proof batches: a second batch is admitted
+    only while the first is small enough; the dispatcher defers the rest, the
+    in-flight charge never exceeds the budget once something is in flight, and
+    every request completes with the right bytes."""
+    from conftest import random_blobs
+    blobs = random_blobs(16, 717)
+    with vkzg_b200.Prover(max_batch_size=16) as p:
+        want = np.frombuffer(p.compute_cell_kzg_proofs_batch(blobs.tobytes(), 16), np.uint8)
+    with vkzg_b200.Server(max_blobs_per_batch=8, lanes=3) as probe:
+        per_blob = probe.stats()["proof_bytes_per_blob"]
+    budget = int(per_blob * 8 * 1.5)
+    with vkzg_b200.Server(max_blobs_per_batch=8, lanes=3, hbm_budget_bytes=budget) as s:
+        jobs = []
+        for k in range(24):
+            out = np.zeros(16 * 6144, np.uint8)
+            jobs.append((s.submit_proofs(out, blobs, 16), out))
+        for t, out in jobs:
+            assert s.wait(t) == vkzg_b200.OK
+            assert np.array_equal(out, want)
+        st = s.stats()
+        assert st["requests"] == 24
+        assert st["deferrals"] > 0
+        assert st["peak_in_flight_bytes"] <= budget
 
 
 def test_server_wait_timeout_keeps_ticket(golden_proofs):

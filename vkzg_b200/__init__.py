@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_server_options_default", "vkzg_b200_server_new", "vkzg_b200_server_free",
     "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
     "vkzg_b200_server_stats", "vkzg_b200_kernel_launches", "vkzg_b200_digit_table",
-    "vkzg_b200_tree_sums_selftest",
+    "vkzg_b200_tree_sums_selftest", "vkzg_b200_window_trials", "vkzg_b200_prover_device_bytes",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -61,13 +61,15 @@ class _Options(ctypes.Structure):
 
 class _ServerOptions(ctypes.Structure):
     _fields_ = [("max_blobs_per_batch", ctypes.c_uint32), ("lanes", ctypes.c_uint32),
-                ("hbm_budget_bytes", ctypes.c_uint64)]
+                ("hbm_budget_bytes", ctypes.c_uint64), ("table_budget_bytes", ctypes.c_uint64)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("requests", ctypes.c_uint64), ("blobs", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
                 ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
-                ("max_ms", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("max_ms", ctypes.c_double), ("seconds", ctypes.c_double), ("deferrals", ctypes.c_uint64),
+                ("peak_in_flight_bytes", ctypes.c_uint64), ("resident_bytes", ctypes.c_uint64),
+                ("proof_bytes_per_blob", ctypes.c_uint64), ("recover_bytes_per_blob", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -152,6 +154,11 @@ def library():
             L.vkzg_b200_tree_sums_selftest.restype = ctypes.c_int
             L.vkzg_b200_digit_table.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]
             L.vkzg_b200_digit_table.restype = ctypes.c_int
+            L.vkzg_b200_window_trials.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, ctypes.c_int]
+            L.vkzg_b200_window_trials.restype = ctypes.c_int
+            L.vkzg_b200_prover_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
+                                                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+            L.vkzg_b200_prover_device_bytes.restype = None
             L.vkzg_b200_kernel_launches.argtypes = []
             L.vkzg_b200_kernel_launches.restype = ctypes.c_uint64
             _lib = L
@@ -332,6 +339,23 @@ class Prover:
         c = self._lib.vkzg_b200_digit_table(self._h, ctypes.byref(ms), ctypes.byref(nb))
         return (c, ms.value, nb.value) if c else None
 
+    def window_trials(self, size_class):
+        """The digit-table windows the tuner timed for a size class:
+        [(window bits c, table bytes, build ms, proof-chunk ms), ...]."""
+        cap = 8
+        c = (ctypes.c_int * cap)()
+        nb = (ctypes.c_uint64 * cap)()
+        bms = (ctypes.c_double * cap)()
+        ms = (ctypes.c_double * cap)()
+        n = self._lib.vkzg_b200_window_trials(self._h, int(size_class), c, nb, bms, ms, cap)
+        return [(int(c[i]), int(nb[i]), bms[i], ms[i]) for i in range(min(n, cap))]
+
+    def device_bytes(self):
+        """{'working', 'tables', 'digit_table'}: device memory this prover holds."""
+        w, t, d = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._lib.vkzg_b200_prover_device_bytes(self._h, ctypes.byref(w), ctypes.byref(t), ctypes.byref(d))
+        return {"working": w.value, "tables": t.value, "digit_table": d.value}
+
     def set_stage_timing(self, enabled):
         self._lib.vkzg_b200_set_stage_timing(self._h, 1 if enabled else 0)
 
@@ -346,11 +370,12 @@ class Server:
     submit_* must stay alive until wait() returns for their ticket; numpy arrays
     or raw addresses are accepted."""
 
-    def __init__(self, max_blobs_per_batch=0, lanes=0, hbm_budget_bytes=0):
+    def __init__(self, max_blobs_per_batch=0, lanes=0, hbm_budget_bytes=0, table_budget_bytes=0):
         L = library()
         o = _ServerOptions()
         L.vkzg_b200_server_options_default(ctypes.byref(o))
         o.max_blobs_per_batch, o.lanes, o.hbm_budget_bytes = max_blobs_per_batch, lanes, hbm_budget_bytes
+        o.table_budget_bytes = table_budget_bytes
         h = ctypes.c_void_p()
         _check(L.vkzg_b200_server_new(ctypes.byref(h), ctypes.byref(o)))
         self._h, self._lib = h, L

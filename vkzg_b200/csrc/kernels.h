@@ -171,6 +171,9 @@ cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, c
 // Writes t.pos; needs `scratch` of at least setup_scratch_bytes().
 size_t setup_scratch_bytes();
 size_t comb_build_scratch_bytes(int c);
+// Window widths of the digit table: 8 bits (32 windows, 3.2 GB) to 14 bits
+// (19 windows, 122 GB).
+constexpr int kCombMinBits = 8, kCombMaxBits = 14;
 struct FlatSizes {
     int blocks = 0;
     size_t lanes = 0, dig = 0, buf0 = 0, buf1 = 0, slots = 0, pre_words = 0;
@@ -186,6 +189,8 @@ cudaError_t configure_kernels();
 struct vkzg_prover;
 namespace vkzg {
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src);
+// digit-table byte budget of a prover (before its first tuning)
+void set_comb_budget(vkzg_prover *p, uint64_t bytes);
 void precapture_graphs(vkzg_prover *p, uint32_t max_n);
 
 // process-wide count of kernels launched by the launchers above

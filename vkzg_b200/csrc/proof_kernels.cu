@@ -623,7 +623,7 @@ __device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, uint32_t o, uint32_
 // contiguous run of 16-byte stores (a thread's own digits are D x 2 bytes apart
 // from its neighbour's: direct stores would scatter).  n_scalars is a multiple
 // of 128 (64 scalars per list, 128 lists per blob).
-constexpr int kDigitMaxWindows = 26; // c >= 10
+constexpr int kDigitMaxWindows = (256 + kCombMinBits - 1) / kCombMinBits;
 __global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, int c, int D,
                                                     int n_scalars) {
     __shared__ __align__(16) int16_t sd[128 * kDigitMaxWindows];

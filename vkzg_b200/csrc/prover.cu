@@ -22,6 +22,7 @@
 #include <atomic>
 #include <chrono>
 #include <map>
+#include <thread>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -105,6 +106,20 @@ struct vkzg_prover {
     std::string tables_id;            // identity of the setup tables, for sharing the digit table
     std::shared_ptr<CombTable> comb;  // plan 3's digit table, once built
     bool comb_failed = false, flat_failed = false;
+    // device memory: everything this prover allocated (tables_bytes of it the
+    // setup tables); the shared digit table is counted apart, in comb->bytes
+    uint64_t dev_bytes = 0, tables_bytes = 0;
+    // digit table: byte budget ($VKZG_COMB_BUDGET_GB, default 20 GiB; a serving
+    // loop passes its own), the window the tuner chose (0 = not yet), and the
+    // window the phase-A round buffers are sized for (they serve any wider one)
+    uint64_t comb_budget = 20ull << 30;
+    int comb_c_chosen = 0, comb_buf_c = 0;
+    struct WindowTrial {
+        int c;
+        uint64_t bytes;
+        double build_ms, ms;
+    };
+    std::map<uint32_t, std::vector<WindowTrial>> window_trials; // per tuned size class
     // CUDA graphs of the proof pipeline per (chunk size, plan), see run_proofs
     struct GraphRec {
         cudaGraphExec_t exec = nullptr;
@@ -126,9 +141,22 @@ struct vkzg_prover {
     cudaEvent_t side_ev[kSides + 1] = {};
     std::string tune_cache;
     cudaEvent_t ev_tune[2] = {nullptr, nullptr};
+    // Pinned staging for callers' pageable host buffers (allocated on the first
+    // call that passes one, cap x 256 KB each way).  A pageable buffer is copied
+    // by host threads into (or out of) it slice by slice, so that those copies,
+    // the DMA on the side streams and the kernels of other slices overlap; the
+    // driver's own staging of pageable copies runs one copy at a time
+    // (measured: 13 k recovery blobs/s at 256 blobs from pageable buffers).
+    static constexpr int kStageSlices = 8;
+    uint8_t *stage_in = nullptr, *stage_out = nullptr;
+    size_t stage_bytes = 0;
 
     ~vkzg_prover() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto &x : side)
+            if (x) cudaStreamSynchronize(x);
+        if (stage_in) cudaFreeHost(stage_in);
+        if (stage_out) cudaFreeHost(stage_out);
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.exec);
         for (auto &x : side)
             if (x) cudaStreamDestroy(x);
@@ -151,6 +179,7 @@ struct vkzg_prover {
         void *p = nullptr;
         if (cudaMalloc(&p, count * sizeof(T) + 16) != cudaSuccess) return false;
         allocs.push_back(p);
+        dev_bytes += count * sizeof(T) + 16;
         ptr = reinterpret_cast<T *>(p);
         return true;
     }
@@ -602,7 +631,12 @@ vkzg_result alloc_working_set(vkzg_prover *p, uint32_t cap) {
     if (const char *cache = getenv("VKZG_TUNE_CACHE")) p->tune_cache = cache;
     if (const char *g = getenv("VKZG_GRAPHS")) p->use_graphs = atoi(g) != 0;
     load_tune_cache(p);
-    w.ba_blocks = (int)p->sm_count * batch_affine_blocks_per_sm();
+    // persistent grid of the batch-affine kernels: a block per resident slot,
+    // but no more than the capacity's tasks (kWarpOutputs outputs per warp) fill
+    const int warps_per_block = VKZG_BA_THREADS / 32;
+    const int tasks = (int)((B * kCells + kWarpOutputs - 1) / kWarpOutputs);
+    w.ba_blocks = std::min((int)p->sm_count * batch_affine_blocks_per_sm(),
+                           (tasks + warps_per_block - 1) / warps_per_block);
     if (!p->alloc(w.bucket_aff, B * kCells * kBuckets) ||
         !p->alloc(w.ba_scratch, (size_t)w.ba_blocks * kBAScratchPoints) ||
         !p->alloc(w.red_scratch, reduce_scratch_points((int)B)) || !p->alloc(w.task_ctr, 2))
@@ -721,7 +755,10 @@ vkzg_result vkzg_prover_new(vkzg_prover **out, const vkzg_options *opts) {
             rc = VKZG_ERR_SETUP;
         }
     }
-    if (rc == VKZG_OK) rc = alloc_working_set(p, opts && opts->max_batch_size ? opts->max_batch_size : 256);
+    p->tables_bytes = p->dev_bytes;
+    if (const char *e = getenv("VKZG_COMB_BUDGET_GB")) p->comb_budget = (uint64_t)(atof(e) * (double)(1ull << 30));
+    // 0 = the reference's default of 4 blobs per launch (src/vkzg.cpp:699)
+    if (rc == VKZG_OK) rc = alloc_working_set(p, opts && opts->max_batch_size ? opts->max_batch_size : 4);
     if (rc == VKZG_OK && cudaStreamSynchronize(p->stream) != cudaSuccess) rc = VKZG_ERR_GPU;
     if (rc != VKZG_OK) {
         delete p;
@@ -821,15 +858,21 @@ constexpr uint32_t kCombMinBlobs = 16; // smaller chunks never pay for the digit
 // ------------------------------------------------------------ digit table
 std::mutex g_comb_mu;
 std::map<std::string, std::weak_ptr<CombTable>> g_comb;
+// the window a tuner chose, per device, setup tables and budget: later provers
+// of the process with the same budget take it (and so share the table)
+std::map<std::string, int> g_comb_choice;
+std::string comb_choice_key(const vkzg_prover *p) {
+    return std::to_string(p->device) + "|" + p->tables_id + "|" + std::to_string(p->comb_budget);
+}
 
-// Window width of the digit table: $VKZG_COMB_BITS (0 disables it; else 10..14),
-// default 13 (64.4 GB: 1279 additions per output; 12 bits take 35.4 GB and 1407).
-int comb_bits_wanted() {
+// $VKZG_COMB_BITS pins the digit table's window (0 disables the table; else
+// 8..14); -1 when unset.
+int comb_bits_forced() {
     if (const char *e = getenv("VKZG_COMB_BITS")) {
         const int c = atoi(e);
-        return c <= 0 ? 0 : std::min(14, std::max(10, c));
+        return c <= 0 ? 0 : std::min(kCombMaxBits, std::max(kCombMinBits, c));
     }
-    return 13;
+    return -1;
 }
 
 size_t comb_bytes(int c) {
@@ -844,7 +887,7 @@ bool ensure_flat_b(vkzg_prover *p) {
     if (w.flat_pre) return true;
     // (chunks beyond 4096 blobs would overflow the rounds' 32-bit pair indices)
     if (p->flat_failed || p->t.fb_rounds == 0 || p->cap > 4096) return false;
-    const FlatSizes z = flat_sizes((int)p->cap, 10); // its slots cover every window and phase B
+    const FlatSizes z = flat_sizes((int)p->cap, kCombMinBits); // its slots cover every window and phase B
     if (!p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
         !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
         !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
@@ -860,26 +903,63 @@ bool ensure_flat_b(vkzg_prover *p) {
     return true;
 }
 
-// Builds or shares the digit table; the window shrinks (down to 10 bits) until
-// the table fits in free device memory with 4 GB to spare.
-bool ensure_comb(vkzg_prover *p) {
-    if (p->comb) return true;
-    if (p->comb_failed) return false;
-    int c = comb_bits_wanted();
+// Windows the tuner tries, widest first: the widest whose table fits the
+// prover's budget and the two below it (8..14 bits; each bit less halves the
+// table and adds ~5 % to phase A's additions), or the pinned or chosen one.
+std::vector<int> comb_candidates(const vkzg_prover *p) {
+    const int forced = comb_bits_forced();
+    if (forced == 0) return {};
+    if (forced > 0) return {forced};
+    if (p->comb_c_chosen) return {p->comb_c_chosen};
+    {
+        std::lock_guard<std::mutex> lk(g_comb_mu);
+        auto it = g_comb_choice.find(comb_choice_key(p));
+        if (it != g_comb_choice.end()) return {it->second};
+    }
+    std::vector<int> out;
+    for (int c = kCombMaxBits; c >= kCombMinBits && out.size() < 3; c--)
+        if (comb_bytes(c) <= p->comb_budget) out.push_back(c);
+    return out;
+}
+
+// This prover's phase-A round buffers, sized for window c_min (narrower
+// windows mean longer lists): they then serve every window >= c_min.
+bool comb_buffers(vkzg_prover *p, int c_min) {
+    if (p->comb_buf_c) return c_min >= p->comb_buf_c;
+    const FlatSizes z = flat_sizes((int)p->cap, c_min);
+    ProofWork &w = p->pw;
+    if (!ensure_flat_b(p) || !p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) ||
+        !p->alloc(w.flat_buf[1], z.buf1)) {
+        cudaGetLastError();
+        w.flat_dig = nullptr;
+        return false;
+    }
+    p->comb_buf_c = c_min;
+    return true;
+}
+
+void drop_comb(vkzg_prover *p) {
+    p->comb.reset();
+    p->pw.comb = nullptr;
+    p->pw.comb_c = 0;
+}
+
+// Shares or builds the digit table of window c (a new one only when it fits in
+// free device memory with 4 GB to spare); the prover's previous table, if
+// another, is released first.
+bool use_comb(vkzg_prover *p, int c) {
+    if (p->comb && p->comb->c == c) return true;
+    drop_comb(p);
+    if (!comb_buffers(p, c)) return false;
     std::lock_guard<std::mutex> lk(g_comb_mu);
-    for (; c >= 10 && !p->comb; c--) {
-        const std::string key = std::to_string(p->device) + "|" + std::to_string(c) + "|" + p->tables_id;
-        auto it = g_comb.find(key);
-        if (it != g_comb.end()) {
-            if (auto sp = it->second.lock()) {
-                p->comb = sp;
-                break;
-            }
-        }
+    const std::string key = std::to_string(p->device) + "|" + std::to_string(c) + "|" + p->tables_id;
+    auto it = g_comb.find(key);
+    if (it != g_comb.end()) p->comb = it->second.lock();
+    if (!p->comb) {
         size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) break;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
         const size_t bytes = comb_bytes(c);
-        if (free_b < bytes + comb_build_scratch_bytes(c) + (4ull << 30)) continue;
+        if (free_b < bytes + comb_build_scratch_bytes(c) + (4ull << 30)) return false;
         auto t = std::make_shared<CombTable>();
         t->device = p->device;
         t->c = c;
@@ -887,40 +967,38 @@ bool ensure_comb(vkzg_prover *p) {
         if (cudaMalloc(&t->d, bytes) != cudaSuccess) {
             t->d = nullptr;
             cudaGetLastError();
-            continue;
+            return false;
         }
         void *scratch = nullptr;
         if (cudaMalloc(&scratch, comb_build_scratch_bytes(c)) != cudaSuccess) {
             cudaGetLastError();
-            break;
+            return false;
         }
         const auto t0 = std::chrono::steady_clock::now();
         cudaError_t e = launch_comb_table(p->t, t->d, scratch, c, p->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
         cudaFree(scratch);
-        if (e != cudaSuccess) break;
+        if (e != cudaSuccess) return false;
         t->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         g_comb[key] = t;
         p->comb = t;
     }
-    if (!p->comb) {
-        p->comb_failed = true;
-        return false;
-    }
-    // this prover's working set for the grid-wide phase-A rounds
-    const FlatSizes z = flat_sizes((int)p->cap, p->comb->c);
-    ProofWork &w = p->pw;
-    if (!ensure_flat_b(p) || !p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) ||
-        !p->alloc(w.flat_buf[1], z.buf1)) {
-        cudaGetLastError();
-        w.flat_dig = nullptr;
-        p->comb.reset();
-        p->comb_failed = true;
-        return false;
-    }
-    w.comb = p->comb->d;
-    w.comb_c = p->comb->c;
+    p->pw.comb = p->comb->d;
+    p->pw.comb_c = p->comb->c;
     return true;
+}
+
+// The digit table of the chosen window, or of the widest candidate that can be
+// had (plan 3 outside the tuner: device-pointer calls, adopted tuning).
+bool ensure_comb(vkzg_prover *p) {
+    if (p->comb) return true;
+    if (p->comb_failed) return false;
+    const std::vector<int> cands = comb_candidates(p);
+    if (!cands.empty() && comb_buffers(p, cands.back()))
+        for (int c : cands)
+            if (use_comb(p, c)) return true;
+    p->comb_failed = true;
+    return false;
 }
 
 uint32_t size_class(uint32_t n) {
@@ -934,6 +1012,7 @@ void save_tune_cache(const vkzg_prover *p) {
     FILE *f = fopen(p->tune_cache.c_str(), "w");
     if (!f) return;
     for (const auto &kv : p->plan_of) fprintf(f, "%s|%u|%u %d\n", p->name.c_str(), p->sm_count, kv.first, kv.second);
+    if (p->comb_c_chosen) fprintf(f, "%s|%u|window %d\n", p->name.c_str(), p->sm_count, p->comb_c_chosen);
     fclose(f);
 }
 
@@ -947,8 +1026,11 @@ void load_tune_cache(vkzg_prover *p) {
         std::string l(line);
         if (l.compare(0, key.size(), key) != 0) continue;
         unsigned c = 0;
-        int plan = -1;
+        int plan = -1, window = 0;
         if (sscanf(l.c_str() + key.size(), "%u %d", &c, &plan) == 2 && plan >= 0 && plan < kPlans) p->plan_of[c] = plan;
+        else if (sscanf(l.c_str() + key.size(), "window %d", &window) == 1 && window >= kCombMinBits &&
+                 window <= kCombMaxBits && comb_bytes(window) <= p->comb_budget)
+            p->comb_c_chosen = window;
     }
     fclose(f);
 }
@@ -958,14 +1040,10 @@ void load_tune_cache(vkzg_prover *p) {
 vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
     cudaStream_t s = p->stream;
     std::array<double, kPlans> ms{};
-    for (int plan = 0; plan < kPlans; plan++) {
-        if ((plan == 3 && (n < kCombMinBlobs || !ensure_comb(p))) || (plan == 4 && !ensure_flat_b(p))) {
-            ms[plan] = 1e30; // not available at this size or in this memory
-            continue;
-        }
+    auto time_plan = [&](int plan, double &best) -> vkzg_result {
         w.plan = plan;
         take_comb(w, p->pw);
-        double best = 1e30;
+        best = 1e30;
         for (int rep = 0; rep < 2; rep++) { // the first run of a plan also pays its first-launch costs
             CK(cudaEventRecord(p->ev_tune[0], s));
             CK(launch_proofs_timed(p->t, w, (int)n, s, nullptr));
@@ -975,7 +1053,42 @@ vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
             CK(cudaEventElapsedTime(&t, p->ev_tune[0], p->ev_tune[1]));
             best = std::min(best, (double)t);
         }
-        ms[plan] = best;
+        return VKZG_OK;
+    };
+    for (int plan = 0; plan < kPlans; plan++) {
+        ms[plan] = 1e30; // not available at this size or in this memory
+        if (plan == 4 && !ensure_flat_b(p)) continue;
+        if (plan == 3) {
+            // the digit table's window: every candidate timed, its table size
+            // the cost (the budget bounds it), the fastest kept
+            const std::vector<int> cands = n >= kCombMinBlobs ? comb_candidates(p) : std::vector<int>{};
+            if (cands.empty() || !comb_buffers(p, cands.back())) continue;
+            std::vector<vkzg_prover::WindowTrial> trials;
+            int best_c = 0;
+            for (int c : cands) {
+                if (!use_comb(p, c)) continue;
+                double t = 0.0;
+                const vkzg_result rc = time_plan(3, t);
+                if (rc != VKZG_OK) return rc;
+                trials.push_back({c, p->comb->bytes, p->comb->build_ms, t});
+                if (t < ms[3]) {
+                    ms[3] = t;
+                    best_c = c;
+                }
+            }
+            p->window_trials[size_class(n)] = trials;
+            if (best_c) {
+                p->comb_c_chosen = best_c;
+                if (comb_bits_forced() < 0) {
+                    std::lock_guard<std::mutex> lk(g_comb_mu);
+                    g_comb_choice[comb_choice_key(p)] = best_c;
+                }
+                if (!use_comb(p, best_c)) ms[3] = 1e30;
+            }
+            continue;
+        }
+        const vkzg_result rc = time_plan(plan, ms[plan]);
+        if (rc != VKZG_OK) return rc;
     }
     const uint32_t c = size_class(n);
     p->plan_ms[c] = ms;
@@ -1007,6 +1120,53 @@ bool tuned(const vkzg_prover *p, uint32_t n) {
     return p->plan_forced >= 0 || p->plan_of.count(size_class(n)) != 0;
 }
 
+// True for page-locked host memory (cudaHostAlloc'd or registered), which the
+// DMA engines read and write directly.
+bool host_pinned(const void *ptr) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy on up to 8 host threads (one per 4 MB, at most half the cores).
+void host_copy(void *dst, const void *src, size_t n) {
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const size_t threads = std::min<size_t>(std::min(8u, hw / 2), n >> 22);
+    if (threads <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t per = ((n + threads - 1) / threads + 4095) & ~(size_t)4095;
+    std::vector<std::thread> ts;
+    for (size_t t = 1; t < threads && t * per < n; t++)
+        ts.emplace_back([=] { memcpy((uint8_t *)dst + t * per, (const uint8_t *)src + t * per, std::min(per, n - t * per)); });
+    memcpy(dst, src, std::min(per, n));
+    for (auto &t : ts) t.join();
+}
+
+// The staging buffers, allocated on first use; false when pinned memory is
+// not available (the caller then copies from the pageable buffer directly).
+bool ensure_stage(vkzg_prover *p) {
+    if (p->stage_in) return true;
+    const size_t bytes = (size_t)p->cap * kExtElems * 32;
+    if (cudaHostAlloc(&p->stage_in, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        p->stage_in = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaHostAlloc(&p->stage_out, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaFreeHost(p->stage_in);
+        p->stage_in = p->stage_out = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    p->stage_bytes = bytes;
+    return true;
+}
+
 // Host blobs of a tuned chunk of >= 64 blobs go up in kUploadPieces pieces on the side
 // streams, and the per-blob front of the pipeline (stages 1-2) runs on each piece
 // as it lands, so the upload overlaps that work; the rest replays its own graph.
@@ -1016,6 +1176,12 @@ static bool upload_in_pieces(vkzg_prover *p, uint32_t n) {
 
 vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
+    // pageable blobs: through the pinned staging buffer (piece by piece below)
+    const bool staged = n >= 16 && !host_pinned(blobs) && ensure_stage(p);
+    if (staged && !upload_in_pieces(p, n)) {
+        host_copy(p->stage_in, blobs, (size_t)n * kBlobBytes);
+        blobs = p->stage_in;
+    }
     if (upload_in_pieces(p, n)) {
         p->pw.plan = plan_for(p, n);
         const vkzg_prover::GraphRec *rec = nullptr;
@@ -1026,9 +1192,14 @@ vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, 
         const uint32_t part = (n + vkzg_prover::kUploadPieces - 1) / vkzg_prover::kUploadPieces;
         for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
             const uint32_t cnt = std::min(part, n - off);
+            const uint8_t *src = blobs + (size_t)off * kBlobBytes;
+            if (staged) {
+                host_copy(p->stage_in + (size_t)off * kBlobBytes, src, (size_t)cnt * kBlobBytes);
+                src = p->stage_in + (size_t)off * kBlobBytes;
+            }
             CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
-            CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, blobs + (size_t)off * kBlobBytes,
-                               (size_t)cnt * kBlobBytes, cudaMemcpyHostToDevice, p->side[k]));
+            CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, src, (size_t)cnt * kBlobBytes,
+                               cudaMemcpyHostToDevice, p->side[k]));
             CK(cudaEventRecord(p->side_ev[k], p->side[k]));
             CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
             CK(launch_proofs_front(p->t, p->pw, (int)off, (int)cnt, s));
@@ -1069,6 +1240,49 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
     }
     cudaStream_t s = p->stream;
     const size_t ext = (size_t)kExtElems * 32;
+    const bool pin_in = host_pinned(cells), pin_out = host_pinned(out);
+    if (!p->timing && n >= 16 && p->side[0] && (!pin_in || !pin_out) && ensure_stage(p)) {
+        // pageable cells or output: slices through the pinned staging buffers,
+        // one host thread per slice copying in, enqueueing its copies and kernel
+        // on its own side stream, and copying out, so that the host copies of the
+        // slices run in parallel and overlap the DMA and kernels of the others
+        const uint32_t slices = std::min<uint32_t>(vkzg_prover::kStageSlices, n / 8);
+        const uint32_t slice = (n + slices - 1) / slices;
+        CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
+        CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
+        auto run_slice = [&](uint32_t k) -> vkzg_result {
+            const uint32_t off = k * slice, cnt = std::min(slice, n - off);
+            cudaStream_t st = p->side[k];
+            if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+            RecoverWork w = p->rw;
+            w.cells += off * ext;
+            w.present += (size_t)off * kCells;
+            w.out += off * ext;
+            w.err += off;
+            const uint8_t *src = cells + off * ext;
+            if (!pin_in) {
+                memcpy(p->stage_in + off * ext, src, cnt * ext);
+                src = p->stage_in + off * ext;
+            }
+            CK(cudaStreamWaitEvent(st, p->side_ev[vkzg_prover::kSides], 0));
+            CK(cudaMemcpyAsync(w.cells, src, cnt * ext, cudaMemcpyHostToDevice, st));
+            CK(launch_recover_timed(p->t, w, (int)cnt, st, nullptr));
+            CK(cudaMemcpyAsync(pin_out ? out + off * ext : p->stage_out + off * ext, w.out, cnt * ext,
+                               cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (!pin_out) memcpy(out + off * ext, p->stage_out + off * ext, cnt * ext);
+            return VKZG_OK;
+        };
+        const uint32_t used = (n + slice - 1) / slice;
+        std::vector<vkzg_result> rcs(used, VKZG_OK);
+        std::vector<std::thread> ts;
+        for (uint32_t k = 1; k < used; k++) ts.emplace_back([&, k] { rcs[k] = run_slice(k); });
+        rcs[0] = run_slice(0);
+        for (auto &t : ts) t.join();
+        for (vkzg_result rc : rcs)
+            if (rc != VKZG_OK) return rc;
+        return VKZG_OK;
+    }
     const uint32_t parts = std::min<uint32_t>(vkzg_prover::kRecMaxParts, n / vkzg_prover::kRecPartBlobs);
     const uint32_t part = n >= 64 && p->side[0] ? (n + parts - 1) / parts : n;
     if (p->timing || part == n) {
@@ -1369,6 +1583,13 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
     std::lock_guard<std::mutex> lock(p->mutex);
     if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
     const uint32_t top = std::min<uint32_t>(max_blobs ? max_blobs : p->cap, p->cap);
+    // size classes from the largest down, so that the digit table's window is
+    // chosen at the largest chunk (later classes keep it)
+    std::vector<uint32_t> sizes;
+    for (uint32_t n = 1; n <= top; n <<= 1) {
+        sizes.push_back(n);
+        if (n < top && (n << 1) > top) sizes.push_back(top); // finish with the capacity itself
+    }
     // seeded canonical blobs (top byte below r's 0x73)
     std::vector<uint8_t> blobs((size_t)top * kBlobBytes);
     uint64_t x = 0x7594ull;
@@ -1381,11 +1602,9 @@ vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs) {
     }
     CK(cudaMemcpyAsync(p->pw.blobs, blobs.data(), blobs.size(), cudaMemcpyHostToDevice, p->stream));
     CK(cudaMemsetAsync(p->pw.err, 0, top * sizeof(uint32_t), p->stream));
-    for (uint32_t n = 1; n <= top; n <<= 1) {
-        if (p->plan_forced >= 0) break;
-        const vkzg_result rc = tune_chunk(p, p->pw, n);
+    for (auto it = sizes.rbegin(); it != sizes.rend() && p->plan_forced < 0; ++it) {
+        const vkzg_result rc = tune_chunk(p, p->pw, *it);
         if (rc != VKZG_OK) return rc;
-        if (n < top && (n << 1) > top) n = top >> 1; // finish with the capacity itself
     }
     return VKZG_OK;
 }
@@ -1409,11 +1628,19 @@ void precapture_graphs(vkzg_prover *p, uint32_t max_n) {
     }
 }
 
+void set_comb_budget(vkzg_prover *p, uint64_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    p->comb_budget = bytes;
+}
+
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src) {
     if (!dst || !src) return;
     std::lock_guard<std::mutex> lock(dst->mutex);
     if (cudaSetDevice(dst->device) != cudaSuccess) return;
     bool want_comb = false, want_flat = false;
+    dst->comb_budget = src->comb_budget;
+    dst->comb_c_chosen = src->comb_c_chosen;
     for (const auto &kv : src->plan_of) {
         dst->plan_of[kv.first] = kv.second;
         want_comb |= kv.second == 3;
@@ -1431,6 +1658,30 @@ int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *byte
     if (build_ms) *build_ms = p->comb->build_ms;
     if (bytes) *bytes = p->comb->bytes;
     return p->comb->c;
+}
+
+void vkzg_b200_prover_device_bytes(const vkzg_prover *p, uint64_t *working, uint64_t *tables, uint64_t *digit_table) {
+    if (working) *working = p ? p->dev_bytes - p->tables_bytes : 0;
+    if (tables) *tables = p ? p->tables_bytes : 0;
+    if (digit_table) *digit_table = p && p->comb ? p->comb->bytes : 0;
+}
+
+int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *window_bits, uint64_t *table_bytes,
+                            double *build_ms, double *ms, int cap) {
+    if (!p) return 0;
+    auto it = p->window_trials.find(size_class);
+    if (it == p->window_trials.end()) return 0;
+    int i = 0;
+    for (const auto &t : it->second) {
+        if (i < cap) {
+            if (window_bits) window_bits[i] = t.c;
+            if (table_bytes) table_bytes[i] = t.bytes;
+            if (build_ms) build_ms[i] = t.build_ms;
+            if (ms) ms[i] = t.ms;
+        }
+        i++;
+    }
+    return i;
 }
 
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class_out, int *plan_out, double *ms_out, int cap) {

@@ -34,9 +34,8 @@ namespace {
 constexpr size_t kBlob = VKZG_BYTES_PER_BLOB;
 constexpr size_t kExt = (size_t)VKZG_NUM_CELL_PROOFS * VKZG_BYTES_PER_CELL;
 constexpr size_t kProofs = (size_t)VKZG_NUM_CELL_PROOFS * VKZG_BYTES_PER_PROOF;
-// device working set per blob in flight (prover working set + lane I/O buffers)
-constexpr uint64_t kProofBytesPerBlob = 7ull << 20;
-constexpr uint64_t kRecoverBytesPerBlob = 1ull << 20;
+// lane I/O buffers per blob of capacity: cells (or blob) in, cells (or proofs) out, presence, error word
+constexpr uint64_t kLaneBytesPerBlob = 2 * kExt + VKZG_NUM_CELL_PROOFS + sizeof(uint32_t);
 
 using Clock = std::chrono::steady_clock;
 
@@ -85,7 +84,10 @@ struct vkzg_server {
     std::deque<Part> pending;
     std::map<uint64_t, std::shared_ptr<Request>> requests;
     uint64_t next_id = 1;
-    uint64_t bytes_in_flight = 0;
+    uint64_t bytes_in_flight = 0, peak_in_flight = 0, deferrals = 0;
+    // admission charges: device working set per blob of a batch in flight
+    // (measured from the lanes' allocations), and the resident tables
+    uint64_t proof_bytes_per_blob = 0, recover_bytes_per_blob = kLaneBytesPerBlob, resident_bytes = 0;
     // the head request does not fit the HBM budget beside the batches in
     // flight: the dispatcher sleeps until one of them completes
     bool over_budget = false;
@@ -116,7 +118,7 @@ void vkzg_server::dispatch_loop() {
             if (l->busy || pending.empty()) continue;
             Batch b;
             b.kind = pending.front().req->kind;
-            const uint64_t per_blob = b.kind == 0 ? kProofBytesPerBlob : kRecoverBytesPerBlob;
+            const uint64_t per_blob = b.kind == 0 ? proof_bytes_per_blob : recover_bytes_per_blob;
             for (auto it = pending.begin(); it != pending.end();) {
                 if (it->req->kind != b.kind) {
                     ++it;
@@ -133,9 +135,11 @@ void vkzg_server::dispatch_loop() {
             }
             if (b.parts.empty()) { // budget exhausted until something completes
                 over_budget = true;
+                deferrals++;
                 break;
             }
             bytes_in_flight += b.bytes;
+            peak_in_flight = std::max(peak_in_flight, bytes_in_flight);
             l->batch = std::move(b);
             l->busy = true;
             l->cv.notify_one();
@@ -225,6 +229,7 @@ void vkzg_b200_server_options_default(vkzg_server_options *o) {
     o->max_blobs_per_batch = 0;
     o->lanes = 0;
     o->hbm_budget_bytes = 0;
+    o->table_budget_bytes = 0;
 }
 
 vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *opts) {
@@ -238,6 +243,7 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
     if (!s->opts.lanes) s->opts.lanes = 3;
     if (!s->opts.hbm_budget_bytes) s->opts.hbm_budget_bytes = 8ull << 30;
     const uint32_t cap = s->opts.max_blobs_per_batch;
+    if (!s->opts.table_budget_bytes) s->opts.table_budget_bytes = 20ull << 30;
     vkzg_result rc = VKZG_OK;
     for (uint32_t k = 0; k < s->opts.lanes && rc == VKZG_OK; k++) {
         auto lane = std::make_unique<Lane>();
@@ -246,6 +252,7 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
         po.max_batch_size = cap;
         rc = vkzg_prover_new(&lane->p, &po);
         if (rc != VKZG_OK) break;
+        vkzg::set_comb_budget(lane->p, s->opts.table_budget_bytes);
         if (cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaMalloc(&lane->d_in, cap * kExt) != cudaSuccess || cudaMalloc(&lane->d_out, cap * kExt) != cudaSuccess ||
             cudaMalloc(&lane->d_present, cap * VKZG_NUM_CELL_PROOFS) != cudaSuccess ||
@@ -270,6 +277,16 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
     // and capture every batch size's proof pipeline on every lane: a capture on
     // first use would hold up the request that meets it
     for (auto &l : s->lanes) vkzg::precapture_graphs(l->p, cap);
+    // admission charges from what the lanes hold: a proof blob in flight uses
+    // its share of a lane prover's working set and of the lane's I/O buffers
+    uint64_t working = 0, tables = 0, digit = 0;
+    vkzg_b200_prover_device_bytes(s->lanes[0]->p, &working, &tables, &digit);
+    s->proof_bytes_per_blob = working / cap + kLaneBytesPerBlob;
+    for (auto &l : s->lanes) {
+        vkzg_b200_prover_device_bytes(l->p, &working, &tables, nullptr);
+        s->resident_bytes += tables;
+    }
+    s->resident_bytes += digit; // shared by the lanes
     for (auto &l : s->lanes) {
         Lane *lp = l.get();
         l->worker = std::thread([s, lp] { s->lane_loop(lp); });
@@ -385,8 +402,15 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
     for (double x : v) sum += x;
     out->mean_ms = v.empty() ? 0.0 : sum / v.size();
     out->seconds = std::chrono::duration<double>(Clock::now() - s->stats_since).count();
+    out->deferrals = s->deferrals;
+    out->peak_in_flight_bytes = s->peak_in_flight;
+    out->resident_bytes = s->resident_bytes;
+    out->proof_bytes_per_blob = s->proof_bytes_per_blob;
+    out->recover_bytes_per_blob = s->recover_bytes_per_blob;
     if (reset) {
         s->lat_ms.clear();
+        s->deferrals = 0;
+        s->peak_in_flight = s->bytes_in_flight;
         s->done_requests = s->done_blobs = 0;
         s->stats_since = Clock::now();
     }
