@@ -78,10 +78,11 @@ def phase_a_executed_imad_per_output(c):
     muls = 5 * adds + 7 * madds + 11
     sqrs = adds + 4 * madds + 5
     return muls * IMAD_FP_MUL_KS + sqrs * IMAD_FP_SQR_KS
-# DRAM bytes of phase A per blob under plan 3, by window: ncu dram__bytes_read +
-# dram__bytes_write of every phase-A kernel of a 16-blob proof call (one kernel
-# per capture, profiles/phase_a_dram_traffic_16blobs.md), divided by 16
-PHASE_A_DRAM_BYTES_PER_BLOB = {}
+# DRAM bytes of phase A per blob under plan 3, by window: per-pair ncu
+# dram__bytes_read + dram__bytes_write of each phase-A kernel in a 16-blob,
+# 9-bit-window capture (one kernel per capture), applied to the exact pair
+# counts of a 13-bit window (profiles/phase_a_dram_traffic_16blobs.md)
+PHASE_A_DRAM_BYTES_PER_BLOB = {13: 30.0e9 / 256}
 
 
 # ------------------------------------------------------------------ inputs
@@ -680,7 +681,8 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": PHASE_A_DRAM_BYTES_PER_BLOB[digit[0]] * n
                      if plan == 3 and digit and digit[0] in PHASE_A_DRAM_BYTES_PER_BLOB else None,
                      "traffic_unit": "DRAM bytes per phase-A pass over the batch (ncu dram__bytes_read + write "
-                                     "of a 16-blob capture per kernel, scaled by blobs)"},
+                                     "per pair from a 16-blob 9-bit-window capture, one kernel each, applied "
+                                     "to this window's pair counts)"},
         "digit_table": {"window_bits": digit[0], "build_ms": round(digit[1], 1), "bytes": digit[2],
                         "budget_bytes": table_budget,
                         "window_trials": [{"window_bits": c, "bytes": b, "build_ms": round(bm, 1), "proof_ms": round(t, 3)}

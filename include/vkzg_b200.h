@@ -220,7 +220,9 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
  * between the passes of a batch-affine round), with variable-time and with
  * fixed 30-divstep batches; 12: Fp multiplies with the partial products on the
  * FP64 pipe, 13: Fp squares on the FP64 pipe, 14: Fp multiplies with half the
- * warps on each pipe (giga-ops/s).  Best of three timed launches.
+ * warps on each pipe, 15 and 16: Fp multiplies on the FP64 pipe and through one
+ * Karatsuba level with four independent chains per thread instead of two
+ * (giga-ops/s).  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
 

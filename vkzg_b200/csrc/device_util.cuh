@@ -162,4 +162,75 @@ __device__ void smem_dif(Fr *s, int log_n, int count, int len_hi, int len_lo, co
     }
 }
 
+// The same stages two at a time: a radix-4 butterfly on the elements
+// j, j + h, j + 2h, j + 3h of each group of 4h does stage len = 2h and stage
+// 4h in registers (the same four products per four elements as two radix-2
+// stages), so each pair of stages is one read and one write of shared memory
+// and one barrier instead of two.  An odd stage count starts (DIT) or ends
+// (DIF) with one radix-2 stage at the shortest length.
+template <int NT>
+__device__ void smem_dit4(Fr *s, int log_n, int count, int len_lo, int len_hi, const Fr *__restrict__ roots) {
+    int stages = 0;
+    for (int len = len_lo; len <= len_hi; len <<= 1) stages++;
+    int len = len_lo;
+    if (stages & 1) {
+        smem_dit<NT>(s, log_n, count, len, len, roots);
+        len <<= 1;
+    }
+    const int n = 1 << log_n;
+    const int total = (n >> 2) * count;
+    for (; len < len_hi; len <<= 2) {
+        const int h = len >> 1, stride = 8192 / (2 * len); // twiddles of the longer stage: w_{2 len}^j
+        for (int q = threadIdx.x; q < total; q += NT) {
+            const int tr = q >> (log_n - 2), k = q & ((n >> 2) - 1);
+            const int blk = k / h, j = k - blk * h;
+            Fr *base = s + tr * n + blk * 4 * h + j;
+            const Fr a0 = ld_vec(base), a1 = ld_vec(base + h), a2 = ld_vec(base + 2 * h), a3 = ld_vec(base + 3 * h);
+            const Fr w1 = ldg_vec(&roots[2 * j * stride]);        // w_len^j
+            const Fr w2 = ldg_vec(&roots[j * stride]);            // w_{2 len}^j
+            const Fr w3 = ldg_vec(&roots[(j + h) * stride]);      // w_{2 len}^(j + h)
+            Fr t = fr_mul(a1, w1);
+            const Fr b0 = fr_add(a0, t), b1 = fr_sub(a0, t);
+            t = fr_mul(a3, w1);
+            const Fr b2 = fr_add(a2, t), b3 = fr_sub(a2, t);
+            t = fr_mul(b2, w2);
+            st_vec(base, fr_add(b0, t));
+            st_vec(base + 2 * h, fr_sub(b0, t));
+            t = fr_mul(b3, w3);
+            st_vec(base + h, fr_add(b1, t));
+            st_vec(base + 3 * h, fr_sub(b1, t));
+        }
+        __syncthreads();
+    }
+}
+
+template <int NT>
+__device__ void smem_dif4(Fr *s, int log_n, int count, int len_hi, int len_lo, const Fr *__restrict__ roots) {
+    int stages = 0;
+    for (int len = len_hi; len >= len_lo; len >>= 1) stages++;
+    const int n = 1 << log_n;
+    const int total = (n >> 2) * count;
+    int len = len_hi; // the longer of each pair of stages
+    for (int pairs = stages >> 1; pairs > 0; pairs--, len >>= 2) {
+        const int h = len >> 2, stride = 8192 / len; // w_len^j and w_{len/2}^j = w_len^(2j)
+        for (int q = threadIdx.x; q < total; q += NT) {
+            const int tr = q >> (log_n - 2), k = q & ((n >> 2) - 1);
+            const int blk = k / h, j = k - blk * h;
+            Fr *base = s + tr * n + blk * 4 * h + j;
+            const Fr a0 = ld_vec(base), a1 = ld_vec(base + h), a2 = ld_vec(base + 2 * h), a3 = ld_vec(base + 3 * h);
+            const Fr w2 = ldg_vec(&roots[j * stride]);            // w_len^j
+            const Fr w3 = ldg_vec(&roots[(j + h) * stride]);      // w_len^(j + h)
+            const Fr w1 = ldg_vec(&roots[2 * j * stride]);        // w_{len/2}^j
+            const Fr t0 = fr_add(a0, a2), t2 = fr_mul(fr_sub(a0, a2), w2);
+            const Fr t1 = fr_add(a1, a3), t3 = fr_mul(fr_sub(a1, a3), w3);
+            st_vec(base, fr_add(t0, t1));
+            st_vec(base + h, fr_mul(fr_sub(t0, t1), w1));
+            st_vec(base + 2 * h, fr_add(t2, t3));
+            st_vec(base + 3 * h, fr_mul(fr_sub(t2, t3), w1));
+        }
+        __syncthreads();
+    }
+    if (stages & 1) smem_dif<NT>(s, log_n, count, len, len, roots);
+}
+
 } // namespace vkzg

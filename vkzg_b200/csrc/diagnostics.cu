@@ -113,6 +113,26 @@ __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint
     b.v[1] ^= seed * 3u + blockIdx.x;
     const Fp c = a;
     const bool odd_warp = (threadIdx.x >> 5) & 1;
+    if constexpr (OP == 8 || OP == 9) { // four independent chains per thread, half the iterations
+        Fp d = b, e = a;
+        d.v[2] ^= 5u;
+        e.v[3] ^= 7u;
+        for (int i = 0; i < iters / 2; i++) {
+            if (OP == 8) {
+                a = fp_mul_f64_call(a, c);
+                b = fp_mul_f64_call(b, c);
+                d = fp_mul_f64_call(d, c);
+                e = fp_mul_f64_call(e, c);
+            } else {
+                a = fp_mul_ks_call(a, c);
+                b = fp_mul_ks_call(b, c);
+                d = fp_mul_ks_call(d, c);
+                e = fp_mul_ks_call(e, c);
+            }
+        }
+        if ((a.v[0] ^ b.v[0] ^ d.v[0] ^ e.v[0]) == 0x12345678u) sink[0] = a.v[1];
+        return;
+    } else {
     for (int i = 0; i < iters; i++) {
         if (OP == 5 || (OP == 7 && odd_warp)) {
             a = fp_mul_f64_call(a, c);
@@ -141,6 +161,7 @@ __global__ void __launch_bounds__(128) k_probe_fp(uint32_t seed, int iters, uint
         }
     }
     if ((a.v[0] ^ b.v[0]) == 0x12345678u) sink[0] = a.v[1];
+    }
 }
 
 // OP 0: fr_mul (CIOS), 1: the Karatsuba product
@@ -287,7 +308,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 14) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 16) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -322,7 +343,9 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
             else if (which == 7) k_probe_fp<4><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 12) k_probe_fp<5><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             else if (which == 13) k_probe_fp<6><<<blocks, 128>>>(rep + 1, fp_iters, sink);
-            else k_probe_fp<7><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 14) k_probe_fp<7><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else if (which == 15) k_probe_fp<8><<<blocks, 128>>>(rep + 1, fp_iters, sink);
+            else k_probe_fp<9><<<blocks, 128>>>(rep + 1, fp_iters, sink);
             ops = (double)blocks * 128 * 2 * fp_iters;
         } else {
             const int blocks = sms * 8;

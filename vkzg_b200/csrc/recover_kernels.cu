@@ -94,7 +94,10 @@ __device__ void cluster_dit_scale_dif(cg::cluster_group &cl, Fr *s, const Fr *__
 
 // three blocks per SM (80 registers; 64 KB of shared memory each) measured
 // faster than two with more registers: 143 k against 138 k blobs/s
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, 3)
+#ifndef VKZG_REC_MIN_BLOCKS
+#define VKZG_REC_MIN_BLOCKS 3
+#endif
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, VKZG_REC_MIN_BLOCKS)
     k_recover_cluster(const uint8_t *__restrict__ cells, const uint8_t *__restrict__ present, uint8_t *out,
                       const Fr *__restrict__ roots_fwd, const Fr *__restrict__ roots_inv,
                       const Fr *__restrict__ shift_fwd, const Fr *__restrict__ shift_inv, Fr seven64,
@@ -175,24 +178,24 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kRecQThreads, 3)
         st_vec(&s[q], fr_mul(ld_vec(&zq[q >> 6]), v)); // raw word second
     }
     __syncthreads();
-    smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
+    smem_dit4<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
     cl.sync();
     // B: finish the IFFT, x 7^k / N, first two stages of the coset FFT
     cluster_dit_scale_dif(cl, s, roots_fwd, roots_inv, shift_fwd);
     cl.sync();
     // C: coset FFT inner stages, divide by Z on the coset, inverse DIT inner stages
-    smem_dif<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
+    smem_dif4<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
     for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads)
         st_vec(&s[q], fr_mul(ld_vec(&s[q]), ld_vec(&izq[q >> 6])));
     __syncthreads();
-    smem_dit<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
+    smem_dit4<kRecQThreads>(s, 11, 1, 2, kRecQuarter, roots_inv);
     cl.sync();
     // D: finish the coset IFFT, x 7^-k / N / R, first two stages of the final FFT
     cluster_dit_scale_dif(cl, s, roots_fwd, roots_inv, shift_inv);
     cl.sync();
     // E: final FFT inner stages; bit-reversed output = wire order (no shared
     // memory of another block is touched after the last cluster barrier)
-    smem_dif<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
+    smem_dif4<kRecQThreads>(s, 11, 1, kRecQuarter, 2, roots_fwd);
     uint8_t *dst = out + ((size_t)b * kExtElems + first) * 32;
     for (int q = threadIdx.x; q < kRecQuarter; q += kRecQThreads) {
         const Fr v = ld_vec(&s[q]);
