@@ -517,6 +517,37 @@ def run_ours(args, rank, world, local_rank):
         c1 = {"blobs": 16, "present_per_blob": 64, "device_blobs_per_s": 16 / (statistics.median(c1_ms) / 1e3),
               "e2e_blobs_per_s": 16 / statistics.median(c1_e2e)}
 
+    # ---- the same proof step in its persistent form ($VKZG_COOP=1: each phase's
+    # grid-wide rounds in one cooperative launch with grid barriers), timed the
+    # same way on its own prover (the digit table is shared)
+    persistent = None
+    os.environ["VKZG_COOP"] = "1"
+    try:
+        with vkzg_b200.Prover(max_batch_size=n) as pc:
+            pc.autotune(n)
+            d_proofs_c = torch.empty_like(d_proofs)
+            for _ in range(args.warmup):
+                pc.compute_proofs_device(d_proofs_c.data_ptr(), d_blobs.data_ptr(), d_err.data_ptr(), n, sp)
+            torch.cuda.synchronize()
+            l0 = vkzg_b200.kernel_launches()
+            c_ms = []
+            for _ in range(args.steps):
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pc.compute_proofs_device(d_proofs_c.data_ptr(), d_blobs.data_ptr(), d_err.data_ptr(), n, sp)
+                e1.record(stream)
+                e1.synchronize()
+                c_ms.append(e0.elapsed_time(e1))
+            c_launches = vkzg_b200.kernel_launches() - l0
+            assert int(d_err[:n].count_nonzero()) == 0
+            assert torch.equal(d_proofs_c, d_proofs), "persistent form's proofs differ"
+            persistent = {"proof_ms": statistics.mean(c_ms), "graph_ms": statistics.mean(proof_ms),
+                          "launches_per_step": c_launches / args.steps,
+                          "graph_launches_per_step": launches / args.steps - 1}
+    finally:
+        del os.environ["VKZG_COOP"]
+
     # ---- per-stage breakdown from untimed steps with stage events (the timed steps
     # above replay the captured pipeline; these launch it stage by stage)
     prover.set_stage_timing(True)
@@ -688,6 +719,7 @@ def run_ours(args, rank, world, local_rank):
                         "window_trials": [{"window_bits": c, "bytes": b, "build_ms": round(bm, 1), "proof_ms": round(t, 3)}
                                           for c, b, bm, t in prover.window_trials(n)]} if digit else None,
         "device_bytes": prover.device_bytes(),
+        "persistent_form": persistent,
         "verified": verified,
         "c1_recovery_16_blobs": c1,
         "cpu_baseline": cpu,

@@ -44,8 +44,11 @@ const char *vkzg_b200_stage_name(int recovery, int i);
  * is ordered after it; the call returns once the work is enqueued.
  * d_err (num_blobs words) receives a nonzero word for each blob with a
  * non-canonical element (proofs) or more than 64 missing cells (recovery);
- * those blobs' outputs are unspecified.
+ * those blobs' outputs are unspecified.  Bit 31 of every word of a proof chunk
+ * (VKZG_B200_DEVICE_FAILED) means a grid barrier of the chunk's cooperative
+ * launches gave up waiting (the host entry points return VKZG_ERR_GPU then).
  */
+#define VKZG_B200_DEVICE_FAILED 0x80000000u
 vkzg_result vkzg_b200_compute_proofs_device(vkzg_prover *p, uint8_t *d_proofs, const uint8_t *d_blobs,
                                             uint32_t *d_err, size_t num_blobs, void *stream);
 vkzg_result vkzg_b200_recover_cells_device(vkzg_prover *p, uint8_t *d_cells_out, const uint8_t *d_cells,
@@ -236,6 +239,20 @@ vkzg_result vkzg_b200_microbench(int which, double *result);
  */
 vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, const uint32_t *bucket_of, size_t n,
                                            uint8_t *sums_xy);
+
+/*
+ * Self-test of the grid barrier that the cooperative launches of plans 3-4 use
+ * between their passes.  No counterpart in the reference.  One cooperative
+ * launch of two blocks per SM crosses `rounds` barriers; *barriers_passed is
+ * the sum over blocks of the barriers each passed, *failed_flag the barrier's
+ * failure flag, *error_words_marked how many of the launch's 8 error words got
+ * VKZG_B200_DEVICE_FAILED.  With extra_arrivals > 0 every barrier waits for
+ * blocks that do not exist: each wait gives up after spin_limit polls (about
+ * 100 ns each), so the launch ends with the flag set instead of waiting forever.
+ */
+vkzg_result vkzg_b200_grid_sync_selftest(uint32_t extra_arrivals, uint32_t spin_limit, int rounds,
+                                         uint32_t *barriers_passed, uint32_t *failed_flag,
+                                         uint32_t *error_words_marked);
 
 /*
  * Sums n_lists lists of m affine points each (points_xy: n_lists * m x 96

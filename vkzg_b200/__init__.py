@@ -45,6 +45,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_server_submit_proofs", "vkzg_b200_server_submit_recovery", "vkzg_b200_server_wait",
     "vkzg_b200_server_stats", "vkzg_b200_kernel_launches", "vkzg_b200_digit_table",
     "vkzg_b200_tree_sums_selftest", "vkzg_b200_window_trials", "vkzg_b200_prover_device_bytes",
+    "vkzg_b200_grid_sync_selftest",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -159,6 +160,9 @@ def library():
             L.vkzg_b200_prover_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                         ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
             L.vkzg_b200_prover_device_bytes.restype = None
+            u32p = ctypes.POINTER(ctypes.c_uint32)
+            L.vkzg_b200_grid_sync_selftest.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, u32p, u32p, u32p]
+            L.vkzg_b200_grid_sync_selftest.restype = ctypes.c_int
             L.vkzg_b200_kernel_launches.argtypes = []
             L.vkzg_b200_kernel_launches.restype = ctypes.c_uint64
             _lib = L
@@ -423,6 +427,15 @@ class Server:
         st = ServerStats()
         _check(self._lib.vkzg_b200_server_stats(self._h, ctypes.byref(st), 1 if reset else 0))
         return st.as_dict()
+
+
+def grid_sync_selftest(extra_arrivals, spin_limit, rounds):
+    """(barriers passed summed over blocks, failure flag, error words marked) of one
+    cooperative launch crossing `rounds` grid barriers (vkzg_b200_grid_sync_selftest)."""
+    a, b, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    _check(library().vkzg_b200_grid_sync_selftest(int(extra_arrivals), int(spin_limit), int(rounds),
+                                                  ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return a.value, b.value, c.value
 
 
 def kernel_launches():

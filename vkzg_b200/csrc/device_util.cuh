@@ -116,6 +116,65 @@ __device__ Fr block_batch_inverse_fr(const Fr &z, Fr *tree) {
     return res;
 }
 
+// ------------------------------------------------------------ grid barrier
+// A barrier across every block of a cooperative launch (all blocks resident),
+// whose every wait is bounded.  word[0] counts arrivals, word[1] is the
+// generation the last arrival advances, word[2] is the failure flag: a block
+// that waits spin_limit polls without the generation moving (or that finds
+// the flag set) sets the flag, marks every error word of err[0..n_err) with
+// kSyncFailed and returns false; the kernel then returns, and the other
+// blocks, finding the flag set at their next wait, return too.  The words
+// start at zero (the launcher clears them); after a barrier the arrival count
+// is zero again, so one launch reuses them across its barriers.
+constexpr uint32_t kSyncFailed = 0x80000000u; // VKZG_B200_DEVICE_FAILED in include/vkzg_b200.h
+struct GridSync {
+    uint32_t *word;
+    uint32_t *err;
+    uint32_t n_err;
+    uint32_t spin_limit;
+    uint32_t expected; // arrivals that complete a barrier: gridDim.x
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+static __device__ __noinline__ bool grid_sync(const GridSync &g) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        uint32_t *cnt = g.word, *gen = g.word + 1, *flag = g.word + 2;
+        if (ld_acquire_gpu(flag)) {
+            ok = 0;
+        } else {
+            const uint32_t my_gen = ld_acquire_gpu(gen);
+            __threadfence();
+            if (atomicAdd(cnt, 1u) == g.expected - 1) {
+                atomicExch(cnt, 0u);
+                __threadfence();
+                atomicAdd(gen, 1u);
+            } else {
+                for (uint32_t spins = 0; ld_acquire_gpu(gen) == my_gen; spins++) {
+                    if (spins >= g.spin_limit || ld_acquire_gpu(flag)) {
+                        if (atomicExch(flag, 1u) == 0u)
+                            for (uint32_t b = 0; b < g.n_err; b++) atomicOr(&g.err[b], kSyncFailed);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(100);
+                }
+            }
+            __threadfence();
+        }
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
 // ------------------------------------------------------------ NTT stages
 // roots: w_8192^(+-i), i < 8192 (Montgomery).  A transform of length n uses
 // w_len^j = roots[j * 8192 / len].

@@ -375,6 +375,67 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
     return VKZG_OK;
 }
 
+// Grid barriers alone, in a cooperative launch of two 256-thread blocks per
+// SM: `rounds` barriers, each block counting the ones it passed.  With
+// extra_arrivals > 0 a barrier waits for more blocks than the grid has, so no
+// barrier can complete: every wait runs out after spin_limit polls, sets the
+// failure flag and marks the error words, and every block returns.
+__global__ void __launch_bounds__(256) k_sync_probe(GridSync g, int rounds, uint32_t *passed) {
+    for (int r = 0; r < rounds; r++) {
+        if (!grid_sync(g)) return;
+        if (threadIdx.x == 0) atomicAdd(passed, 1u);
+    }
+}
+
+extern "C" vkzg_result vkzg_b200_grid_sync_selftest(uint32_t extra_arrivals, uint32_t spin_limit, int rounds,
+                                                    uint32_t *barriers_passed, uint32_t *failed_flag,
+                                                    uint32_t *error_words_marked) {
+    if (!barriers_passed || !failed_flag || !error_words_marked || rounds < 0 || rounds > 1000 ||
+        extra_arrivals > 1024)
+        return VKZG_ERR_BADARGS;
+    int dev = 0, sms = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+        return VKZG_ERR_GPU;
+    const int blocks = 2 * sms;
+    constexpr uint32_t kErrWords = 8;
+    uint32_t *d = nullptr; // [0..4) barrier words, [4] passed, [8..16) error words
+    if (cudaMalloc(&d, 16 * sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
+    vkzg_result rc = VKZG_OK;
+    if (cudaMemset(d, 0, 16 * sizeof(uint32_t)) != cudaSuccess) rc = VKZG_ERR_GPU;
+    GridSync g;
+    g.word = d;
+    g.err = d + 8;
+    g.n_err = kErrWords;
+    g.spin_limit = spin_limit;
+    g.expected = (uint32_t)blocks + extra_arrivals;
+    uint32_t *passed = d + 4;
+    if (rc == VKZG_OK) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)blocks);
+        cfg.blockDim = dim3(256);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (cudaLaunchKernelEx(&cfg, k_sync_probe, g, rounds, passed) != cudaSuccess ||
+            cudaDeviceSynchronize() != cudaSuccess)
+            rc = VKZG_ERR_GPU;
+    }
+    uint32_t h[16] = {};
+    if (rc == VKZG_OK && cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) rc = VKZG_ERR_GPU;
+    cudaFree(d);
+    if (rc != VKZG_OK) return rc;
+    *barriers_passed = h[4];
+    *failed_flag = h[2];
+    uint32_t marked = 0;
+    for (uint32_t i = 0; i < kErrWords; i++) marked += (h[8 + i] & kSyncFailed) ? 1u : 0u;
+    *error_words_marked = marked;
+    return VKZG_OK;
+}
+
 // Sums n_lists lists of m points each with the proof path's grid-wide
 // batch-affine tree rounds (plan 3's phase-A rounds, without the digit table).
 // points_xy: n_lists * m points of 96 bytes (list o first), or NULL for seeded

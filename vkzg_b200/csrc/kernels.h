@@ -139,6 +139,10 @@ struct ProofWork {
     G1A *flatb_buf[2] = {nullptr, nullptr}; // phase B's round buffers
     int plan = 1;               // 0 serial Jacobian; 1 batch-affine + binary-split reduction; 2 batch-affine + serial reduction
     G1A *red_scratch = nullptr; // [cap * 128][247] batch-affine reduction slots
+    // plans 3-4: the grid-wide rounds of each phase as one cooperative launch
+    // (grid barriers between passes) when true, else three launches per round
+    bool coop = false;
+    uint32_t *sync = nullptr;   // [4] grid-barrier words of the cooperative launches
 };
 // Batch-affine kernels: VKZG_BA_THREADS threads per block, one warp sums the
 // buckets of kWarpOutputs MSM outputs at a time.  Per-warp scratch: round-1 and
@@ -189,6 +193,11 @@ cudaError_t configure_kernels();
 struct vkzg_prover;
 namespace vkzg {
 void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src);
+// the cooperative forms of plans 3-4 fit blocks_per_sm blocks per SM
+bool coop_supported(int blocks_per_sm);
+// no cooperative launches for this prover (a serving lane: several lanes'
+// pipelines run at once, and each cooperative launch wants the whole GPU)
+void disable_coop(vkzg_prover *p);
 // digit-table byte budget of a prover (before its first tuning)
 void set_comb_budget(vkzg_prover *p, uint64_t bytes);
 void precapture_graphs(vkzg_prover *p, uint32_t max_n);

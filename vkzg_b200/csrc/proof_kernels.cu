@@ -590,8 +590,16 @@ __device__ __forceinline__ void flat_pass1_products(const Fp &acc, Fp *others, F
     if (lane == 0) st_vec(&tot[wg], total);
 }
 
+// A round's input and output lists, apart from the phase's other arguments:
+// a cooperative launch changes them every round while the rest stays in the
+// kernel's parameters.
+struct RoundIO {
+    const G1A *src;
+    G1A *dst;
+};
+
 template <bool FIRST>
-__device__ __forceinline__ G1A flat_load(const FlatArgs &a, uint32_t o, uint32_t t, uint32_t m) {
+__device__ __forceinline__ G1A flat_load(const FlatArgs &a, RoundIO io, uint32_t o, uint32_t t, uint32_t m) {
     if (FIRST) {
         const int v = a.dig[(size_t)o * a.L + t];
         G1A pt;
@@ -604,18 +612,18 @@ __device__ __forceinline__ G1A flat_load(const FlatArgs &a, uint32_t o, uint32_t
         if (v < 0) pt.y = fp_neg(pt.y);
         return pt;
     }
-    return ld_vec(&a.src[(size_t)o * m + t]);
+    return ld_vec(&io.src[(size_t)o * m + t]);
 }
 
 // the x coordinate of flat_load's point (0 for a zero digit)
 template <bool FIRST>
-__device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, uint32_t o, uint32_t t, uint32_t m) {
+__device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, RoundIO io, uint32_t o, uint32_t t, uint32_t m) {
     if (FIRST) {
         const int v = a.dig[(size_t)o * a.L + t];
         if (v == 0) return fp_zero();
         return ldg_vec(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)].x);
     }
-    return ld_vec(&a.src[(size_t)o * m + t].x);
+    return ld_vec(&io.src[(size_t)o * m + t].x);
 }
 
 // Signed c-bit digits of every scalar: scalar q = o 64 + i fills dig[q D ..].
@@ -666,8 +674,7 @@ __device__ __forceinline__ void pair_step_down(uint32_t &o, uint32_t &i, uint32_
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void flat_pass1_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1;
     const uint32_t P = (uint32_t)a.n_lists * h;
@@ -677,22 +684,29 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint
     int s = 0;
     uint32_t o = gl / h, i = gl % h;
     for (uint32_t p = gl; p < P; p += NL, s++) {
-        const Fp x = flat_load_x<FIRST>(a, o, 2 * i, m), y = flat_load_x<FIRST>(a, o, 2 * i + 1, m);
+        const Fp x = flat_load_x<FIRST>(a, io, o, 2 * i, m), y = flat_load_x<FIRST>(a, io, o, 2 * i + 1, m);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<FIRST>(a, o, 2 * i, m); },
-                                             [&] { return flat_load<FIRST>(a, o, 2 * i + 1, m); }));
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<FIRST>(a, io, o, 2 * i, m); },
+                                             [&] { return flat_load<FIRST>(a, io, o, 2 * i + 1, m); }));
         pair_step_up(o, i, h, dq, dr);
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
+    flat_pass1_body<FIRST>(a, RoundIO{a.src, a.dst}, m, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // Inverts the n warp products, one per thread: the launch sits on the critical
 // path between the passes, and one divstep inversion per lane (all in parallel)
 // has less latency than a shared batch inversion (a product scan of 32 values,
 // one inversion, a scan back).
-__global__ void __launch_bounds__(64) k_flat_invert(const Fp *__restrict__ tot, Fp *totinv, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) st_vec(&totinv[t], fp_inv_fast(ld_vec(&tot[t])));
+__device__ __forceinline__ void flat_invert_body(const Fp *tot, Fp *totinv, uint32_t n, uint32_t gl, uint32_t NL) {
+    for (uint32_t t = gl; t < n; t += NL) st_vec(&totinv[t], fp_inv_fast(ld_vec(&tot[t])));
+}
+__global__ void __launch_bounds__(64) k_flat_invert(const Fp *tot, Fp *totinv, int n) {
+    flat_invert_body(tot, totinv, (uint32_t)n, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // Products inlined into this loop instead of called: measured 14.1 against
@@ -703,8 +717,7 @@ __global__ void __launch_bounds__(64) k_flat_invert(const Fp *__restrict__ tot, 
 #endif
 constexpr bool kPass2Inline = VKZG_PASS2_INLINE != 0;
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint32_t m) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void flat_pass2_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1, m_next = (m + 1) >> 1;
     const uint32_t P = (uint32_t)a.n_lists * h;
@@ -720,16 +733,21 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint
     }
     for (int t = S - 1; t >= 0; t--) {
         if (t < S - 1) pair_step_down(o, i, h, dq, dr);
-        const G1A x = flat_load<FIRST>(a, o, 2 * i, m), y = flat_load<FIRST>(a, o, 2 * i + 1, m);
+        const G1A x = flat_load<FIRST>(a, io, o, 2 * i, m), y = flat_load<FIRST>(a, io, o, 2 * i + 1, m);
         const int kind = pair_kind(x, y);
         const Fp den = pair_denominator(x, y, kind);
         const Fp inv_den = pmul<kPass2Inline>(inv, wb_load_pre(pre, t));
         inv = pmul<kPass2Inline>(inv, den);
-        st_vec(&a.dst[(size_t)o * m_next + i], pair_result<kPass2Inline>(x, y, kind, inv_den));
+        st_vec(&io.dst[(size_t)o * m_next + i], pair_result<kPass2Inline>(x, y, kind, inv_den));
     }
     if (m & 1u)
         for (uint32_t l = gl; l < (uint32_t)a.n_lists; l += NL)
-            st_vec(&a.dst[(size_t)l * m_next + h], flat_load<FIRST>(a, l, m - 1, m));
+            st_vec(&io.dst[(size_t)l * m_next + h], flat_load<FIRST>(a, io, l, m - 1, m));
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint32_t m) {
+    flat_pass2_body<FIRST>(a, RoundIO{a.src, a.dst}, m, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // The last m <= kTreeTail points of each list (affine, left by the tree
@@ -828,6 +846,108 @@ int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *
     return launched;
 }
 
+// The pass bodies as the cooperative kernels call them: inlined (default), or
+// out of line with their arguments by value (VKZG_COOP_NOINLINE=1), each then
+// with its own register allocation.
+#ifndef VKZG_COOP_NOINLINE
+#define VKZG_COOP_NOINLINE 0
+#endif
+#if VKZG_COOP_NOINLINE
+#define VKZG_COOP_FN __device__ __noinline__
+#else
+#define VKZG_COOP_FN __device__ __forceinline__
+#endif
+template <bool FIRST>
+VKZG_COOP_FN void coop_flat_pass1(FlatArgs a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+    flat_pass1_body<FIRST>(a, io, m, gl, NL);
+}
+template <bool FIRST>
+VKZG_COOP_FN void coop_flat_pass2(FlatArgs a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+    flat_pass2_body<FIRST>(a, io, m, gl, NL);
+}
+
+// The inversions between the passes of a cooperative round: one warp in 32
+// inverts the products of warps wg..wg+31, one per lane, so that they spread
+// over the SMs as the separate inversion launch does (the first 2368 threads
+// of the grid would put them all on a few SMs).
+__device__ __noinline__ void coop_invert(const Fp *tot, Fp *totinv, uint32_t n, uint32_t gl, uint32_t NL) {
+    (void)NL;
+    const uint32_t wg = gl >> 5;
+    if (wg & 31u) return;
+    const uint32_t t = wg + (gl & 31u);
+    if (t < n) st_vec(&totinv[t], fp_inv_fast(ld_vec(&tot[t])));
+}
+
+// Cooperative form of run_tree_rounds: every round of the tree in one launch,
+// the passes and the inversion between them separated by grid barriers.  The
+// phase's arguments stay in the kernel's parameters (only the round's lists
+// change from round to round), so the passes compile as in their own kernels.
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_tree(FlatArgs a, const G1A *first_src, G1A *buf0,
+                                                               G1A *buf1, uint32_t m, uint32_t stop, GridSync g) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    RoundIO io{first_src, buf0};
+    bool first = FIRST;
+    while (m > stop) {
+        if (FIRST && first) coop_flat_pass1<true>(a, io, m, gl, NL);
+        else coop_flat_pass1<false>(a, io, m, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
+        if (!grid_sync(g)) return;
+        if (FIRST && first) coop_flat_pass2<true>(a, io, m, gl, NL);
+        else coop_flat_pass2<false>(a, io, m, gl, NL);
+        io.src = io.dst;
+        io.dst = io.dst == buf0 ? buf1 : buf0;
+        m = (m + 1) >> 1;
+        first = false;
+        if (m > stop && !grid_sync(g)) return;
+    }
+}
+
+// the buffer holding the lists after run_tree_rounds' rounds from m down to stop
+const G1A *tree_result(const G1A *first_src, uint32_t *m_io, uint32_t stop, G1A *buf0, G1A *buf1) {
+    uint32_t m = *m_io;
+    const G1A *cur = first_src;
+    int out = 0;
+    while (m > stop) {
+        cur = out ? buf1 : buf0;
+        out ^= 1;
+        m = (m + 1) >> 1;
+    }
+    *m_io = m;
+    return cur;
+}
+
+// a launch with every block resident at once (cudaLaunchAttributeCooperative),
+// so that grid barriers inside it complete; capturable into a CUDA graph
+template <typename... KArgs, typename... Args>
+cudaError_t launch_coop(void (*kernel)(KArgs...), int blocks, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(kFlatThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// polls of a grid barrier before it gives up: far above any round's duration
+constexpr uint32_t kSyncSpinLimit = 1u << 24;
+
+GridSync make_sync(const ProofWork &w, int n) {
+    GridSync g;
+    g.word = w.sync;
+    g.err = w.err;
+    g.n_err = (uint32_t)n;
+    g.spin_limit = kSyncSpinLimit;
+    g.expected = (uint32_t)w.flat_blocks;
+    return g;
+}
+
 // Phase A of plan 3 for n blobs: digits, tree rounds, Jacobian outputs in
 // w.points.  Returns the number of kernels launched.
 int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
@@ -848,8 +968,16 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     int launched = 1;
     k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
     uint32_t m = (uint32_t)L;
-    const G1A *res =
-        run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s, &launched);
+    const G1A *res;
+    if (w.coop) {
+        launch_coop(k_coop_tree<true>, w.flat_blocks, 0, s, a, (const G1A *)nullptr, w.flat_buf[0], w.flat_buf[1],
+                    m, kTreeTail, make_sync(w, n));
+        res = tree_result(nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1]);
+        launched++;
+    } else {
+        res = run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s,
+                                    &launched);
+    }
     k_flat_finish<<<(2 * lists + 63) / 64, 64, 0, s>>>(res, m, w.points, lists);
     return launched + 1;
 }
@@ -986,7 +1114,7 @@ __device__ __forceinline__ const G1A *flatb_src(const FlatBArgs &a, const FlatBR
 
 // element e of bucket k of output o (part q)
 template <bool FIRST>
-__device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
+__device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, RoundIO io, const FlatBRound &sr, const uint32_t *items,
                                           const uint32_t *offs, uint32_t o, int q, int k, uint32_t e) {
     if (FIRST) {
         const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
@@ -996,12 +1124,12 @@ __device__ __forceinline__ G1A flatb_load(const FlatBArgs &a, const FlatBRound &
         if (((packed >> 16) & 1u) != (sr.nega[q] && tap > (int)aa)) pt.y = fp_neg(pt.y);
         return pt;
     }
-    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e]);
+    return ld_vec(&io.src[(size_t)o * sr.stride + sr.base[q][k] + e]);
 }
 
 // the x coordinate of flatb_load's point
 template <bool FIRST>
-__device__ __forceinline__ Fp flatb_load_x(const FlatBArgs &a, const FlatBRound &sr, const uint32_t *items,
+__device__ __forceinline__ Fp flatb_load_x(const FlatBArgs &a, RoundIO io, const FlatBRound &sr, const uint32_t *items,
                                            const uint32_t *offs, uint32_t o, int q, int k, uint32_t e) {
     if (FIRST) {
         const uint32_t packed = items[kDigits * sr.off[q] + offs[q * (kBuckets + 1) + k] + e];
@@ -1009,7 +1137,7 @@ __device__ __forceinline__ Fp flatb_load_x(const FlatBArgs &a, const FlatBRound 
         const uint32_t b = o / kCells, aa = o % kCells - sr.off[q];
         return ld_vec(&flatb_src(a, sr, b, q, (aa - (uint32_t)tap) & (sr.size[q] - 1), d)->x);
     }
-    return ld_vec(&a.src[(size_t)o * sr.stride + sr.base[q][k] + e].x);
+    return ld_vec(&io.src[(size_t)o * sr.stride + sr.base[q][k] + e].x);
 }
 
 // pair p of the round -> output, part, bucket, index
@@ -1027,12 +1155,11 @@ __device__ __forceinline__ void flatb_pair(const FlatBRound &sr, uint32_t p, uin
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, int r) {
-    extern __shared__ uint4 dyn_smem[];
+__device__ __forceinline__ void flatb_pass1_body(const FlatBArgs &a, RoundIO io, int r, uint4 *dyn_smem, uint32_t gl,
+                                                 uint32_t NL) {
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
     uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + kPartItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
     const uint32_t P = sr.pair_end[sr.n_parts - 1];
     uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
@@ -1042,22 +1169,28 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, in
         uint32_t o, i;
         int q, k;
         flatb_pair(sr, p, o, q, k, i);
-        const Fp x = flatb_load_x<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
-        const Fp y = flatb_load_x<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
+        const Fp x = flatb_load_x<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i);
+        const Fp y = flatb_load_x<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i + 1);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i); },
-                                             [&] { return flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1); }));
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flatb_load<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i); },
+                                             [&] { return flatb_load<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i + 1); }));
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, int r) {
     extern __shared__ uint4 dyn_smem[];
+    flatb_pass1_body<FIRST>(a, RoundIO{a.src, a.dst}, r, dyn_smem, blockIdx.x * blockDim.x + threadIdx.x,
+                            gridDim.x * blockDim.x);
+}
+
+template <bool FIRST>
+__device__ __forceinline__ void flatb_pass2_body(const FlatBArgs &a, RoundIO io, int r, uint4 *dyn_smem, uint32_t gl,
+                                                 uint32_t NL) {
     FlatBRound &sr = *reinterpret_cast<FlatBRound *>(dyn_smem);
     uint32_t *items = reinterpret_cast<uint32_t *>(&sr + 1), *offs = items + kPartItemsMax;
     flatb_stage<FIRST>(a, r, sr, items, offs);
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
     const uint32_t P = sr.pair_end[sr.n_parts - 1];
     const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
@@ -1069,13 +1202,13 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
         uint32_t o, i;
         int q, k;
         flatb_pair(sr, p, o, q, k, i);
-        const G1A x = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i);
-        const G1A y = flatb_load<FIRST>(a, sr, items, offs, o, q, k, 2 * i + 1);
+        const G1A x = flatb_load<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i);
+        const G1A y = flatb_load<FIRST>(a, io, sr, items, offs, o, q, k, 2 * i + 1);
         const int kind = pair_kind(x, y);
         const Fp den = pair_denominator(x, y, kind);
         const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
         inv = fp_mul(inv, den);
-        G1A *d = last ? &a.bucket_aff[(size_t)o * kBuckets + k] : &a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + i];
+        G1A *d = last ? &a.bucket_aff[(size_t)o * kBuckets + k] : &io.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + i];
         st_vec(d, pair_result(x, y, kind, inv_den));
     }
     // odd last elements move up unchanged
@@ -1094,8 +1227,8 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
             const uint32_t o = (ol / m) * kCells + sr.off[q] + ol % m;
             const uint32_t c = sr.cnt[q][k];
             G1A *d = last ? &a.bucket_aff[(size_t)o * kBuckets + k]
-                          : &a.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + (c >> 1)];
-            st_vec(d, flatb_load<FIRST>(a, sr, items, offs, o, q, k, c - 1));
+                          : &io.dst[(size_t)o * sr.stride_next + sr.base_next[q][k] + (c >> 1)];
+            st_vec(d, flatb_load<FIRST>(a, io, sr, items, offs, o, q, k, c - 1));
         }
         odd_begin += odd_q;
     }
@@ -1117,6 +1250,13 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, in
             e_begin += e_q;
         }
     }
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, int r) {
+    extern __shared__ uint4 dyn_smem[];
+    flatb_pass2_body<FIRST>(a, RoundIO{a.src, a.dst}, r, dyn_smem, blockIdx.x * blockDim.x + threadIdx.x,
+                            gridDim.x * blockDim.x);
 }
 
 // The shared pair sums of phase B as one grid-wide round: point m of blob b is
@@ -1147,8 +1287,7 @@ __device__ __forceinline__ void deriv_pair(const DerivArgs &a, uint32_t p, const
     neg_b = (ty.neg != 0) != (wrap && a.parts.nega[ty.part]);
 }
 
-__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass1(DerivArgs a) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void deriv_pass1_body(const DerivArgs &a, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     const uint32_t P = (uint32_t)a.n_blobs * a.points;
     uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
@@ -1168,9 +1307,11 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass1(DerivArgs a) {
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
+__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass1(DerivArgs a) {
+    deriv_pass1_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
-__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass2(DerivArgs a) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void deriv_pass2_body(const DerivArgs &a, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     const uint32_t P = (uint32_t)a.n_blobs * a.points;
     const uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
@@ -1191,10 +1332,12 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass2(DerivArgs a) {
         st_vec(&a.out[p], pair_result(x, y, kind, inv_den));
     }
 }
+__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass2(DerivArgs a) {
+    deriv_pass2_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
 // the shared pair sums into w.deriv_buf; returns the launches made (0 without any)
-int launch_deriv_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
-    if (!t.deriv_points) return 0;
+DerivArgs deriv_args(const DeviceTables &t, const ProofWork &w, int n) {
     DerivArgs a;
     a.types = t.deriv;
     a.type_of = t.deriv_of;
@@ -1208,6 +1351,12 @@ int launch_deriv_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStre
     a.totinv = w.flat_totinv;
     a.slots_pre = w.flat_slots;
     a.n_blobs = n;
+    return a;
+}
+
+int launch_deriv_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    if (!t.deriv_points) return 0;
+    const DerivArgs a = deriv_args(t, w, n);
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     k_deriv_pass1<<<blocks, kFlatThreads, 0, s>>>(a);
     k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
@@ -1216,7 +1365,7 @@ int launch_deriv_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStre
 }
 
 // Phase B of plan 3 into w.bucket_aff; returns the number of kernels launched.
-int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+FlatBArgs flatb_args(const DeviceTables &t, const ProofWork &w, int n) {
     FlatBArgs a;
     a.plan = t.fb_plan;
     a.ladder_aff = w.ladder_aff;
@@ -1232,6 +1381,58 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
     a.totinv = w.flat_totinv;
     a.slots = w.flat_slots;
     a.n_blobs = n;
+    return a;
+}
+
+VKZG_COOP_FN void coop_deriv_pass1(DerivArgs a, uint32_t gl, uint32_t NL) { deriv_pass1_body(a, gl, NL); }
+VKZG_COOP_FN void coop_deriv_pass2(DerivArgs a, uint32_t gl, uint32_t NL) { deriv_pass2_body(a, gl, NL); }
+template <bool FIRST>
+VKZG_COOP_FN void coop_flatb_pass1(FlatBArgs a, RoundIO io, int r, uint4 *smem, uint32_t gl, uint32_t NL) {
+    flatb_pass1_body<FIRST>(a, io, r, smem, gl, NL);
+}
+template <bool FIRST>
+VKZG_COOP_FN void coop_flatb_pass2(FlatBArgs a, RoundIO io, int r, uint4 *smem, uint32_t gl, uint32_t NL) {
+    flatb_pass2_body<FIRST>(a, io, r, smem, gl, NL);
+}
+
+// Cooperative form of the shared pair sums and phase B's rounds: one launch,
+// grid barriers between the passes (the arguments stay in the kernel's
+// parameters; only the round's lists change).
+__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_phase_b(DerivArgs da, int has_deriv, FlatBArgs fa,
+                                                                  G1A *buf0, G1A *buf1, int rounds, GridSync g) {
+    extern __shared__ uint4 dyn_smem[];
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    if (has_deriv) {
+        coop_deriv_pass1(da, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_invert(da.tot, da.totinv, NL >> 5, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_deriv_pass2(da, gl, NL);
+        if (!grid_sync(g)) return;
+    }
+    RoundIO io{nullptr, buf0};
+    for (int r = 0; r < rounds; r++) {
+        if (r == 0) coop_flatb_pass1<true>(fa, io, r, dyn_smem, gl, NL);
+        else coop_flatb_pass1<false>(fa, io, r, dyn_smem, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_invert(fa.tot, fa.totinv, NL >> 5, gl, NL);
+        if (!grid_sync(g)) return;
+        if (r == 0) coop_flatb_pass2<true>(fa, io, r, dyn_smem, gl, NL);
+        else coop_flatb_pass2<false>(fa, io, r, dyn_smem, gl, NL);
+        io.src = io.dst;
+        io.dst = io.dst == buf0 ? buf1 : buf0;
+        if (r + 1 < rounds && !grid_sync(g)) return;
+    }
+}
+
+int launch_phase_b_coop(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    launch_coop(k_coop_phase_b, w.flat_blocks, kFlatBSmem, s, deriv_args(t, w, n), t.deriv_points ? 1 : 0,
+                flatb_args(t, w, n), w.flatb_buf[0], w.flatb_buf[1], t.fb_rounds, make_sync(w, n));
+    return 1;
+}
+
+int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaStream_t s) {
+    FlatBArgs a = flatb_args(t, w, n);
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     G1A *bufs[2] = {w.flatb_buf[0], w.flatb_buf[1]};
     const G1A *cur = nullptr;
@@ -1575,10 +1776,8 @@ __device__ void red_stage(RedRound &rr, int r) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, int r) {
-    __shared__ RedRound rr;
+__device__ __forceinline__ void flatr_pass1_body(const FlatRArgs &a, int r, RedRound &rr, uint32_t gl, uint32_t NL) {
     red_stage(rr, r);
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
     const uint32_t nops = (uint32_t)rr.nops;
     const uint32_t P = (uint32_t)a.n_out * nops;
@@ -1594,11 +1793,13 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, in
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
-
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, int r) {
     __shared__ RedRound rr;
+    flatr_pass1_body(a, r, rr, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+__device__ __forceinline__ void flatr_pass2_body(const FlatRArgs &a, int r, RedRound &rr, uint32_t gl, uint32_t NL) {
     red_stage(rr, r);
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     const uint32_t wg = gl >> 5;
     const uint32_t nops = (uint32_t)rr.nops;
     const uint32_t P = (uint32_t)a.n_out * nops;
@@ -1616,6 +1817,10 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, in
         st_vec(red_slot(a, o, rr.d[q]), pair_result(x, y, kind, inv_den));
     }
 }
+__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, int r) {
+    __shared__ RedRound rr;
+    flatr_pass2_body(a, r, rr, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
 // H = sum_b 2^b T_b (Horner over the 7 bit sums), then + S: the reduction's result.
 // One thread per output: at 7.5 M products per 256 blobs the step is near the
@@ -1625,6 +1830,28 @@ __global__ void __launch_bounds__(128) k_flatr_horner(FlatRArgs a, G1J *out) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= (uint32_t)a.n_out) return;
     st_vec(&out[o], red_horner([&](int x) { return ld_vec(red_slot(a, o, x)); }));
+}
+
+VKZG_COOP_FN void coop_flatr_pass1(FlatRArgs a, int r, RedRound &rr, uint32_t gl, uint32_t NL) {
+    flatr_pass1_body(a, r, rr, gl, NL);
+}
+VKZG_COOP_FN void coop_flatr_pass2(FlatRArgs a, int r, RedRound &rr, uint32_t gl, uint32_t NL) {
+    flatr_pass2_body(a, r, rr, gl, NL);
+}
+
+// Cooperative form of the reduction's rounds (the Horner step stays its own
+// launch: one output per thread, a different register budget).
+__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_reduce(FlatRArgs a, int rounds, GridSync g) {
+    __shared__ RedRound rr;
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    for (int r = 0; r < rounds; r++) {
+        coop_flatr_pass1(a, r, rr, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_flatr_pass2(a, r, rr, gl, NL);
+        if (r + 1 < rounds && !grid_sync(g)) return;
+    }
 }
 
 int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_out, cudaStream_t s) {
@@ -1644,13 +1871,20 @@ int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_o
     a.slots_pre = w.flat_slots;
     a.n_out = n_out;
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
-    for (int r = 0; r < rounds; r++) {
-        k_flatr_pass1<<<blocks, kFlatThreads, 0, s>>>(a, r);
-        k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
-        k_flatr_pass2<<<blocks, kFlatThreads, 0, s>>>(a, r);
+    int launched = 1;
+    if (w.coop) {
+        launch_coop(k_coop_reduce, blocks, 0, s, a, rounds, make_sync(w, n_out / kCells));
+        launched += 1;
+    } else {
+        for (int r = 0; r < rounds; r++) {
+            k_flatr_pass1<<<blocks, kFlatThreads, 0, s>>>(a, r);
+            k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
+            k_flatr_pass2<<<blocks, kFlatThreads, 0, s>>>(a, r);
+        }
+        launched += 3 * rounds;
     }
     k_flatr_horner<<<(n_out + 127) / 128, 128, 0, s>>>(a, out);
-    return 3 * rounds + 1;
+    return launched;
 }
 
 // The ladder to affine form as one grid-wide round (plans 3-4): Z values dealt
@@ -1665,8 +1899,7 @@ struct NormArgs {
     uint32_t n;
 };
 
-__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass1(NormArgs a) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void norm_pass1_body(const NormArgs &a, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
     Fp acc = fp_one();
@@ -1678,9 +1911,11 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass1(NormArgs a) {
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
+__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass1(NormArgs a) {
+    norm_pass1_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
-__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
-    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+__device__ __forceinline__ void norm_pass2_body(const NormArgs &a, uint32_t gl, uint32_t NL) {
     const uint32_t wg = gl >> 5;
     const uint32_t *pre = a.pre + (size_t)wg * a.slots_pre * 384;
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
@@ -1706,8 +1941,24 @@ __global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
         st_vec(&a.out[dst + kLadderDigits], g1_phi(r));
     }
 }
+__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
+    norm_pass2_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
 // the ladder to affine form with its phi images, into w.ladder_aff; returns the launches made
+VKZG_COOP_FN void coop_norm_pass1(NormArgs a, uint32_t gl, uint32_t NL) { norm_pass1_body(a, gl, NL); }
+VKZG_COOP_FN void coop_norm_pass2(NormArgs a, uint32_t gl, uint32_t NL) { norm_pass2_body(a, gl, NL); }
+
+// Cooperative form of the ladder's normalisation round.
+__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_norm(NormArgs a, GridSync g) {
+    const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
+    coop_norm_pass1(a, gl, NL);
+    if (!grid_sync(g)) return;
+    coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
+    if (!grid_sync(g)) return;
+    coop_norm_pass2(a, gl, NL);
+}
+
 int launch_normalize_flat(const ProofWork &w, int n, cudaStream_t s) {
     const int blocks = w.flat_blocks, warps = blocks * kFlatThreads / 32;
     NormArgs na;
@@ -1719,6 +1970,10 @@ int launch_normalize_flat(const ProofWork &w, int n, cudaStream_t s) {
     na.totinv = w.flat_totinv;
     na.slots_pre = w.flat_slots;
     na.n = (uint32_t)(n * kCells * kLadderDigits);
+    if (w.coop) {
+        launch_coop(k_coop_norm, blocks, 0, s, na, make_sync(w, n));
+        return 1;
+    }
     k_norm_pass1<<<blocks, kFlatThreads, 0, s>>>(na);
     k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(na.tot, na.totinv, warps);
     k_norm_pass2<<<blocks, kFlatThreads, 0, s>>>(na);
@@ -1767,6 +2022,11 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     const bool affine = w.plan != 0 && w.ba_blocks > 0;
     const bool comb = w.plan == 3 && w.comb != nullptr && w.flat_dig != nullptr && w.ba_blocks > 0;
     const bool flatb = (w.plan == 3 || w.plan == 4) && w.flat_pre != nullptr && t.fb_rounds > 0 && w.ba_blocks > 0;
+    if (!flatb && w.coop) { // the cooperative forms serve plans 3-4 only
+        ProofWork w2 = w;
+        w2.coop = false;
+        return launch_proofs_timed(t, w2, n, s, ev, skip_front);
+    }
     const bool hier = w.plan == 1 || w.plan == 3 || w.plan == 4;
     int launched = skip_front ? 8 : 10;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
@@ -1778,6 +2038,8 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
                                                                                        w.red_scratch, n_out);
         else k_reduce_affine<<<red_blocks, kReduceThreads, 0, s>>>(w.bucket_aff, w.points, n_out);
     };
+    // the cooperative launches' barrier words start at zero each step
+    if (flatb && w.coop) cudaMemsetAsync(w.sync, 0, 4 * sizeof(uint32_t), s);
     if (comb) {
         cudaMemsetAsync(w.task_ctr, 0, 2 * sizeof(uint32_t), s);
         launched += launch_phase_a_flat(w, n, s) - 2; // no phase-A bucket kernel, no reduction
@@ -1800,7 +2062,9 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
     if (flatb) launched += launch_normalize_flat(w, n, s) - 1;
     else k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, w.ladder_aff, n_lad);
     mark();
-    if (flatb) {
+    if (flatb && w.coop) {
+        launched += launch_phase_b_coop(t, w, n, s) - 1;
+    } else if (flatb) {
         launched += launch_deriv_flat(t, w, n, s);
         launched += launch_phase_b_flat(t, w, n, s) - 1;
     } else if (affine) {
@@ -1834,6 +2098,24 @@ int batch_affine_blocks_per_sm() {
 }
 
 size_t reduce_scratch_points(int cap_blobs) { return (size_t)cap_blobs * kCells * kRedOps; }
+
+// True when every cooperative kernel of plans 3-4 fits blocks_per_sm resident
+// blocks per SM (the grid of the rounds) and the device takes cooperative launches.
+bool coop_supported(int blocks_per_sm) {
+    int dev = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+        return false;
+    int a = 0, b = 0, c = 0, d = 0;
+    if (cudaFuncSetAttribute(k_coop_phase_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlatBSmem) !=
+        cudaSuccess)
+        return false;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_coop_tree<true>, kFlatThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_coop_norm, kFlatThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_coop_phase_b, kFlatThreads, kFlatBSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_coop_reduce, kFlatThreads, 0);
+    return std::min(std::min(a, b), std::min(c, d)) >= blocks_per_sm;
+}
 
 cudaError_t configure_proof_kernels() {
     cudaError_t e = configure_reduce_schedule();

@@ -180,7 +180,8 @@ void vkzg_server::run_batch(Lane *lane) {
         const Part &part = b.parts[k];
         if (part_rc[k] == VKZG_OK) {
             for (size_t i = 0; i < part.count; i++)
-                if (lane->h_err[off + i]) part_rc[k] = b.kind == 0 ? VKZG_ERR_INVALID_BLOB : VKZG_ERR_BADARGS;
+                if (lane->h_err[off + i] & VKZG_B200_DEVICE_FAILED) part_rc[k] = VKZG_ERR_GPU;
+                else if (lane->h_err[off + i]) part_rc[k] = b.kind == 0 ? VKZG_ERR_INVALID_BLOB : VKZG_ERR_BADARGS;
         }
         if (part_rc[k] == VKZG_OK &&
             cudaMemcpyAsync(part.req->out + part.first * out_b, lane->d_out + off * out_b, part.count * out_b,
@@ -253,6 +254,7 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
         rc = vkzg_prover_new(&lane->p, &po);
         if (rc != VKZG_OK) break;
         vkzg::set_comb_budget(lane->p, s->opts.table_budget_bytes);
+        vkzg::disable_coop(lane->p);
         if (cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaMalloc(&lane->d_in, cap * kExt) != cudaSuccess || cudaMalloc(&lane->d_out, cap * kExt) != cudaSuccess ||
             cudaMalloc(&lane->d_present, cap * VKZG_NUM_CELL_PROOFS) != cudaSuccess ||
