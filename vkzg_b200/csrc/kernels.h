@@ -198,6 +198,8 @@ bool coop_supported(int blocks_per_sm);
 // no cooperative launches for this prover (a serving lane: several lanes'
 // pipelines run at once, and each cooperative launch wants the whole GPU)
 void disable_coop(vkzg_prover *p);
+// frees the buffers none of a fully tuned prover's plans uses (before any capture)
+void trim_working_set(vkzg_prover *p);
 // digit-table byte budget of a prover (before its first tuning)
 void set_comb_budget(vkzg_prover *p, uint64_t bytes);
 void precapture_graphs(vkzg_prover *p, uint32_t max_n);

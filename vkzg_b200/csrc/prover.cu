@@ -85,7 +85,7 @@ struct vkzg_prover {
     cudaStream_t stream = nullptr;
     std::mutex mutex;
     DeviceTables t;
-    std::vector<void *> allocs;
+    std::vector<std::pair<void *, size_t>> allocs;
     uint32_t cap = 0;
     ProofWork pw;
     RecoverWork rw;
@@ -114,6 +114,8 @@ struct vkzg_prover {
     // window the phase-A round buffers are sized for (they serve any wider one)
     uint64_t comb_budget = 20ull << 30;
     bool coop_off = false; // see vkzg::disable_coop
+    bool trimmed = false;  // see vkzg::trim_working_set: only the tuned plans' buffers are left
+    uint32_t plan0_cap = 0; // blobs the Jacobian bucket array holds once trimmed
     int comb_c_chosen = 0, comb_buf_c = 0;
     struct WindowTrial {
         int c;
@@ -163,7 +165,7 @@ struct vkzg_prover {
             if (x) cudaStreamDestroy(x);
         for (auto &e : side_ev)
             if (e) cudaEventDestroy(e);
-        for (void *a : allocs) cudaFree(a);
+        for (auto &a : allocs) cudaFree(a.first);
         if (h_err) cudaFreeHost(h_err);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
@@ -179,10 +181,22 @@ struct vkzg_prover {
     bool alloc(T *&ptr, size_t count) {
         void *p = nullptr;
         if (cudaMalloc(&p, count * sizeof(T) + 16) != cudaSuccess) return false;
-        allocs.push_back(p);
+        allocs.push_back({p, count * sizeof(T) + 16});
         dev_bytes += count * sizeof(T) + 16;
         ptr = reinterpret_cast<T *>(p);
         return true;
+    }
+    // frees one allocation made by alloc (the stream must be idle)
+    template <typename T>
+    void release(T *&ptr) {
+        for (auto it = allocs.begin(); it != allocs.end(); ++it)
+            if (it->first == (void *)ptr) {
+                cudaFree(it->first);
+                dev_bytes -= it->second;
+                allocs.erase(it);
+                break;
+            }
+        ptr = nullptr;
     }
 };
 
@@ -1122,9 +1136,15 @@ int planned(const vkzg_prover *p, uint32_t n) {
 // planned(), with the digit table or the grid-wide buffers made ready for plans
 // 3 and 4 (plan 1 without them)
 int plan_for(vkzg_prover *p, uint32_t n) {
-    const int plan = planned(p, n);
-    if (plan == 3 && !ensure_comb(p)) return ensure_flat_b(p) ? 4 : 1;
-    if (plan == 4 && !ensure_flat_b(p)) return 1;
+    int plan = planned(p, n);
+    if (plan == 3 && !ensure_comb(p)) plan = ensure_flat_b(p) ? 4 : 1;
+    if (plan == 4 && !ensure_flat_b(p)) plan = 1;
+    // a trimmed working set (trim_working_set) holds only the tuned plans'
+    // buffers: a plan whose buffers went is replaced by plan 3, which every
+    // trimmed prover keeps (its classes above the Jacobian buckets' size run it)
+    if (p->trimmed && (((plan == 1 || plan == 2 || plan == 4) && !p->pw.ba_scratch) ||
+                       (plan == 0 && n > p->plan0_cap)))
+        plan = 3;
     return plan;
 }
 
@@ -1649,6 +1669,40 @@ void disable_coop(vkzg_prover *p) {
     std::lock_guard<std::mutex> lock(p->mutex);
     p->coop_off = true;
     p->pw.coop = false;
+}
+
+// Frees the buffers that none of the prover's tuned plans uses, so that its
+// working set per blob (a serving lane's admission charge) covers only them:
+// the per-warp batch-affine scratch when no size class runs plan 1, 2 or 4,
+// and the Jacobian bucket array beyond the largest class that runs plan 0.
+// Every size class up to the capacity must be tuned (a serving lane's are) and
+// no pipeline captured yet; a prover with a forced plan keeps everything.
+void trim_working_set(vkzg_prover *p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(p->mutex);
+    if (p->plan_forced >= 0 || p->plan_of.empty() || !p->graphs.empty()) return;
+    for (uint32_t c = 1; c < p->cap; c <<= 1)
+        if (!p->plan_of.count(c)) return;
+    if (!p->plan_of.count(size_class(p->cap))) return;
+    if (cudaSetDevice(p->device) != cudaSuccess || cudaStreamSynchronize(p->stream) != cudaSuccess) return;
+    bool batch_affine = false;
+    uint32_t plan0 = 0;
+    for (const auto &kv : p->plan_of) {
+        batch_affine |= kv.second == 1 || kv.second == 2 || kv.second == 4;
+        if (kv.second == 0) plan0 = std::max(plan0, std::min(kv.first, p->cap));
+    }
+    ProofWork &w = p->pw;
+    // plan 3 stands in for any plan whose buffers go (plan_for): keep them all
+    // unless the digit table and its buffers are in place
+    if (!p->comb || !w.flat_dig || !w.flat_pre) return;
+    if (!batch_affine && w.ba_scratch) p->release(w.ba_scratch);
+    p->plan0_cap = p->cap;
+    if (plan0 < p->cap && w.buckets) {
+        p->release(w.buckets);
+        p->plan0_cap = 0;
+        if (plan0 && p->alloc(w.buckets, (size_t)plan0 * kCells * kBuckets)) p->plan0_cap = plan0;
+    }
+    p->trimmed = true;
 }
 
 void set_comb_budget(vkzg_prover *p, uint64_t bytes) {

@@ -276,6 +276,8 @@ vkzg_result vkzg_b200_server_new(vkzg_server **out, const vkzg_server_options *o
         return VKZG_ERR_GPU;
     }
     for (auto &l : s->lanes) vkzg::adopt_tuning(l->p, s->lanes[0]->p);
+    // then each lane keeps only its tuned plans' buffers (its per-blob charge below)
+    for (auto &l : s->lanes) vkzg::trim_working_set(l->p);
     // and capture every batch size's proof pipeline on every lane: a capture on
     // first use would hold up the request that meets it
     for (auto &l : s->lanes) vkzg::precapture_graphs(l->p, cap);
