@@ -673,8 +673,96 @@ __device__ __forceinline__ void pair_step_down(uint32_t &o, uint32_t &i, uint32_
     }
 }
 
+// ---- round 1's digit-table gathers, prefetched one pair ahead
+// In the first round every point is a random 96-byte read from a table of tens
+// of GB; with a pair's loads issued only when the pair is reached, the lanes
+// waited on them (fewer than a quarter of the warps are resident).  Each
+// thread instead stages the points of its next pair in shared memory with
+// cp.async while it computes the current pair.  The staging is chunk-major,
+// [buffer][16-byte chunk][thread], so a warp's reads of one chunk are one
+// contiguous 512-byte run (no bank conflicts).
+constexpr int kStageChunks = 12; // two 96-byte points
+constexpr size_t kStage1Bytes = 2 * 6 * kFlatThreads * sizeof(uint4);            // pass 1: x coordinates
+constexpr size_t kStage2Bytes = 2 * kStageChunks * kFlatThreads * sizeof(uint4); // pass 2: whole points
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// the digit-table entry of digit v (nonzero) of element t of list o
+__device__ __forceinline__ const uint4 *comb_entry(const FlatArgs &a, uint32_t o, uint32_t t, int v) {
+    return reinterpret_cast<const uint4 *>(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)]);
+}
+
+// pass 1 of the first round: the x coordinates of each pair staged one pair ahead
+__device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, uint32_t gl, uint32_t NL) {
+    extern __shared__ uint4 stage[];
+    uint4 *my = stage + threadIdx.x; // chunk c of buffer b: my[(b * 6 + c) * kFlatThreads]
+    const uint32_t wg = gl >> 5;
+    const uint32_t h = m >> 1;
+    const uint32_t P = (uint32_t)a.n_lists * h;
+    const uint32_t dq = NL / h, dr = NL % h;
+    uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
+    const RoundIO io{nullptr, nullptr};
+    auto issue = [&](int b, uint32_t o, uint32_t i, int &v0, int &v1) {
+        const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
+        v0 = d[0];
+        v1 = d[1];
+        if (v0) {
+            const uint4 *src = comb_entry(a, o, 2 * i, v0);
+            for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + c) * kFlatThreads], src + c);
+        }
+        if (v1) {
+            const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
+            for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + 3 + c) * kFlatThreads], src + c);
+        }
+        cp_async_commit();
+    };
+    auto x_of = [&](int b, int half, int v) {
+        Fp x;
+        if (v == 0) return fp_zero();
+        uint4 *w = reinterpret_cast<uint4 *>(&x);
+        for (int c = 0; c < 3; c++) w[c] = my[(b * 6 + 3 * half + c) * kFlatThreads];
+        return x;
+    };
+    Fp acc = fp_one();
+    int s = 0, v0 = 0, v1 = 0;
+    uint32_t o = gl / h, i = gl % h;
+    if (gl < P) issue(0, o, i, v0, v1);
+    for (uint32_t p = gl; p < P; p += NL, s++) {
+        uint32_t on = o, in = i;
+        int w0 = 0, w1 = 0;
+        if (p + NL < P) {
+            pair_step_up(on, in, h, dq, dr);
+            issue((s + 1) & 1, on, in, w0, w1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        const Fp x = x_of(s & 1, 0, v0), y = x_of(s & 1, 1, v1);
+        wb_store_pre(pre, s, acc);
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<true>(a, io, o, 2 * i, m); },
+                                             [&] { return flat_load<true>(a, io, o, 2 * i + 1, m); }));
+        o = on;
+        i = in;
+        v0 = w0;
+        v1 = w1;
+    }
+    flat_pass1_products(acc, a.others, a.tot, gl, wg);
+}
+
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass1_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+    if constexpr (FIRST) {
+        flat_pass1_first(a, m, gl, NL);
+        return;
+    }
     const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1;
     const uint32_t P = (uint32_t)a.n_lists * h;
@@ -716,8 +804,83 @@ __global__ void __launch_bounds__(64) k_flat_invert(const Fp *tot, Fp *totinv, i
 #define VKZG_PASS2_INLINE 0
 #endif
 constexpr bool kPass2Inline = VKZG_PASS2_INLINE != 0;
+// pass 2 of the first round: the two points of each pair staged one pair ahead
+__device__ __forceinline__ void flat_pass2_first(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+    extern __shared__ uint4 stage[];
+    uint4 *my = stage + threadIdx.x; // chunk c of buffer b: my[(b * kStageChunks + c) * kFlatThreads]
+    const uint32_t wg = gl >> 5;
+    const uint32_t h = m >> 1, m_next = (m + 1) >> 1;
+    const uint32_t P = (uint32_t)a.n_lists * h;
+    const uint32_t dq = NL / h, dr = NL % h;
+    const uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
+    Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
+    const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
+    auto issue = [&](int b, uint32_t o, uint32_t i, int &v0, int &v1) {
+        const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
+        v0 = d[0];
+        v1 = d[1];
+        if (v0) {
+            const uint4 *src = comb_entry(a, o, 2 * i, v0);
+            for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + c) * kFlatThreads], src + c);
+        }
+        if (v1) {
+            const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
+            for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + 6 + c) * kFlatThreads], src + c);
+        }
+        cp_async_commit();
+    };
+    auto point = [&](int b, int half, int v) {
+        G1A pt;
+        if (v == 0) {
+            pt.x = fp_zero();
+            pt.y = fp_zero();
+            return pt;
+        }
+        uint4 *w = reinterpret_cast<uint4 *>(&pt);
+        for (int c = 0; c < 6; c++) w[c] = my[(b * kStageChunks + 6 * half + c) * kFlatThreads];
+        if (v < 0) pt.y = fp_neg(pt.y);
+        return pt;
+    };
+    uint32_t o = 0, i = 0;
+    int v0 = 0, v1 = 0;
+    if (S > 0) {
+        const uint32_t p_last = gl + (uint32_t)(S - 1) * NL;
+        o = p_last / h;
+        i = p_last % h;
+        issue((S - 1) & 1, o, i, v0, v1);
+    }
+    for (int t = S - 1; t >= 0; t--) {
+        uint32_t on = o, in = i;
+        int w0 = 0, w1 = 0;
+        if (t > 0) {
+            pair_step_down(on, in, h, dq, dr);
+            issue((t - 1) & 1, on, in, w0, w1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        const G1A x = point(t & 1, 0, v0), y = point(t & 1, 1, v1);
+        const int kind = pair_kind(x, y);
+        const Fp den = pair_denominator(x, y, kind);
+        const Fp inv_den = pmul<kPass2Inline>(inv, wb_load_pre(pre, t));
+        inv = pmul<kPass2Inline>(inv, den);
+        st_vec(&io.dst[(size_t)o * m_next + i], pair_result<kPass2Inline>(x, y, kind, inv_den));
+        o = on;
+        i = in;
+        v0 = w0;
+        v1 = w1;
+    }
+    if (m & 1u)
+        for (uint32_t l = gl; l < (uint32_t)a.n_lists; l += NL)
+            st_vec(&io.dst[(size_t)l * m_next + h], flat_load<true>(a, io, l, m - 1, m));
+}
+
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass2_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+    if constexpr (FIRST) {
+        flat_pass2_first(a, io, m, gl, NL);
+        return;
+    }
     const uint32_t wg = gl >> 5;
     const uint32_t h = m >> 1, m_next = (m + 1) >> 1;
     const uint32_t P = (uint32_t)a.n_lists * h;
@@ -811,10 +974,10 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t *m_io, uin
     while (m > stop) {
         a.src = cur;
         a.dst = bufs[out];
-        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, FIRST ? kStage1Bytes : 0, s>>>(a, m);
         else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
         k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
-        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, FIRST ? kStage2Bytes : 0, s>>>(a, m);
         else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
         *launched += 3;
         cur = bufs[out];
@@ -970,8 +1133,8 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     uint32_t m = (uint32_t)L;
     const G1A *res;
     if (w.coop) {
-        launch_coop(k_coop_tree<true>, w.flat_blocks, 0, s, a, (const G1A *)nullptr, w.flat_buf[0], w.flat_buf[1],
-                    m, kTreeTail, make_sync(w, n));
+        launch_coop(k_coop_tree<true>, w.flat_blocks, kStage2Bytes, s, a, (const G1A *)nullptr, w.flat_buf[0],
+                    w.flat_buf[1], m, kTreeTail, make_sync(w, n));
         res = tree_result(nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1]);
         launched++;
     } else {
@@ -2110,7 +2273,10 @@ bool coop_supported(int blocks_per_sm) {
     if (cudaFuncSetAttribute(k_coop_phase_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlatBSmem) !=
         cudaSuccess)
         return false;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_coop_tree<true>, kFlatThreads, 0);
+    if (cudaFuncSetAttribute(k_coop_tree<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage2Bytes) !=
+        cudaSuccess)
+        return false;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_coop_tree<true>, kFlatThreads, kStage2Bytes);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_coop_norm, kFlatThreads, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_coop_phase_b, kFlatThreads, kFlatBSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_coop_reduce, kFlatThreads, 0);
@@ -2124,6 +2290,10 @@ cudaError_t configure_proof_kernels() {
                                          (int)(kBlobElems * sizeof(Fr)));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_phase_a_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBASmem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_flat_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage1Bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_flat_pass2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage2Bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_phase_b_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseBSmem);
 }
