@@ -771,10 +771,20 @@ def main():
             for _ in range(args.steps):
                 assert prover.compute_cells_raw(out, blobs, args.blobs) == 0
         else:
+            # device buffers: one launch of all the blobs (host buffers of 16
+            # blobs or more would be staged in slices)
+            import torch
             cells, present = make_recovery(args.blobs, 6)
-            out = np.zeros(args.blobs * EXT, np.uint8)
+            d_cells = torch.from_numpy(cells).cuda()
+            d_present = torch.from_numpy(present).cuda()
+            d_out = torch.empty(args.blobs * EXT, dtype=torch.uint8, device="cuda")
+            d_err = torch.zeros(args.blobs, dtype=torch.int32, device="cuda")
+            sp = torch.cuda.current_stream().cuda_stream
             for _ in range(args.steps):
-                assert prover.recover_cells_raw(out, cells, present, args.blobs) == 0
+                assert prover.recover_cells_device(d_out.data_ptr(), d_cells.data_ptr(), d_present.data_ptr(),
+                                                   d_err.data_ptr(), args.blobs, sp) == 0
+            torch.cuda.synchronize()
+            assert int(d_err.count_nonzero()) == 0
         print(json.dumps({"profile_case": args.profile_case, "blobs": args.blobs, "steps": args.steps,
                           "launches": vkzg_b200.kernel_launches()}))
         return
