@@ -555,6 +555,12 @@ __device__ __forceinline__ uint32_t scalar_window(const Fr &s, int off, int c) {
 // one-lane inversion of its own, and every lane has pairs until the lists are
 // short.
 constexpr int kFlatThreads = 256;
+// resident blocks per SM of the grid-wide round kernels (their grid is this
+// many blocks per SM, and their register budget follows from it)
+#ifndef VKZG_FLAT_BLOCKS_PER_SM
+#define VKZG_FLAT_BLOCKS_PER_SM 2
+#endif
+constexpr int kFlatBlocksPerSM = VKZG_FLAT_BLOCKS_PER_SM;
 
 struct FlatArgs {
     const int16_t *dig;  // [list][64 D] signed digits
@@ -681,6 +687,10 @@ __device__ __forceinline__ void pair_step_down(uint32_t &o, uint32_t &i, uint32_
 // cp.async while it computes the current pair.  The staging is chunk-major,
 // [buffer][16-byte chunk][thread], so a warp's reads of one chunk are one
 // contiguous 512-byte run (no bank conflicts).
+#ifndef VKZG_GATHER_PREFETCH
+#define VKZG_GATHER_PREFETCH 1
+#endif
+constexpr bool kGatherPrefetch = VKZG_GATHER_PREFETCH != 0;
 constexpr int kStageChunks = 12; // two 96-byte points
 constexpr size_t kStage1Bytes = 2 * 6 * kFlatThreads * sizeof(uint4);            // pass 1: x coordinates
 constexpr size_t kStage2Bytes = 2 * kStageChunks * kFlatThreads * sizeof(uint4); // pass 2: whole points
@@ -759,7 +769,7 @@ __device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, 
 
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass1_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
-    if constexpr (FIRST) {
+    if constexpr (FIRST && kGatherPrefetch) {
         flat_pass1_first(a, m, gl, NL);
         return;
     }
@@ -782,7 +792,7 @@ __device__ __forceinline__ void flat_pass1_body(const FlatArgs &a, RoundIO io, u
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass1(FlatArgs a, uint32_t m) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flat_pass1(FlatArgs a, uint32_t m) {
     flat_pass1_body<FIRST>(a, RoundIO{a.src, a.dst}, m, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -877,7 +887,7 @@ __device__ __forceinline__ void flat_pass2_first(const FlatArgs &a, RoundIO io, 
 
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass2_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
-    if constexpr (FIRST) {
+    if constexpr (FIRST && kGatherPrefetch) {
         flat_pass2_first(a, io, m, gl, NL);
         return;
     }
@@ -909,7 +919,7 @@ __device__ __forceinline__ void flat_pass2_body(const FlatArgs &a, RoundIO io, u
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flat_pass2(FlatArgs a, uint32_t m) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flat_pass2(FlatArgs a, uint32_t m) {
     flat_pass2_body<FIRST>(a, RoundIO{a.src, a.dst}, m, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -940,7 +950,7 @@ int flat_blocks() {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms * 2;
+    return sms * kFlatBlocksPerSM;
 }
 
 // Working set of the grid-wide rounds for cap blobs and window c.
@@ -974,10 +984,10 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t *m_io, uin
     while (m > stop) {
         a.src = cur;
         a.dst = bufs[out];
-        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, FIRST ? kStage1Bytes : 0, s>>>(a, m);
+        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, FIRST && kGatherPrefetch ? kStage1Bytes : 0, s>>>(a, m);
         else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
         k_flat_invert<<<(warps + 63) / 64, 64, 0, s>>>(a.tot, a.totinv, warps);
-        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, FIRST ? kStage2Bytes : 0, s>>>(a, m);
+        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, FIRST && kGatherPrefetch ? kStage2Bytes : 0, s>>>(a, m);
         else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
         *launched += 3;
         cur = bufs[out];
@@ -1046,7 +1056,7 @@ __device__ __noinline__ void coop_invert(const Fp *tot, Fp *totinv, uint32_t n, 
 // phase's arguments stay in the kernel's parameters (only the round's lists
 // change from round to round), so the passes compile as in their own kernels.
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_tree(FlatArgs a, const G1A *first_src, G1A *buf0,
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_tree(FlatArgs a, const G1A *first_src, G1A *buf0,
                                                                G1A *buf1, uint32_t m, uint32_t stop, GridSync g) {
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     RoundIO io{first_src, buf0};
@@ -1342,7 +1352,7 @@ __device__ __forceinline__ void flatb_pass1_body(const FlatBArgs &a, RoundIO io,
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass1(FlatBArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flatb_pass1(FlatBArgs a, int r) {
     extern __shared__ uint4 dyn_smem[];
     flatb_pass1_body<FIRST>(a, RoundIO{a.src, a.dst}, r, dyn_smem, blockIdx.x * blockDim.x + threadIdx.x,
                             gridDim.x * blockDim.x);
@@ -1416,7 +1426,7 @@ __device__ __forceinline__ void flatb_pass2_body(const FlatBArgs &a, RoundIO io,
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatb_pass2(FlatBArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flatb_pass2(FlatBArgs a, int r) {
     extern __shared__ uint4 dyn_smem[];
     flatb_pass2_body<FIRST>(a, RoundIO{a.src, a.dst}, r, dyn_smem, blockIdx.x * blockDim.x + threadIdx.x,
                             gridDim.x * blockDim.x);
@@ -1470,7 +1480,7 @@ __device__ __forceinline__ void deriv_pass1_body(const DerivArgs &a, uint32_t gl
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass1(DerivArgs a) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_deriv_pass1(DerivArgs a) {
     deriv_pass1_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -1495,7 +1505,7 @@ __device__ __forceinline__ void deriv_pass2_body(const DerivArgs &a, uint32_t gl
         st_vec(&a.out[p], pair_result(x, y, kind, inv_den));
     }
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_deriv_pass2(DerivArgs a) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_deriv_pass2(DerivArgs a) {
     deriv_pass2_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -1561,7 +1571,7 @@ VKZG_COOP_FN void coop_flatb_pass2(FlatBArgs a, RoundIO io, int r, uint4 *smem, 
 // Cooperative form of the shared pair sums and phase B's rounds: one launch,
 // grid barriers between the passes (the arguments stay in the kernel's
 // parameters; only the round's lists change).
-__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_phase_b(DerivArgs da, int has_deriv, FlatBArgs fa,
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_phase_b(DerivArgs da, int has_deriv, FlatBArgs fa,
                                                                   G1A *buf0, G1A *buf1, int rounds, GridSync g) {
     extern __shared__ uint4 dyn_smem[];
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
@@ -1956,7 +1966,7 @@ __device__ __forceinline__ void flatr_pass1_body(const FlatRArgs &a, int r, RedR
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass1(FlatRArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flatr_pass1(FlatRArgs a, int r) {
     __shared__ RedRound rr;
     flatr_pass1_body(a, r, rr, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
@@ -1980,7 +1990,7 @@ __device__ __forceinline__ void flatr_pass2_body(const FlatRArgs &a, int r, RedR
         st_vec(red_slot(a, o, rr.d[q]), pair_result(x, y, kind, inv_den));
     }
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_flatr_pass2(FlatRArgs a, int r) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flatr_pass2(FlatRArgs a, int r) {
     __shared__ RedRound rr;
     flatr_pass2_body(a, r, rr, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
@@ -2004,7 +2014,7 @@ VKZG_COOP_FN void coop_flatr_pass2(FlatRArgs a, int r, RedRound &rr, uint32_t gl
 
 // Cooperative form of the reduction's rounds (the Horner step stays its own
 // launch: one output per thread, a different register budget).
-__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_reduce(FlatRArgs a, int rounds, GridSync g) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_reduce(FlatRArgs a, int rounds, GridSync g) {
     __shared__ RedRound rr;
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     for (int r = 0; r < rounds; r++) {
@@ -2074,7 +2084,7 @@ __device__ __forceinline__ void norm_pass1_body(const NormArgs &a, uint32_t gl, 
     }
     flat_pass1_products(acc, a.others, a.tot, gl, wg);
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass1(NormArgs a) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_norm_pass1(NormArgs a) {
     norm_pass1_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -2104,7 +2114,7 @@ __device__ __forceinline__ void norm_pass2_body(const NormArgs &a, uint32_t gl, 
         st_vec(&a.out[dst + kLadderDigits], g1_phi(r));
     }
 }
-__global__ void __launch_bounds__(kFlatThreads, 2) k_norm_pass2(NormArgs a) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_norm_pass2(NormArgs a) {
     norm_pass2_body(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -2113,7 +2123,7 @@ VKZG_COOP_FN void coop_norm_pass1(NormArgs a, uint32_t gl, uint32_t NL) { norm_p
 VKZG_COOP_FN void coop_norm_pass2(NormArgs a, uint32_t gl, uint32_t NL) { norm_pass2_body(a, gl, NL); }
 
 // Cooperative form of the ladder's normalisation round.
-__global__ void __launch_bounds__(kFlatThreads, 2) k_coop_norm(NormArgs a, GridSync g) {
+__global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_norm(NormArgs a, GridSync g) {
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     coop_norm_pass1(a, gl, NL);
     if (!grid_sync(g)) return;
