@@ -576,6 +576,14 @@ struct FlatArgs {
     int n_lists;
 };
 
+// Entry idx of the digit table (kCombEntryBytes apart).
+__host__ __device__ __forceinline__ const G1A *comb_at(const G1A *comb, size_t idx) {
+    return reinterpret_cast<const G1A *>(reinterpret_cast<const char *>(comb) + idx * kCombEntryBytes);
+}
+__host__ __device__ __forceinline__ G1A *comb_at(G1A *comb, size_t idx) {
+    return reinterpret_cast<G1A *>(reinterpret_cast<char *>(comb) + idx * kCombEntryBytes);
+}
+
 // End of every pass-1 kernel: the product of the other lanes' running products
 // (prefix x suffix) for each lane, and the warp's product of all of them.
 __device__ __forceinline__ void flat_pass1_products(const Fp &acc, Fp *others, Fp *tot, size_t gl, size_t wg) {
@@ -614,7 +622,7 @@ __device__ __forceinline__ G1A flat_load(const FlatArgs &a, RoundIO io, uint32_t
             pt.y = fp_zero();
             return pt;
         }
-        pt = ldg_vec(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)]);
+        pt = ldg_vec(comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)));
         if (v < 0) pt.y = fp_neg(pt.y);
         return pt;
     }
@@ -627,7 +635,7 @@ __device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, RoundIO io, uint32_
     if (FIRST) {
         const int v = a.dig[(size_t)o * a.L + t];
         if (v == 0) return fp_zero();
-        return ldg_vec(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)].x);
+        return ldg_vec(&comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1))->x);
     }
     return ld_vec(&io.src[(size_t)o * m + t].x);
 }
@@ -707,7 +715,7 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // the digit-table entry of digit v (nonzero) of element t of list o
 __device__ __forceinline__ const uint4 *comb_entry(const FlatArgs &a, uint32_t o, uint32_t t, int v) {
-    return reinterpret_cast<const uint4 *>(&a.comb[(size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)]);
+    return reinterpret_cast<const uint4 *>(comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)));
 }
 
 // pass 1 of the first round: the x coordinates of each pair staged one pair ahead
@@ -1666,8 +1674,8 @@ __global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__r
     for (int task = wid; task < n_tasks; task += n_warps) {
         const int b0 = task * kCombRows;
         const uint32_t nb = (uint32_t)min(kCombRows, n_bases - b0);
-        G1A *rows = comb + (size_t)b0 * H;
-        for (uint32_t r = lane; r < nb; r += 32) st_vec(&rows[(size_t)r * H], ld_vec(&bases[b0 + r]));
+        G1A *rows = comb_at(comb, (size_t)b0 * H);
+        for (uint32_t r = lane; r < nb; r += 32) st_vec(comb_at(rows, (size_t)r * H), ld_vec(&bases[b0 + r]));
         __syncwarp();
         for (uint32_t L = 1; L < (uint32_t)H; L <<= 1) {
             const uint32_t P = nb * L;
@@ -1675,7 +1683,7 @@ __global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__r
             int s = 0;
             for (uint32_t q = lane; q < P; q += 32, s++) {
                 const uint32_t rb = q / L, r = q - rb * L + 1;
-                const G1A x = ld_vec(&rows[(size_t)rb * H + r - 1]), y = ld_vec(&rows[(size_t)rb * H + L - 1]);
+                const G1A x = ld_vec(comb_at(rows, (size_t)rb * H + r - 1)), y = ld_vec(comb_at(rows, (size_t)rb * H + L - 1));
                 wb_store_pre(pre, s, acc);
                 acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
             }
@@ -1683,12 +1691,12 @@ __global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__r
             for (int t = s - 1; t >= 0; t--) {
                 const uint32_t q = lane + (uint32_t)t * 32;
                 const uint32_t rb = q / L, r = q - rb * L + 1;
-                const G1A x = ld_vec(&rows[(size_t)rb * H + r - 1]), y = ld_vec(&rows[(size_t)rb * H + L - 1]);
+                const G1A x = ld_vec(comb_at(rows, (size_t)rb * H + r - 1)), y = ld_vec(comb_at(rows, (size_t)rb * H + L - 1));
                 const int kind = pair_kind(x, y);
                 const Fp den = pair_denominator(x, y, kind);
                 const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
                 inv = fp_mul(inv, den);
-                st_vec(&rows[(size_t)rb * H + L + r - 1], pair_result(x, y, kind, inv_den));
+                st_vec(comb_at(rows, (size_t)rb * H + L + r - 1), pair_result(x, y, kind, inv_den));
             }
             __syncwarp();
         }

@@ -894,7 +894,7 @@ int comb_bits_forced() {
 
 size_t comb_bytes(int c) {
     const size_t D = (256 + c - 1) / c;
-    return (size_t)kCells * kCellElems * D * ((size_t)1 << (c - 1)) * sizeof(G1A);
+    return (size_t)kCells * kCellElems * D * ((size_t)1 << (c - 1)) * kCombEntryBytes;
 }
 
 // The grid-wide rounds' shared working set (prefix products, per-lane and
