@@ -391,7 +391,7 @@ def run_ours(args, rank, world, local_rank):
     tune_dir = tempfile.mkdtemp(prefix="vkzg_tune_")
     os.environ["VKZG_TUNE_CACHE"] = os.path.join(tune_dir, "plans.txt")
     # digit-table budget: opted in above the library's 20 GiB default, so the
-    # tuner may pick windows up to 13 bits (64.4 GB)
+    # tuner may pick windows up to 14 bits (122 GB of the device's 179 GiB)
     os.environ.setdefault("VKZG_COMB_BUDGET_GB", str(args.table_budget_gb))
     table_budget = int(float(os.environ["VKZG_COMB_BUDGET_GB"]) * (1 << 30))
     prover = vkzg_b200.Prover(max_batch_size=n)
@@ -750,7 +750,7 @@ def main():
     ap.add_argument("--serve-lanes", type=int, default=3, help="the server's lanes")
     ap.add_argument("--c4-seconds", type=float, default=60.0,
                     help="BASELINE config 4 at the top load with an 8 GiB budget; 0 skips it")
-    ap.add_argument("--table-budget-gb", type=float, default=100.0,
+    ap.add_argument("--table-budget-gb", type=float, default=128.0,
                     help="digit-table budget (GiB) unless $VKZG_COMB_BUDGET_GB is set")
     args = ap.parse_args()
 
