@@ -255,6 +255,16 @@ vkzg_result vkzg_b200_grid_sync_selftest(uint32_t extra_arrivals, uint32_t spin_
                                          uint32_t *error_words_marked);
 
 /*
+ * Self-test of the inversion used between the passes of the proof path's
+ * grid-wide rounds (four lanes per value, divsteps in table-driven groups)
+ * against the one-lane divstep inversion, on n seeded pseudo-random Fp values
+ * (the first four: 0, 1, 2, p - 1).  *mismatched_words: how many 32-bit words
+ * of the n results differ (0 when the two agree).  No counterpart in the
+ * reference.
+ */
+vkzg_result vkzg_b200_inverse_selftest(int n, uint32_t seed, uint32_t *mismatched_words);
+
+/*
  * Sums n_lists lists of m affine points each (points_xy: n_lists * m x 96
  * bytes, list o first; all zero = infinity) with the grid-wide batch-affine
  * tree rounds of the proof path's plan 3.  points_xy NULL: seeded pseudo-random

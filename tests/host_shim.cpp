@@ -155,6 +155,16 @@ void shim_fp_inv_var(const uint32_t *a, uint32_t *r) {
     memcpy(x.v, a, 48);
     memcpy(r, fp_inv_fast<true>(x).v, 48);
 }
+// divsteps30 against its table-driven grouped form (seven groups of 4 and one
+// of 2): 0 when delta and the matrix agree
+int shim_divsteps_grouped_differs(int32_t delta, uint32_t f, uint32_t g) {
+    static const DivstepTable<4> t4 = make_divstep_table<4>();
+    static const DivstepTable<2> t2 = make_divstep_table<2>();
+    int32_t d1 = delta, d2 = delta, a[4], b[4];
+    divsteps30(d1, f, g, a[0], a[1], a[2], a[3]);
+    divsteps30_grouped(t4.e, t2.e, d2, f, g, b[0], b[1], b[2], b[3]);
+    return d1 != d2 || memcmp(a, b, sizeof a) != 0;
+}
 void shim_fr_inv_fast(const uint32_t *a, uint32_t *r) {
     Fr x;
     memcpy(x.v, a, 32);

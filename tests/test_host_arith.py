@@ -139,6 +139,22 @@ def test_divstep_inverse(shim, field):
         assert value(out, n) == 0
 
 
+def test_divsteps_grouped_equal_serial(shim):
+    """The table-driven divstep groups (seven of 4 steps and one of 2, as the
+    proof rounds' four-lane inversion runs them) give the same delta and
+    transition matrix as 30 single divsteps, for deltas inside and far outside
+    the tables' clamped range."""
+    fn = shim.shim_divsteps_grouped_differs
+    fn.argtypes = [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32]
+    fn.restype = ctypes.c_int
+    rng = random.Random(5)
+    for k in range(40000):
+        delta = rng.randint(-6, 6) if k % 2 else rng.randint(-900, 900)
+        f = rng.getrandbits(32) | 1
+        g = rng.getrandbits(32) if k % 7 else rng.getrandbits(32) & ~0x3FF  # long runs of even g
+        assert fn(delta, f, g) == 0, (delta, hex(f), hex(g))
+
+
 Z2 = 0xD201000000010000 ** 2
 
 

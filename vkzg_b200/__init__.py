@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "vkzg_b200_server_stats", "vkzg_b200_kernel_launches", "vkzg_b200_digit_table",
     "vkzg_b200_tree_sums_selftest", "vkzg_b200_window_trials", "vkzg_b200_prover_device_bytes",
     "vkzg_b200_grid_sync_selftest",
+    "vkzg_b200_inverse_selftest",
 )
 NOALLOC_MAX_BLOBS = 16  # VKZG_B200_NOALLOC_MAX_BLOBS
 
@@ -163,6 +164,8 @@ def library():
             u32p = ctypes.POINTER(ctypes.c_uint32)
             L.vkzg_b200_grid_sync_selftest.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, u32p, u32p, u32p]
             L.vkzg_b200_grid_sync_selftest.restype = ctypes.c_int
+            L.vkzg_b200_inverse_selftest.argtypes = [ctypes.c_int, ctypes.c_uint32, u32p]
+            L.vkzg_b200_inverse_selftest.restype = ctypes.c_int
             L.vkzg_b200_kernel_launches.argtypes = []
             L.vkzg_b200_kernel_launches.restype = ctypes.c_uint64
             _lib = L
@@ -436,6 +439,14 @@ def grid_sync_selftest(extra_arrivals, spin_limit, rounds):
     _check(library().vkzg_b200_grid_sync_selftest(int(extra_arrivals), int(spin_limit), int(rounds),
                                                   ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
     return a.value, b.value, c.value
+
+
+def inverse_selftest(n, seed=1):
+    """Words that differ between the four-lane and the one-lane Fp inversion on n
+    seeded values (vkzg_b200_inverse_selftest); 0 when they agree."""
+    out = ctypes.c_uint32()
+    _check(library().vkzg_b200_inverse_selftest(int(n), int(seed), ctypes.byref(out)))
+    return out.value
 
 
 def kernel_launches():

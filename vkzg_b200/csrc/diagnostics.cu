@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_probe_dfma(uint32_t seed, uint32_t *sin
     if (acc == 0.125) sink[0] = 1u;
 }
 
-// one inversion per thread on pseudo-random values below p, as k_flat_invert
+// one inversion per thread on pseudo-random values below p (the scalar form)
 template <bool VAR>
 __global__ void __launch_bounds__(64) k_probe_inv(uint32_t seed, int n, uint32_t *sink) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -434,6 +434,64 @@ extern "C" vkzg_result vkzg_b200_grid_sync_selftest(uint32_t extra_arrivals, uin
     for (uint32_t i = 0; i < kErrWords; i++) marked += (h[8 + i] & kSyncFailed) ? 1u : 0u;
     *error_words_marked = marked;
     return VKZG_OK;
+}
+
+// fp_inv_quad (four lanes a value, as the proof rounds' inversion launches)
+// against fp_inv_fast (one lane) on n seeded pseudo-random values below p, the
+// first four 0, 1, 2 and p - 1: the number of 32-bit words that differ.
+__device__ Fp selftest_value(uint32_t seed, int t) {
+    Fp x;
+    uint32_t h = seed * 0x9e3779b9u + (uint32_t)t * 0x85ebca6bu;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        h ^= h >> 15;
+        h *= 0x2c1b3c6du;
+        h ^= h >> 12;
+        x.v[k] = h;
+    }
+    x.v[11] &= 0x0fffffffu;
+    if (t < 3) {
+#pragma unroll
+        for (int k = 0; k < 12; k++) x.v[k] = k == 0 ? (uint32_t)t : 0u;
+    } else if (t == 3) {
+#pragma unroll
+        for (int k = 0; k < 12; k++) x.v[k] = fp_p(k) - (k == 0 ? 1u : 0u);
+    }
+    return x;
+}
+__global__ void __launch_bounds__(128) k_inverse_selftest(uint32_t seed, int n, uint32_t *mismatch) {
+    __shared__ uint64_t t4[kDivstepEntries<4>], t2[kDivstepEntries<2>];
+    for (int i = threadIdx.x; i < kDivstepEntries<4>; i += blockDim.x) t4[i] = kDivstepTable4.e[i];
+    for (int i = threadIdx.x; i < kDivstepEntries<2>; i += blockDim.x) t2[i] = kDivstepTable2.e[i];
+    __syncthreads();
+    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 2);
+    const Fp x = selftest_value(seed, min(k, n - 1));
+    const Fp q = fp_inv_quad(t4, t2, x);
+    if (k < n && (threadIdx.x & 3) == 2) {
+        const Fp s = fp_inv_fast(x);
+        uint32_t bad = 0;
+#pragma unroll
+        for (int i = 0; i < 12; i++) bad += q.v[i] != s.v[i] ? 1u : 0u;
+        if (bad) atomicAdd(mismatch, bad);
+    }
+}
+
+extern "C" vkzg_result vkzg_b200_inverse_selftest(int n, uint32_t seed, uint32_t *mismatched_words) {
+    if (!mismatched_words || n <= 0 || n > (1 << 20)) return VKZG_ERR_BADARGS;
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, sizeof(uint32_t)) != cudaSuccess) return VKZG_ERR_MALLOC;
+    vkzg_result rc = VKZG_OK;
+    if (cudaMemset(d, 0, sizeof(uint32_t)) != cudaSuccess) rc = VKZG_ERR_GPU;
+    if (rc == VKZG_OK) {
+        k_inverse_selftest<<<(4 * n + 127) / 128, 128>>>(seed, n, d);
+        count_launches(1);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = VKZG_ERR_GPU;
+    }
+    uint32_t h = 0;
+    if (rc == VKZG_OK && cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) rc = VKZG_ERR_GPU;
+    cudaFree(d);
+    if (rc == VKZG_OK) *mismatched_words = h;
+    return rc;
 }
 
 // Sums n_lists lists of m points each with the proof path's grid-wide
