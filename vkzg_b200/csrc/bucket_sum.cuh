@@ -133,6 +133,12 @@ __device__ __forceinline__ Fp fp_shfl_down(const Fp &a, int d) {
     for (int i = 0; i < 12; i++) r.v[i] = __shfl_down_sync(0xffffffffu, a.v[i], d);
     return r;
 }
+__device__ __forceinline__ Fp fp_shfl_xor(const Fp &a, int mask) {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 12; i++) r.v[i] = __shfl_xor_sync(0xffffffffu, a.v[i], mask);
+    return r;
+}
 __device__ __forceinline__ Fp fp_shfl(const Fp &a, int src) {
     Fp r;
 #pragma unroll

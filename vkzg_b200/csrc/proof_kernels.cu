@@ -585,23 +585,23 @@ __host__ __device__ __forceinline__ G1A *comb_at(G1A *comb, size_t idx) {
 }
 
 // End of every pass-1 kernel: the product of the other lanes' running products
-// (prefix x suffix) for each lane, and the warp's product of all of them.
+// for each lane, and the warp's product of all of them.  A butterfly over the
+// lanes: at level k each lane multiplies in the product of the partner group
+// of 2^k lanes (lane ^ 2^k's group), so after five levels every lane holds the
+// total, and the five partner groups' products together are the other lanes':
+// 9 products per lane, against 11 for a prefix and a suffix scan.
 __device__ __forceinline__ void flat_pass1_products(const Fp &acc, Fp *others, Fp *tot, size_t gl, size_t wg) {
     const int lane = threadIdx.x & 31;
-    Fp pr = acc, sf = acc;
+    Fp group = acc, rest = fp_shfl_xor(acc, 1);
+    group = fp_mul(group, rest);
 #pragma unroll 1
-    for (int d = 1; d < 32; d <<= 1) {
-        const Fp u = fp_shfl_up(pr, d);
-        if (lane >= d) pr = fp_mul(pr, u);
-        const Fp w = fp_shfl_down(sf, d);
-        if (lane + d < 32) sf = fp_mul(sf, w);
+    for (int d = 2; d < 32; d <<= 1) {
+        const Fp partner = fp_shfl_xor(group, d);
+        rest = fp_mul(rest, partner);
+        group = fp_mul(group, partner);
     }
-    const Fp total = fp_shfl(pr, 31);
-    Fp pre_x = fp_shfl_up(pr, 1), suf_x = fp_shfl_down(sf, 1);
-    if (lane == 0) pre_x = fp_one();
-    if (lane == 31) suf_x = fp_one();
-    st_vec(&others[gl], fp_mul(pre_x, suf_x));
-    if (lane == 0) st_vec(&tot[wg], total);
+    st_vec(&others[gl], rest);
+    if (lane == 0) st_vec(&tot[wg], group);
 }
 
 // A round's input and output lists, apart from the phase's other arguments:
