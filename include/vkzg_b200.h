@@ -225,7 +225,8 @@ vkzg_result vkzg_b200_server_stats(vkzg_server *s, vkzg_server_stats *out, int r
  * FP64 pipe, 13: Fp squares on the FP64 pipe, 14: Fp multiplies with half the
  * warps on each pipe, 15 and 16: Fp multiplies on the FP64 pipe and through one
  * Karatsuba level with four independent chains per thread instead of two
- * (giga-ops/s).  Best of three timed launches.
+ * (giga-ops/s); 17: as 11, each value inverted by four lanes (the form the
+ * proof rounds use), in microseconds.  Best of three timed launches.
  */
 vkzg_result vkzg_b200_microbench(int which, double *result);
 

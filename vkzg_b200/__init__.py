@@ -461,7 +461,8 @@ def microbench(which):
     8: mad.wide.u32 and 9: fma.rn.f64 issue rates (T/s); 10 / 11: one launch of
     16 Fp inversions per SM, variable-time / fixed divstep batches (microseconds);
     12 / 13: Fp multiplies / squares on the FP64 pipe; 14: half the warps on each
-    pipe; 15 / 16: FP64-pipe / Karatsuba multiplies with four chains per thread (G/s)."""
+    pipe; 15 / 16: FP64-pipe / Karatsuba multiplies with four chains per thread (G/s);
+    17: as 11 with four lanes per inversion (microseconds)."""
     out = ctypes.c_double()
     _check(library().vkzg_b200_microbench(int(which), ctypes.byref(out)))
     return out.value

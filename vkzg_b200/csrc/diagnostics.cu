@@ -81,6 +81,27 @@ __global__ void __launch_bounds__(64) k_probe_inv(uint32_t seed, int n, uint32_t
     if (y.v[0] == 0x12345678u) sink[0] = y.v[1];
 }
 
+// the same values inverted four lanes a value, as k_flat_invert does
+__global__ void __launch_bounds__(128) k_probe_inv_quad(uint32_t seed, int n, uint32_t *sink) {
+    __shared__ uint64_t t4[kDivstepEntries<4>], t2[kDivstepEntries<2>];
+    for (int i = threadIdx.x; i < kDivstepEntries<4>; i += blockDim.x) t4[i] = kDivstepTable4.e[i];
+    for (int i = threadIdx.x; i < kDivstepEntries<2>; i += blockDim.x) t2[i] = kDivstepTable2.e[i];
+    __syncthreads();
+    const int t = min((int)((blockIdx.x * blockDim.x + threadIdx.x) >> 2), n - 1);
+    Fp x;
+    uint32_t h = seed * 0x9e3779b9u + (uint32_t)t * 0x85ebca6bu;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        h ^= h >> 15;
+        h *= 0x2c1b3c6du;
+        h ^= h >> 12;
+        x.v[k] = h;
+    }
+    x.v[11] &= 0x0fffffffu;
+    const Fp y = fp_inv_quad(t4, t2, x);
+    if (y.v[0] == 0x12345678u) sink[0] = y.v[1];
+}
+
 __device__ __noinline__ Fp fp_mul_ks_call(Fp a, Fp b) {
     Fp r;
     mont_mul_ks<12>(r.v, a.v, b.v);
@@ -308,7 +329,7 @@ extern "C" vkzg_result vkzg_b200_bucket_sums_selftest(const uint8_t *points_xy, 
 
 // which: 0 = 32-bit IMAD issue rate (T/s), 1 = Fp multiplies (G/s), 2 = Fr multiplies (G/s)
 extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
-    if (!result || which < 0 || which > 16) return VKZG_ERR_BADARGS;
+    if (!result || which < 0 || which > 17) return VKZG_ERR_BADARGS;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -323,10 +344,11 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
     for (int rep = 0; rep < 4; rep++) {
         cudaEventRecord(e0);
         double ops = 0.0;
-        if (which == 10 || which == 11) {
+        if (which == 10 || which == 11 || which == 17) {
             const int n = sms * 16; // the warps of the round kernels' grid, one inversion each
             if (which == 10) k_probe_inv<true><<<(n + 63) / 64, 64>>>(rep + 1, n, sink);
-            else k_probe_inv<false><<<(n + 63) / 64, 64>>>(rep + 1, n, sink);
+            else if (which == 11) k_probe_inv<false><<<(n + 63) / 64, 64>>>(rep + 1, n, sink);
+            else k_probe_inv_quad<<<(4 * n + 127) / 128, 128>>>(rep + 1, n, sink);
             ops = 1.0;
         } else if (which == 0 || which == 8 || which == 9) {
             const int blocks = sms * 8;
@@ -360,7 +382,7 @@ extern "C" vkzg_result vkzg_b200_microbench(int which, double *result) {
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (which == 10 || which == 11) { // launch time in microseconds, the smallest
+        if (which == 10 || which == 11 || which == 17) { // launch time in microseconds, the smallest
             const double us = ms * 1e3;
             if (rep > 0 && (best == 0.0 || us < best)) best = us;
             continue;
