@@ -45,8 +45,9 @@ constexpr uint32_t kMask30 = (1u << 30) - 1;
 // (g - f) / 2); otherwise (1 + delta, f, (g + (g mod 2) f) / 2).  The candidate
 // values of g (and of the cofactor rows) are formed from the old values in
 // parallel and then selected, which keeps the step's dependency chain through
-// g short: 31.8 against 41.1 us for a launch of 2368 inversions with the
-// masked-arithmetic form of the same step.
+// g short: 31.8 against 41.1 us per launch of 2368 inversions (one per lane,
+// averaged over 50 back-to-back launches) with the masked-arithmetic form of
+// the same step.
 VK_HD void divsteps30(int32_t &delta, uint32_t f, uint32_t g, int32_t &u_out, int32_t &v_out, int32_t &q_out,
                       int32_t &r_out) {
     uint32_t u = 1, v = 0, q = 0, r = 1;
@@ -403,8 +404,9 @@ static __device__ const DivstepTable<2> kDivstepTable2 = make_divstep_table<2>()
 // 3 e'), which the pair's two lanes then exchange.  A batch thus costs one row
 // of 13-limb products per lane instead of four; the same batches as
 // inverse_words, so the same result.  The quad's four lanes must run this
-// together (they shuffle among themselves only).  Measured on a launch of 2368
-// inversions: 24.7 us, against 41.1 us at one inversion per lane.
+// together (they shuffle among themselves only).  Measured per launch of 2368
+// inversions, averaged over 50 back-to-back launches: 24.7 us, against 31.8 us
+// at one inversion per lane.
 static __device__ __noinline__ Fp fp_inv_quad(const uint64_t *t4, const uint64_t *t2, const Fp &a) {
     constexpr int N = 12, L = 13;
     const int lane = threadIdx.x & 31, role = lane & 3, base = lane & ~3;

@@ -809,8 +809,8 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flat_pass1(F
 // the critical path between the passes, so it is latency that counts: all n
 // inversions run at once, and one inversion per value has less latency than a
 // shared batch inversion (a product scan of 32 values, one inversion, a scan
-// back).  Measured per launch of 2368 values: 24.7 us at four lanes a value,
-// 41.1 us at one.
+// back).  Measured per launch of 2368 values, averaged over 50 back-to-back
+// launches: 24.7 us at four lanes a value, 31.8 us at one.
 constexpr int kInvThreads = 128;
 __global__ void __launch_bounds__(kInvThreads) k_flat_invert(const Fp *tot, Fp *totinv, int n) {
     __shared__ uint64_t t4[kDivstepEntries<4>], t2[kDivstepEntries<2>];
