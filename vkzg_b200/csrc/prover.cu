@@ -1567,6 +1567,42 @@ namespace {
 // every blob of the chunk is canonical (the proofs path's rule).
 vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
+    const size_t ext = (size_t)kExtElems * 32;
+    if (!proofs && !p->timing && n >= 64 && p->side[0] && host_pinned(blobs) && host_pinned(cells)) {
+        // cells only, page-locked buffers: parts of the chunk on the side
+        // streams as recovery runs them (copy in, kernel, copy out per part), so
+        // that the 384 KB per blob of copies overlap the kernels.  The cells go
+        // out before the blobs' error words are read, so a chunk with an invalid
+        // blob has its cells zeroed before INVALID_BLOB is returned.
+        const uint32_t parts = std::min<uint32_t>(vkzg_prover::kRecMaxParts, n / vkzg_prover::kRecPartBlobs);
+        const uint32_t part = (n + parts - 1) / parts;
+        CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
+        CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
+        for (int k = 0; k < vkzg_prover::kSides; k++)
+            CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
+        for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
+            const uint32_t cnt = std::min(part, n - off);
+            cudaStream_t st = p->side[k % vkzg_prover::kSides];
+            CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, blobs + (size_t)off * kBlobBytes,
+                               (size_t)cnt * kBlobBytes, cudaMemcpyHostToDevice, st));
+            CK(launch_cells(p->t, p->pw.blobs + (size_t)off * kBlobBytes, p->rw.out + off * ext, p->pw.err + off,
+                            (int)cnt, st));
+            CK(cudaMemcpyAsync(cells + off * ext, p->rw.out + off * ext, cnt * ext, cudaMemcpyDeviceToHost, st));
+        }
+        for (int k = 0; k < vkzg_prover::kSides; k++) {
+            CK(cudaEventRecord(p->side_ev[k], p->side[k]));
+            CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
+        }
+        CK(cudaMemcpyAsync(p->h_err, p->pw.err, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        vkzg_result rc = VKZG_OK;
+        for (uint32_t b = 0; b < n && rc == VKZG_OK; b++)
+            if (p->h_err[b] & kSyncFailed) rc = VKZG_ERR_GPU;
+        for (uint32_t b = 0; b < n && rc == VKZG_OK; b++)
+            if (p->h_err[b]) rc = VKZG_ERR_INVALID_BLOB;
+        if (rc != VKZG_OK) memset(cells, 0, (size_t)n * ext);
+        return rc;
+    }
     CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
     CK(launch_cells(p->t, p->pw.blobs, p->rw.out, p->pw.err, (int)n, s));
