@@ -78,11 +78,25 @@ def phase_a_executed_imad_per_output(c):
     muls = 5 * adds + 7 * madds + 11
     sqrs = adds + 4 * madds + 5
     return muls * IMAD_FP_MUL_KS + sqrs * IMAD_FP_SQR_KS
-# DRAM bytes of phase A per blob under plan 3, by window: per-pair ncu
-# dram__bytes_read + dram__bytes_write of each phase-A kernel in a 16-blob,
-# 9-bit-window capture (one kernel per capture), applied to the exact pair
-# counts of a 13-bit window (profiles/phase_a_dram_traffic_16blobs.md)
-PHASE_A_DRAM_BYTES_PER_BLOB = {13: 30.0e9 / 256}
+def phase_a_dram_bytes(c, n_blobs):
+    """DRAM bytes of one plan-3 phase-A pass over n_blobs with a c-bit digit
+    table: the per-pair ncu dram__bytes_read + dram__bytes_write of the round
+    kernels in a 16-blob, 9-bit-window capture, one kernel per capture
+    (profiles/phase_a_dram_traffic_16blobs.md) -- 893 B per pair in round 1,
+    which gathers digit-table points, 546 B in later rounds while a round's
+    input lists exceed the 126 MB L2, 500 B once they fit -- applied to the
+    window's exact pair counts, plus the digit recoding and the Jacobian tail
+    (0.05 GB per 256 blobs).  For c = 13 at 256 blobs: 30.0 GB."""
+    lists = 128 * n_blobs
+    m = 64 * -(-256 // c)
+    total, first = 0.0, True
+    while m > 10:
+        pairs = lists * (m // 2)
+        per = 893 if first else (546 if lists * m * 96 > 126e6 else 500)
+        total += pairs * per
+        first = False
+        m = (m + 1) // 2
+    return total + 0.05e9 * n_blobs / 256
 
 
 # ------------------------------------------------------------------ inputs
@@ -709,8 +723,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac_of_product_rate": products / product_rate if products else None,
                      "reference_algorithm_tera_imad_per_s": reference_work,
                      "work_saved": reference_work / executed if executed else None,
-                     "traffic": PHASE_A_DRAM_BYTES_PER_BLOB[digit[0]] * n
-                     if plan == 3 and digit and digit[0] in PHASE_A_DRAM_BYTES_PER_BLOB else None,
+                     "traffic": phase_a_dram_bytes(digit[0], n) if plan == 3 and digit else None,
                      "traffic_unit": "DRAM bytes per phase-A pass over the batch (ncu dram__bytes_read + write "
                                      "per pair from a 16-blob 9-bit-window capture, one kernel each, applied "
                                      "to this window's pair counts)"},
