@@ -53,9 +53,10 @@ IMAD_FP_MUL_KS, IMAD_FP_SQR_KS = 516, 426
 PHASE_A_TAIL = 10  # lists of at most this many points finish in Jacobian form
 
 
-def phase_a_executed_products_per_output(c):
-    """Fp products and squares plan 3's phase A executes per MSM output at window c."""
-    m = 64 * ((256 + c - 1) // c)
+def phase_a_executed_products_per_output(d):
+    """Fp products and squares plan 3's phase A executes per MSM output with a
+    digit table of d windows (lists of 64 d points)."""
+    m = 64 * d
     adds = 0
     while m > PHASE_A_TAIL:
         adds += m // 2
@@ -64,12 +65,12 @@ def phase_a_executed_products_per_output(c):
     return 6 * adds + 11 * madds + 16
 
 
-def phase_a_executed_imad_per_output(c):
-    """Multiply instructions plan 3's phase A executes per MSM output at window c:
-    affine additions (5 products + 1 square) in tree rounds down to lists of
-    PHASE_A_TAIL points, then mixed additions (7 + 4) on two chains and one
-    Jacobian addition (11 + 5)."""
-    m = 64 * ((256 + c - 1) // c)
+def phase_a_executed_imad_per_output(d):
+    """Multiply instructions plan 3's phase A executes per MSM output with d
+    windows: affine additions (5 products + 1 square) in tree rounds down to
+    lists of PHASE_A_TAIL points, then mixed additions (7 + 4) on two chains and
+    one Jacobian addition (11 + 5)."""
+    m = 64 * d
     adds = 0
     while m > PHASE_A_TAIL:
         adds += m // 2
@@ -78,17 +79,19 @@ def phase_a_executed_imad_per_output(c):
     muls = 5 * adds + 7 * madds + 11
     sqrs = adds + 4 * madds + 5
     return muls * IMAD_FP_MUL_KS + sqrs * IMAD_FP_SQR_KS
-def phase_a_dram_bytes(c, n_blobs):
-    """DRAM bytes of one plan-3 phase-A pass over n_blobs with a c-bit digit
-    table: the per-pair ncu dram__bytes_read + dram__bytes_write of the round
+
+
+def phase_a_dram_bytes(d, n_blobs):
+    """DRAM bytes of one plan-3 phase-A pass over n_blobs with a digit table of
+    d windows: the per-pair ncu dram__bytes_read + dram__bytes_write of the round
     kernels in a 16-blob, 9-bit-window capture, one kernel per capture
     (profiles/phase_a_dram_traffic_16blobs.md) -- 893 B per pair in round 1,
     which gathers digit-table points, 546 B in later rounds while a round's
     input lists exceed the 126 MB L2, 500 B once they fit -- applied to the
-    window's exact pair counts, plus the digit recoding and the Jacobian tail
-    (0.05 GB per 256 blobs).  For c = 13 at 256 blobs: 30.0 GB."""
+    table's exact pair counts, plus the digit recoding and the Jacobian tail
+    (0.05 GB per 256 blobs).  For 20 windows at 256 blobs: 30.0 GB."""
     lists = 128 * n_blobs
-    m = 64 * -(-256 // c)
+    m = 64 * d
     total, first = 0.0, True
     while m > 10:
         pairs = lists * (m // 2)
@@ -405,7 +408,7 @@ def run_ours(args, rank, world, local_rank):
     tune_dir = tempfile.mkdtemp(prefix="vkzg_tune_")
     os.environ["VKZG_TUNE_CACHE"] = os.path.join(tune_dir, "plans.txt")
     # digit-table budget: opted in above the library's 20 GiB default, so the
-    # tuner may pick windows up to 14 bits (122 GB of the device's 179 GiB)
+    # tuner may pick tables up to 18 windows (141.7 GB of the device's 179 GiB)
     os.environ.setdefault("VKZG_COMB_BUDGET_GB", str(args.table_budget_gb))
     table_budget = int(float(os.environ["VKZG_COMB_BUDGET_GB"]) * (1 << 30))
     prover = vkzg_b200.Prover(max_batch_size=n)
@@ -715,7 +718,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": "measured in-process (vkzg_b200_microbench(0): mad.lo.u32 issue rate; "
                                     "MEASURED_PEAKS.json has no integer figure); nominal 148 SM x 64/clk x "
                                     f"1.965 GHz = {NOMINAL_IMAD_TPS:.1f}",
-                     "algorithmic": "multiply instructions phase A executes: per MSM output 64 ceil(256/c) - 1 "
+                     "algorithmic": "multiply instructions phase A executes: per MSM output 64 D - 1 (D windows) "
                                     "digit-table points summed by affine additions (5 products + 1 square, "
                                     "516 / 426 multiply instructions each) down to lists of 10, then mixed "
                                     "Jacobian additions",
@@ -726,11 +729,12 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": phase_a_dram_bytes(digit[0], n) if plan == 3 and digit else None,
                      "traffic_unit": "DRAM bytes per phase-A pass over the batch (ncu dram__bytes_read + write "
                                      "per pair from a 16-blob 9-bit-window capture, one kernel each, applied "
-                                     "to this window's pair counts)"},
-        "digit_table": {"window_bits": digit[0], "build_ms": round(digit[1], 1), "bytes": digit[2],
+                                     "to this table's pair counts)"},
+        "digit_table": {"windows": digit[0], "window_bits": vkzg_b200.comb_windows(digit[0]),
+                        "build_ms": round(digit[1], 1), "bytes": digit[2],
                         "budget_bytes": table_budget,
-                        "window_trials": [{"window_bits": c, "bytes": b, "build_ms": round(bm, 1), "proof_ms": round(t, 3)}
-                                          for c, b, bm, t in prover.window_trials(n)]} if digit else None,
+                        "window_trials": [{"windows": d, "bytes": b, "build_ms": round(bm, 1), "proof_ms": round(t, 3)}
+                                          for d, b, bm, t in prover.window_trials(n)]} if digit else None,
         "device_bytes": prover.device_bytes(),
         "persistent_form": persistent,
         "verified": verified,
@@ -763,7 +767,7 @@ def main():
     ap.add_argument("--serve-lanes", type=int, default=3, help="the server's lanes")
     ap.add_argument("--c4-seconds", type=float, default=60.0,
                     help="BASELINE config 4 at the top load with an 8 GiB budget; 0 skips it")
-    ap.add_argument("--table-budget-gb", type=float, default=128.0,
+    ap.add_argument("--table-budget-gb", type=float, default=136.0,
                     help="digit-table budget (GiB) unless $VKZG_COMB_BUDGET_GB is set")
     args = ap.parse_args()
 

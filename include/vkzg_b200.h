@@ -124,20 +124,24 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * max_batch_size) on seeded synthetic blobs; vkzg_b200_tuning_table reports the
  * decisions (size class, plan, and VKZG_B200_PLANS times in ms per class, -1
  * where a plan was not timed) and returns how many classes are tuned.
- * vkzg_b200_digit_table returns the digit table's window c (0 = none built),
- * its build time and size.
+ * vkzg_b200_digit_table returns the digit table's windows per scalar D (0 =
+ * none built), its build time and size.
  *
- * Plan 3's digit table holds m 2^(c k) X[j][i] for every window k of c bits:
- * 128 x 64 x ceil(256/c) x 2^(c-1) points of 96 bytes (c = 8: 3.2 GB, 10: 10.5,
- * 11: 19.3, 12: 35.4, 13: 64.4, 14: 122 GB); wider windows mean fewer
- * additions per output (64 ceil(256/c) - 1).  Its size is bounded by a budget:
- * $VKZG_COMB_BUDGET_GB (GiB, default 20, so c <= 11 unless raised); a serving
- * loop uses its table_budget_bytes.  When plan 3 is tuned, the widest window
- * that fits the budget and the two below it are each built and timed, and the
- * fastest is kept (and remembered in $VKZG_TUNE_CACHE); $VKZG_COMB_BITS pins
- * the window (0: no digit table).  vkzg_b200_window_trials reports those
- * trials for a size class (window, table bytes, build ms, proof-chunk ms) and
- * returns their count.  vkzg_b200_prover_device_bytes reports the device
+ * Plan 3's digit table cuts a scalar's 256 bits into D signed windows of
+ * widths W + 1 (the first 256 mod D of them) and W = floor(256 / D), and holds
+ * m 2^(b_k) X[j][i] for every window k (at bit b_k) and m = 1..2^(width - 1):
+ * points of 96 bytes, 128 x 64 x that many per base (D = 32: 8-bit windows,
+ * 3.2 GB; 26: 9.7 GB; 24: 16.1 GB; 23: 20.9 GB; 22: 29.0 GB; 21: 40.3 GB; 20:
+ * 58.0 GB; 19: 90.2 GB; 18: 141.7 GB); fewer windows mean fewer additions per
+ * output (64 D - 1).  Its size is bounded by a budget: $VKZG_COMB_BUDGET_GB
+ * (GiB, default 20, so D >= 24 unless raised); a serving loop uses its
+ * table_budget_bytes.  When plan 3 is tuned, the fewest windows whose table
+ * fits the budget and the next two counts are each built and timed, and the
+ * fastest is kept (and remembered in $VKZG_TUNE_CACHE); $VKZG_COMB_WINDOWS pins
+ * D (18..32), $VKZG_COMB_BITS pins the widest window instead (D =
+ * ceil(256 / bits)), and 0 in either means no digit table.
+ * vkzg_b200_window_trials reports those trials for a size class (windows,
+ * table bytes, build ms, proof-chunk ms) and returns their count.  vkzg_b200_prover_device_bytes reports the device
  * memory a prover holds: its working set, its setup tables, and the digit
  * table it uses (shared by all provers of the process with the same setup).
  */
@@ -145,7 +149,7 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
 vkzg_result vkzg_b200_autotune(vkzg_prover *p, uint32_t max_blobs);
 int vkzg_b200_tuning_table(const vkzg_prover *p, uint32_t *size_class, int *plan, double *ms, int cap);
 int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *bytes);
-int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *window_bits, uint64_t *table_bytes,
+int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *windows, uint64_t *table_bytes,
                             double *build_ms, double *ms, int cap);
 void vkzg_b200_prover_device_bytes(const vkzg_prover *p, uint64_t *working, uint64_t *tables, uint64_t *digit_table);
 

@@ -124,6 +124,7 @@ int shim_g1_mul(const uint8_t *p48, const uint32_t *k, uint8_t *out48) {
 }
 }
 
+#include "../vkzg_b200/csrc/comb_windows.h"
 #include "../vkzg_b200/csrc/glv.h"
 #include "../vkzg_b200/csrc/inverse.cuh"
 extern "C" {
@@ -154,6 +155,17 @@ void shim_fp_inv_var(const uint32_t *a, uint32_t *r) {
     Fp x;
     memcpy(x.v, a, 48);
     memcpy(r, fp_inv_fast<true>(x).v, 48);
+}
+// the digit table's layout for d windows: each window's width, bit and first
+// entry within a base column, and the column's entry count
+void shim_comb_windows(int d, int *width, int *bit, uint32_t *entry, uint32_t *entries) {
+    const CombWindows w = comb_windows(d);
+    for (int k = 0; k < d; k++) {
+        width[k] = w.width(k);
+        bit[k] = w.bit_off(k);
+        entry[k] = w.entry_off(k);
+    }
+    *entries = w.entries();
 }
 // divsteps30 against its table-driven grouped form (seven groups of 4 and one
 // of 2): 0 when delta and the matrix agree

@@ -139,6 +139,30 @@ def test_divstep_inverse(shim, field):
         assert value(out, n) == 0
 
 
+def test_comb_window_layout(shim):
+    """The digit table's windows (CombWindows, the device's layout) for every
+    window count 18..32: widths of W and W + 1 bits summing to exactly 256,
+    each window at the sum of the widths below it, each window's 2^(width - 1)
+    entries after those of the windows below it; and the same table sizes as the
+    Python helper the tests and the bench use."""
+    import vkzg_b200
+    fn = shim.shim_comb_windows
+    for d in range(18, 33):
+        width = (ctypes.c_int * 32)()
+        bit = (ctypes.c_int * 32)()
+        entry = (ctypes.c_uint32 * 32)()
+        entries = ctypes.c_uint32()
+        fn(d, width, bit, entry, ctypes.byref(entries))
+        widths = list(width[:d])
+        assert sum(widths) == 256 and max(widths) - min(widths) <= 1
+        assert widths == vkzg_b200.comb_windows(d)
+        assert list(bit[:d]) == [sum(widths[:k]) for k in range(d)]
+        assert list(entry[:d]) == [sum(1 << (w - 1) for w in widths[:k]) for k in range(d)]
+        assert entries.value == sum(1 << (w - 1) for w in widths)
+        assert vkzg_b200.comb_table_bytes(d) == 128 * 64 * entries.value * 96
+        assert max(widths) <= 15  # digits up to 2^14 in magnitude fit int16
+
+
 def test_divsteps_grouped_equal_serial(shim):
     """The table-driven divstep groups (seven of 4 steps and one of 2, as the
     proof rounds' four-lane inversion runs them) give the same delta and

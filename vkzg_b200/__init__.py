@@ -340,15 +340,16 @@ class Prover:
         return {int(sc[i]): (int(pl[i]), tuple(ms[PLANS * i:PLANS * i + PLANS])) for i in range(min(n, cap))}
 
     def digit_table(self):
-        """(window bits c, build ms, bytes) of plan 3's digit table, or None before it is built."""
+        """(windows per scalar D, build ms, bytes) of plan 3's digit table, or None
+        before it is built (comb_windows(D) gives the window widths)."""
         ms = ctypes.c_double()
         nb = ctypes.c_uint64()
         c = self._lib.vkzg_b200_digit_table(self._h, ctypes.byref(ms), ctypes.byref(nb))
         return (c, ms.value, nb.value) if c else None
 
     def window_trials(self, size_class):
-        """The digit-table windows the tuner timed for a size class:
-        [(window bits c, table bytes, build ms, proof-chunk ms), ...]."""
+        """The digit tables the tuner timed for a size class:
+        [(windows per scalar D, table bytes, build ms, proof-chunk ms), ...]."""
         cap = 8
         c = (ctypes.c_int * cap)()
         nb = (ctypes.c_uint64 * cap)()
@@ -430,6 +431,19 @@ class Server:
         st = ServerStats()
         _check(self._lib.vkzg_b200_server_stats(self._h, ctypes.byref(st), 1 if reset else 0))
         return st.as_dict()
+
+
+def comb_windows(d):
+    """The widths of the digit table's d windows (as the library cuts a scalar's
+    256 bits: the first 256 mod d windows one bit wider than the rest)."""
+    w, r = divmod(256, d)
+    return [w + 1] * r + [w] * (d - r)
+
+
+def comb_table_bytes(d):
+    """Bytes of the digit table of d windows: 128 x 64 base columns, each with
+    2^(width - 1) points of 96 bytes per window."""
+    return 128 * 64 * sum(1 << (w - 1) for w in comb_windows(d)) * 96
 
 
 def grid_sync_selftest(extra_arrivals, spin_limit, rounds):

@@ -12,7 +12,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvkzg.so")
 SOURCES = ["proof_kernels.cu", "recover_kernels.cu", "cells_kernels.cu", "setup_kernels.cu", "prover.cu",
            "server.cu", "diagnostics.cu"]
-HEADERS = ["field.cuh", "field_f64.cuh", "curve.cuh", "inverse.cuh", "device_util.cuh", "bucket_sum.cuh", "kernels.h", "glv.h"]
+HEADERS = ["field.cuh", "field_f64.cuh", "curve.cuh", "inverse.cuh", "device_util.cuh", "bucket_sum.cuh", "kernels.h",
+           "comb_windows.h", "glv.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",

@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "comb_windows.h"
+
 namespace vkzg {
 
 struct Fr;
@@ -127,8 +129,8 @@ struct ProofWork {
     G1A *ba_scratch = nullptr;  // [ba_blocks][kBAScratchPoints]
     int ba_blocks = 0;          // persistent grid size of the batch-affine kernels
     uint32_t *task_ctr = nullptr; // [2] next task of phase A / phase B (zeroed before phase A)
-    const G1A *comb = nullptr;    // plan 3: digit table [128 j][64 i][D][2^(c-1)], shared by provers
-    int comb_c = 0;               // its window width
+    const G1A *comb = nullptr;    // plan 3: digit table [128 j][64 i][entries of D windows], shared by provers
+    int comb_windows = 0;         // its windows per scalar (CombWindows)
     // plan 3's grid-wide tree rounds (flat_sizes gives the sizes)
     int16_t *flat_dig = nullptr;  // [cap * 128][64 D] digits
     G1A *flat_buf[2] = {nullptr, nullptr};
@@ -174,10 +176,8 @@ cudaError_t launch_recover(const DeviceTables &t, const RecoverWork &w, int n, c
 // Table generation from 4096 compressed monomial points already on the device.
 // Writes t.pos; needs `scratch` of at least setup_scratch_bytes().
 size_t setup_scratch_bytes();
-size_t comb_build_scratch_bytes(int c);
-// Window widths of the digit table: 8 bits (32 windows, 3.2 GB) to 14 bits
-// (19 windows, 122 GB).
-constexpr int kCombMinBits = 8, kCombMaxBits = 14;
+size_t comb_build_scratch_bytes(int windows);
+constexpr int kCombMinWindows = 18, kCombMaxWindows = 32;
 // Bytes per digit-table entry: an affine point (96 bytes), or with
 // VKZG_COMB_ENTRY_BYTES=128 a point padded to one 128-byte line, so that a
 // random gather touches one line instead of straddling two half of the time.
@@ -193,10 +193,10 @@ struct FlatSizes {
     int blocks = 0;
     size_t lanes = 0, dig = 0, buf0 = 0, buf1 = 0, slots = 0, pre_words = 0;
 };
-FlatSizes flat_sizes(int cap, int c);
+FlatSizes flat_sizes(int cap, int windows);
 int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *buf1, uint32_t *pre, Fp *others,
                      Fp *tot, Fp *totinv, size_t slots, int blocks, G1A *sums, cudaStream_t s);
-cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int c, cudaStream_t s);
+cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int windows, cudaStream_t s);
 cudaError_t launch_setup_tables(const uint8_t *d_g1_monomial, G1A *pos, const Fr *roots_fwd, void *scratch,
                                 uint32_t *d_err, cudaStream_t s);
 cudaError_t configure_kernels();

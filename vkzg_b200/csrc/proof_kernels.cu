@@ -530,13 +530,16 @@ __global__ void __launch_bounds__(kBAThreads, kBAMinBlocks) k_phase_b_affine(con
 
 // ------------------------------------------------ phase A over a digit table
 // Fixed-base comb: the bases X[j][i] of phase A are setup constants, so with
-// c-bit signed windows every digit value has its own precomputed point,
-//   comb[j][i][k][m - 1] = m 2^(c k) X[j][i],   m = 1..2^(c-1), k < D = ceil(256 / c),
-// and output o = (blob, j) is a plain sum of 64 * D table points (one per
+// the scalar's 256 bits in D signed windows (CombWindows: widths W and W + 1,
+// window k at bit b_k) every digit value has its own precomputed point,
+//   comb[j][i][entry_off(k) + m - 1] = m 2^(b_k) X[j][i],   m = 1..2^(width_k - 1),
+// and output o = (blob, j) is a plain sum of 64 D table points (one per
 // nonzero digit, negated for negative digits): no buckets, no bucket
-// reduction.  c = 12 takes 1408 additions per output against the reference
-// form's 2048 bucket additions plus the 128-bucket reduction, for a 35.4 GB
-// table (HBM holds it; the reads are 96-byte gathers, ~4 GB per 256 blobs).
+// reduction.  D = 19 (9 windows of 14 bits, 10 of 13) sums 1216 points per
+// output against the reference form's 2048 bucket additions plus the
+// 128-bucket reduction, for a 90.2 GB table (HBM holds it; the reads are
+// 96-byte gathers).  Windows of even widths waste no table: 19 uniform 14-bit
+// windows (266 bits) took 122 GB for the same sums.
 
 // Bits [off, off + c) of a canonical 256-bit scalar.
 __device__ __forceinline__ uint32_t scalar_window(const Fr &s, int off, int c) {
@@ -565,8 +568,11 @@ constexpr int kFlatBlocksPerSM = VKZG_FLAT_BLOCKS_PER_SM;
 struct FlatArgs {
     const int16_t *dig;  // [list][64 D] signed digits
     const G1A *comb;     // digit table
-    size_t per_j;        // points per column j of the table
-    int H, L;            // 2^(c-1), 64 D
+    size_t per_j;        // points per column j of the table (64 per_i)
+    uint32_t per_i;      // points per base column (j, i): win.entries()
+    uint32_t dmagic;     // ceil(2^32 / D): t / D = umulhi(t, dmagic) for t < 2^16
+    CombWindows win;
+    int L;               // 64 D
     const G1A *src;      // round input lists (round 1: the table)
     G1A *dst;            // round output lists
     uint32_t *pre;       // per warp: slots x 12 x 32 words of prefix products
@@ -582,6 +588,13 @@ __host__ __device__ __forceinline__ const G1A *comb_at(const G1A *comb, size_t i
 }
 __host__ __device__ __forceinline__ G1A *comb_at(G1A *comb, size_t idx) {
     return reinterpret_cast<G1A *>(reinterpret_cast<char *>(comb) + idx * kCombEntryBytes);
+}
+
+// Table entry of element t of list o (scalar i = t / D of the output, window
+// k = t mod D) for its digit v != 0.
+__device__ __forceinline__ size_t comb_index(const FlatArgs &a, uint32_t o, uint32_t t, int v) {
+    const uint32_t i = __umulhi(t, a.dmagic), k = t - i * (uint32_t)a.win.D;
+    return (size_t)(o % kCells) * a.per_j + (size_t)i * a.per_i + a.win.entry_off((int)k) + (uint32_t)(abs(v) - 1);
 }
 
 // End of every pass-1 kernel: the product of the other lanes' running products
@@ -622,7 +635,7 @@ __device__ __forceinline__ G1A flat_load(const FlatArgs &a, RoundIO io, uint32_t
             pt.y = fp_zero();
             return pt;
         }
-        pt = ldg_vec(comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)));
+        pt = ldg_vec(comb_at(a.comb, comb_index(a, o, t, v)));
         if (v < 0) pt.y = fp_neg(pt.y);
         return pt;
     }
@@ -635,29 +648,32 @@ __device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, RoundIO io, uint32_
     if (FIRST) {
         const int v = a.dig[(size_t)o * a.L + t];
         if (v == 0) return fp_zero();
-        return ldg_vec(&comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1))->x);
+        return ldg_vec(&comb_at(a.comb, comb_index(a, o, t, v))->x);
     }
     return ld_vec(&io.src[(size_t)o * m + t].x);
 }
 
-// Signed c-bit digits of every scalar: scalar q = o 64 + i fills dig[q D ..].
-// A block's 128 scalars are recoded into shared memory and written out as one
-// contiguous run of 16-byte stores (a thread's own digits are D x 2 bytes apart
-// from its neighbour's: direct stores would scatter).  n_scalars is a multiple
-// of 128 (64 scalars per list, 128 lists per blob).
-constexpr int kDigitMaxWindows = (256 + kCombMinBits - 1) / kCombMinBits;
-__global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, int c, int D,
+// Signed digits of every scalar in the table's windows (window k: width w_k
+// at bit b_k, digits in (-2^(w_k - 1), 2^(w_k - 1)]; the top window takes the
+// last carry, the scalars being below 2^255): scalar q = o 64 + i fills
+// dig[q D ..].  A block's 128 scalars are recoded into shared memory and
+// written out as one contiguous run of 16-byte stores (a thread's own digits
+// are D x 2 bytes apart from its neighbour's: direct stores would scatter).
+// n_scalars is a multiple of 128 (64 scalars per list, 128 lists per blob).
+constexpr int kDigitMaxWindows = kCombMaxWindows;
+__global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, CombWindows win,
                                                     int n_scalars) {
     __shared__ __align__(16) int16_t sd[128 * kDigitMaxWindows];
     const int q0 = blockIdx.x * 128, q = q0 + threadIdx.x;
     if (q0 >= n_scalars) return;
     const Fr sc = ld_vec(&scalars[q]);
-    const int H = 1 << (c - 1);
+    const int D = win.D;
     int carry = 0;
     for (int k = 0; k < D; k++) {
-        const int v = (int)scalar_window(sc, k * c, c) + carry;
-        carry = v > H ? 1 : 0;
-        sd[threadIdx.x * D + k] = (int16_t)(v - (carry << c));
+        const int w = win.width(k);
+        const int v = (int)scalar_window(sc, win.bit_off(k), w) + carry;
+        carry = v > (1 << (w - 1)) ? 1 : 0;
+        sd[threadIdx.x * D + k] = (int16_t)(v - (carry << w));
     }
     __syncthreads();
     const uint4 *src = reinterpret_cast<const uint4 *>(sd);
@@ -715,7 +731,7 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // the digit-table entry of digit v (nonzero) of element t of list o
 __device__ __forceinline__ const uint4 *comb_entry(const FlatArgs &a, uint32_t o, uint32_t t, int v) {
-    return reinterpret_cast<const uint4 *>(comb_at(a.comb, (size_t)(o % kCells) * a.per_j + (size_t)t * a.H + (abs(v) - 1)));
+    return reinterpret_cast<const uint4 *>(comb_at(a.comb, comb_index(a, o, t, v)));
 }
 
 // pass 1 of the first round: the x coordinates of each pair staged one pair ahead
@@ -973,10 +989,10 @@ int flat_blocks() {
     return sms * kFlatBlocksPerSM;
 }
 
-// Working set of the grid-wide rounds for cap blobs and window c.
-FlatSizes flat_sizes(int cap, int c) {
+// Working set of the grid-wide rounds for cap blobs and a table of D windows.
+FlatSizes flat_sizes(int cap, int windows) {
     FlatSizes z;
-    const size_t D = (256 + c - 1) / c, L = (size_t)kCellElems * D, lists = (size_t)cap * kCells;
+    const size_t D = (size_t)windows, L = (size_t)kCellElems * D, lists = (size_t)cap * kCells;
     z.blocks = flat_blocks();
     const size_t lanes = (size_t)z.blocks * kFlatThreads;
     z.dig = lists * L;
@@ -1144,14 +1160,16 @@ GridSync make_sync(const ProofWork &w, int n) {
 // Phase A of plan 3 for n blobs: digits, tree rounds, Jacobian outputs in
 // w.points.  Returns the number of kernels launched.
 int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
-    const int c = w.comb_c, D = (256 + c - 1) / c, L = kCellElems * D;
+    const int D = w.comb_windows, L = kCellElems * D;
     const int lists = n * kCells;
     FlatArgs a;
     a.dig = w.flat_dig;
     a.comb = w.comb;
-    a.H = 1 << (c - 1);
+    a.win = comb_windows(D);
+    a.per_i = a.win.entries();
+    a.per_j = (size_t)kCellElems * a.per_i;
+    a.dmagic = (uint32_t)(((1ull << 32) + (uint64_t)D - 1) / (uint64_t)D);
     a.L = L;
-    a.per_j = (size_t)L * a.H;
     a.pre = w.flat_pre;
     a.others = w.flat_others;
     a.tot = w.flat_tot;
@@ -1159,7 +1177,7 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.slots = w.flat_slots;
     a.n_lists = lists;
     int launched = 1;
-    k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, c, D, lists * kCellElems);
+    k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, a.win, lists * kCellElems);
     uint32_t m = (uint32_t)L;
     const G1A *res;
     if (w.coop) {
@@ -1645,12 +1663,14 @@ int launch_phase_b_flat(const DeviceTables &t, const ProofWork &w, int n, cudaSt
     return launched;
 }
 
-// Bases of the digit table: B[j][i][k] = 2^(c k) X[j][i], from the position
-// table entry 2^(8 floor(ck / 8)) X[j][i] and (ck mod 8) doublings.
-__global__ void __launch_bounds__(128) k_comb_bases(const G1A *__restrict__ pos, G1A *bases, int c, int D) {
+// Bases of the digit table: B[j][i][k] = 2^(b_k) X[j][i] (b_k the bit of
+// window k), from the position table entry 2^(8 floor(b_k / 8)) X[j][i] and
+// (b_k mod 8) doublings.
+__global__ void __launch_bounds__(128) k_comb_bases(const G1A *__restrict__ pos, G1A *bases, CombWindows win) {
+    const int D = win.D;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= kCells * kCellElems * D) return;
-    const int ji = idx / D, k = idx % D, bit = c * k;
+    const int ji = idx / D, k = idx % D, bit = win.bit_off(k);
     G1J p = g1_from_affine(ld_vec(&pos[(size_t)ji * kDigits + (bit >> 3)]));
     for (int r = 0; r < (bit & 7); r++) p = g1_dbl(p);
     G1A a;
@@ -1665,37 +1685,42 @@ __global__ void __launch_bounds__(128) k_comb_bases(const G1A *__restrict__ pos,
     st_vec(&bases[idx], a);
 }
 
-// Rows of the digit table, row[m - 1] = m B for m = 1..H (H a power of two),
-// built level by level: level L (L = 1, 2, 4, ..., H / 2) makes entries
-// L + 1..2L as (L + r) B = r B + L B for r = 1..L (r = L is a doubling).  The
-// additions of a level are independent, so one inversion per level serves all
-// of them for the warp's kCombRows rows: log2(H) inversions per row group
-// instead of one per table entry.
+// Rows of the digit table, row[m - 1] = m B for m = 1..H (H = 2^(width - 1) of
+// the base's window), built level by level: level L (L = 1, 2, 4, ..., H / 2)
+// makes entries L + 1..2L as (L + r) B = r B + L B for r = 1..L (r = L is a
+// doubling).  The additions of a level are independent, so one inversion per
+// level serves all of them for the warp's kCombRows rows: log2(H) inversions
+// per row group instead of one per table entry.  A warp's task is kCombRows
+// base columns of one window, so that its rows have one length; the row of
+// column ji and window k starts at entry ji per_i + entry_off(k).
 constexpr int kCombRows = 8;
 constexpr int kCombBuildThreads = 128;
 
 __host__ __device__ inline size_t comb_build_pre_words(int H) { return ((size_t)kCombRows * (H / 2) / 32 + 1) * 384; }
 
-__global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__restrict__ bases, G1A *comb, int H,
-                                                                 int n_bases, uint32_t *pre_all) {
+__global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__restrict__ bases, G1A *comb,
+                                                                 CombWindows win, int n_cols, uint32_t *pre_all) {
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * (kCombBuildThreads / 32) + (threadIdx.x >> 5);
     const int n_warps = gridDim.x * (kCombBuildThreads / 32);
-    uint32_t *pre = pre_all + (size_t)wid * comb_build_pre_words(H);
-    const int n_tasks = (n_bases + kCombRows - 1) / kCombRows;
+    uint32_t *pre = pre_all + (size_t)wid * comb_build_pre_words(1 << (win.widest() - 1));
+    const int D = win.D;
+    const uint32_t per_i = win.entries();
+    const int n_tasks = (n_cols + kCombRows - 1) / kCombRows * D;
     for (int task = wid; task < n_tasks; task += n_warps) {
-        const int b0 = task * kCombRows;
-        const uint32_t nb = (uint32_t)min(kCombRows, n_bases - b0);
-        G1A *rows = comb_at(comb, (size_t)b0 * H);
-        for (uint32_t r = lane; r < nb; r += 32) st_vec(comb_at(rows, (size_t)r * H), ld_vec(&bases[b0 + r]));
+        const int k = task % D, ji0 = task / D * kCombRows;
+        const uint32_t nb = (uint32_t)min(kCombRows, n_cols - ji0);
+        const uint32_t H = 1u << (win.width(k) - 1), off = win.entry_off(k);
+        auto entry = [&](uint32_t rb, uint32_t m) { return comb_at(comb, (size_t)(ji0 + rb) * per_i + off + m); };
+        for (uint32_t r = lane; r < nb; r += 32) st_vec(entry(r, 0), ld_vec(&bases[(size_t)(ji0 + r) * D + k]));
         __syncwarp();
-        for (uint32_t L = 1; L < (uint32_t)H; L <<= 1) {
+        for (uint32_t L = 1; L < H; L <<= 1) {
             const uint32_t P = nb * L;
             Fp acc = fp_one();
             int s = 0;
             for (uint32_t q = lane; q < P; q += 32, s++) {
                 const uint32_t rb = q / L, r = q - rb * L + 1;
-                const G1A x = ld_vec(comb_at(rows, (size_t)rb * H + r - 1)), y = ld_vec(comb_at(rows, (size_t)rb * H + L - 1));
+                const G1A x = ld_vec(entry(rb, r - 1)), y = ld_vec(entry(rb, L - 1));
                 wb_store_pre(pre, s, acc);
                 acc = fp_mul(acc, pair_denominator(x, y, pair_kind(x, y)));
             }
@@ -1703,21 +1728,20 @@ __global__ void __launch_bounds__(kCombBuildThreads) k_comb_table(const G1A *__r
             for (int t = s - 1; t >= 0; t--) {
                 const uint32_t q = lane + (uint32_t)t * 32;
                 const uint32_t rb = q / L, r = q - rb * L + 1;
-                const G1A x = ld_vec(comb_at(rows, (size_t)rb * H + r - 1)), y = ld_vec(comb_at(rows, (size_t)rb * H + L - 1));
+                const G1A x = ld_vec(entry(rb, r - 1)), y = ld_vec(entry(rb, L - 1));
                 const int kind = pair_kind(x, y);
                 const Fp den = pair_denominator(x, y, kind);
                 const Fp inv_den = fp_mul(inv, wb_load_pre(pre, t));
                 inv = fp_mul(inv, den);
-                st_vec(comb_at(rows, (size_t)rb * H + L + r - 1), pair_result(x, y, kind, inv_den));
+                st_vec(entry(rb, L + r - 1), pair_result(x, y, kind, inv_den));
             }
             __syncwarp();
         }
     }
 }
 
-// Digit table for window c (D = ceil(256 / c) windows) into comb; scratch holds
-// the bases (128 * 64 * D points) followed by the build's prefix products
-// (comb_build_scratch_bytes).
+// Digit table of D windows into comb; scratch holds the bases (128 * 64 * D
+// points) followed by the build's prefix products (comb_build_scratch_bytes).
 int comb_build_blocks() {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -1725,18 +1749,19 @@ int comb_build_blocks() {
     return sms * 4;
 }
 
-size_t comb_build_scratch_bytes(int c) {
-    const int D = (256 + c - 1) / c, H = 1 << (c - 1);
-    return (size_t)kCells * kCellElems * D * sizeof(G1A) +
-           (size_t)comb_build_blocks() * (kCombBuildThreads / 32) * comb_build_pre_words(H) * 4;
+size_t comb_build_scratch_bytes(int windows) {
+    const CombWindows win = comb_windows(windows);
+    return (size_t)kCells * kCellElems * win.D * sizeof(G1A) +
+           (size_t)comb_build_blocks() * (kCombBuildThreads / 32) * comb_build_pre_words(1 << (win.widest() - 1)) * 4;
 }
 
-cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int c, cudaStream_t s) {
-    const int D = (256 + c - 1) / c, n_bases = kCells * kCellElems * D;
+cudaError_t launch_comb_table(const DeviceTables &t, G1A *comb, void *scratch, int windows, cudaStream_t s) {
+    const CombWindows win = comb_windows(windows);
+    const int n_cols = kCells * kCellElems, n_bases = n_cols * win.D;
     G1A *bases = reinterpret_cast<G1A *>(scratch);
     uint32_t *pre = reinterpret_cast<uint32_t *>(bases + n_bases);
-    k_comb_bases<<<(n_bases + 127) / 128, 128, 0, s>>>(t.pos, bases, c, D);
-    k_comb_table<<<comb_build_blocks(), kCombBuildThreads, 0, s>>>(bases, comb, 1 << (c - 1), n_bases, pre);
+    k_comb_bases<<<(n_bases + 127) / 128, 128, 0, s>>>(t.pos, bases, win);
+    k_comb_table<<<comb_build_blocks(), kCombBuildThreads, 0, s>>>(bases, comb, win, n_cols, pre);
     count_launches(2);
     return cudaGetLastError();
 }

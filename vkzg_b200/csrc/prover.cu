@@ -63,7 +63,7 @@ static const char *kRecoverStageNames[kRecoverStages] = {"recover"};
 // with the same setup tables; freed with the last of them.
 struct CombTable {
     int device = 0;
-    int c = 0;
+    int windows = 0; // per scalar (CombWindows)
     G1A *d = nullptr;
     size_t bytes = 0;
     double build_ms = 0.0;
@@ -110,15 +110,15 @@ struct vkzg_prover {
     // setup tables); the shared digit table is counted apart, in comb->bytes
     uint64_t dev_bytes = 0, tables_bytes = 0;
     // digit table: byte budget ($VKZG_COMB_BUDGET_GB, default 20 GiB; a serving
-    // loop passes its own), the window the tuner chose (0 = not yet), and the
-    // window the phase-A round buffers are sized for (they serve any wider one)
+    // loop passes its own), the window count the tuner chose (0 = not yet), and
+    // the count the phase-A round buffers are sized for (they serve any smaller)
     uint64_t comb_budget = 20ull << 30;
     bool coop_off = false; // see vkzg::disable_coop
     bool trimmed = false;  // see vkzg::trim_working_set: only the tuned plans' buffers are left
     uint32_t plan0_cap = 0; // blobs the Jacobian bucket array holds once trimmed
-    int comb_c_chosen = 0, comb_buf_c = 0;
+    int comb_windows_chosen = 0, comb_buf_windows = 0;
     struct WindowTrial {
-        int c;
+        int windows;
         uint64_t bytes;
         double build_ms, ms;
     };
@@ -809,7 +809,7 @@ constexpr int kPlans = 5;
 // plan 3's table and buffers, from the prover's working set into a copy of it
 void take_comb(ProofWork &w, const ProofWork &from) {
     w.comb = from.comb;
-    w.comb_c = from.comb_c;
+    w.comb_windows = from.comb_windows;
     w.flat_dig = from.flat_dig;
     w.flat_buf[0] = from.flat_buf[0];
     w.flat_buf[1] = from.flat_buf[1];
@@ -882,19 +882,24 @@ std::string comb_choice_key(const vkzg_prover *p) {
     return std::to_string(p->device) + "|" + p->tables_id + "|" + std::to_string(p->comb_budget);
 }
 
-// $VKZG_COMB_BITS pins the digit table's window (0 disables the table; else
-// 8..14); -1 when unset.
-int comb_bits_forced() {
+// $VKZG_COMB_WINDOWS pins the digit table's windows per scalar (18..32), or
+// $VKZG_COMB_BITS its widest window (D = ceil(256 / bits): 8 bits 32 windows,
+// 14 bits 19, 15 bits 18); 0 in either disables the table; -1 when neither is
+// set.
+int comb_windows_forced() {
+    if (const char *e = getenv("VKZG_COMB_WINDOWS")) {
+        const int d = atoi(e);
+        return d <= 0 ? 0 : std::min(kCombMaxWindows, std::max(kCombMinWindows, d));
+    }
     if (const char *e = getenv("VKZG_COMB_BITS")) {
         const int c = atoi(e);
-        return c <= 0 ? 0 : std::min(kCombMaxBits, std::max(kCombMinBits, c));
+        return c <= 0 ? 0 : std::min(kCombMaxWindows, std::max(kCombMinWindows, (256 + c - 1) / c));
     }
     return -1;
 }
 
-size_t comb_bytes(int c) {
-    const size_t D = (256 + c - 1) / c;
-    return (size_t)kCells * kCellElems * D * ((size_t)1 << (c - 1)) * kCombEntryBytes;
+size_t comb_bytes(int windows) {
+    return (size_t)kCells * kCellElems * comb_windows(windows).entries() * kCombEntryBytes;
 }
 
 // The grid-wide rounds' shared working set (prefix products, per-lane and
@@ -904,7 +909,7 @@ bool ensure_flat_b(vkzg_prover *p) {
     if (w.flat_pre) return true;
     // (chunks beyond 4096 blobs would overflow the rounds' 32-bit pair indices)
     if (p->flat_failed || p->t.fb_rounds == 0 || p->cap > 4096) return false;
-    const FlatSizes z = flat_sizes((int)p->cap, kCombMinBits); // its slots cover every window and phase B
+    const FlatSizes z = flat_sizes((int)p->cap, kCombMaxWindows); // its slots cover every table and phase B
     if (!p->alloc(w.flat_pre, z.pre_words) || !p->alloc(w.flat_others, z.lanes) ||
         !p->alloc(w.flat_tot, z.lanes / 32) || !p->alloc(w.flat_totinv, z.lanes / 32) ||
         !p->alloc(w.flatb_buf[0], (size_t)p->cap * kCells * std::max<uint32_t>(1, p->t.fb_stride[0])) ||
@@ -929,30 +934,31 @@ bool ensure_flat_b(vkzg_prover *p) {
     return true;
 }
 
-// Windows the tuner tries, widest first: the widest whose table fits the
-// prover's budget and the two below it (8..14 bits; each bit less halves the
-// table and adds ~5 % to phase A's additions), or the pinned or chosen one.
+// Window counts the tuner tries, largest table first: the fewest windows
+// whose table fits the prover's budget and the next two (each window more
+// adds 64 points to every phase-A output, ~5 %, and shrinks the table by
+// about a third), or the pinned or chosen count.
 std::vector<int> comb_candidates(const vkzg_prover *p) {
-    const int forced = comb_bits_forced();
+    const int forced = comb_windows_forced();
     if (forced == 0) return {};
     if (forced > 0) return {forced};
-    if (p->comb_c_chosen) return {p->comb_c_chosen};
+    if (p->comb_windows_chosen) return {p->comb_windows_chosen};
     {
         std::lock_guard<std::mutex> lk(g_comb_mu);
         auto it = g_comb_choice.find(comb_choice_key(p));
         if (it != g_comb_choice.end()) return {it->second};
     }
     std::vector<int> out;
-    for (int c = kCombMaxBits; c >= kCombMinBits && out.size() < 3; c--)
-        if (comb_bytes(c) <= p->comb_budget) out.push_back(c);
+    for (int d = kCombMinWindows; d <= kCombMaxWindows && out.size() < 3; d++)
+        if (comb_bytes(d) <= p->comb_budget) out.push_back(d);
     return out;
 }
 
-// This prover's phase-A round buffers, sized for window c_min (narrower
-// windows mean longer lists): they then serve every window >= c_min.
-bool comb_buffers(vkzg_prover *p, int c_min) {
-    if (p->comb_buf_c) return c_min >= p->comb_buf_c;
-    const FlatSizes z = flat_sizes((int)p->cap, c_min);
+// This prover's phase-A round buffers, sized for d_max windows (more windows
+// mean longer lists): they then serve every count <= d_max.
+bool comb_buffers(vkzg_prover *p, int d_max) {
+    if (p->comb_buf_windows) return d_max <= p->comb_buf_windows;
+    const FlatSizes z = flat_sizes((int)p->cap, d_max);
     ProofWork &w = p->pw;
     if (!ensure_flat_b(p) || !p->alloc(w.flat_dig, z.dig) || !p->alloc(w.flat_buf[0], z.buf0) ||
         !p->alloc(w.flat_buf[1], z.buf1)) {
@@ -960,35 +966,35 @@ bool comb_buffers(vkzg_prover *p, int c_min) {
         w.flat_dig = nullptr;
         return false;
     }
-    p->comb_buf_c = c_min;
+    p->comb_buf_windows = d_max;
     return true;
 }
 
 void drop_comb(vkzg_prover *p) {
     p->comb.reset();
     p->pw.comb = nullptr;
-    p->pw.comb_c = 0;
+    p->pw.comb_windows = 0;
 }
 
-// Shares or builds the digit table of window c (a new one only when it fits in
-// free device memory with 4 GB to spare); the prover's previous table, if
+// Shares or builds the digit table of d windows (a new one only when it fits
+// in free device memory with 4 GB to spare); the prover's previous table, if
 // another, is released first.
-bool use_comb(vkzg_prover *p, int c) {
-    if (p->comb && p->comb->c == c) return true;
+bool use_comb(vkzg_prover *p, int d) {
+    if (p->comb && p->comb->windows == d) return true;
     drop_comb(p);
-    if (!comb_buffers(p, c)) return false;
+    if (!comb_buffers(p, d)) return false;
     std::lock_guard<std::mutex> lk(g_comb_mu);
-    const std::string key = std::to_string(p->device) + "|" + std::to_string(c) + "|" + p->tables_id;
+    const std::string key = std::to_string(p->device) + "|" + std::to_string(d) + "|" + p->tables_id;
     auto it = g_comb.find(key);
     if (it != g_comb.end()) p->comb = it->second.lock();
     if (!p->comb) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
-        const size_t bytes = comb_bytes(c);
-        if (free_b < bytes + comb_build_scratch_bytes(c) + (4ull << 30)) return false;
+        const size_t bytes = comb_bytes(d);
+        if (free_b < bytes + comb_build_scratch_bytes(d) + (4ull << 30)) return false;
         auto t = std::make_shared<CombTable>();
         t->device = p->device;
-        t->c = c;
+        t->windows = d;
         t->bytes = bytes;
         if (cudaMalloc(&t->d, bytes) != cudaSuccess) {
             t->d = nullptr;
@@ -996,12 +1002,12 @@ bool use_comb(vkzg_prover *p, int c) {
             return false;
         }
         void *scratch = nullptr;
-        if (cudaMalloc(&scratch, comb_build_scratch_bytes(c)) != cudaSuccess) {
+        if (cudaMalloc(&scratch, comb_build_scratch_bytes(d)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
         const auto t0 = std::chrono::steady_clock::now();
-        cudaError_t e = launch_comb_table(p->t, t->d, scratch, c, p->stream);
+        cudaError_t e = launch_comb_table(p->t, t->d, scratch, d, p->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
         cudaFree(scratch);
         if (e != cudaSuccess) return false;
@@ -1010,19 +1016,19 @@ bool use_comb(vkzg_prover *p, int c) {
         p->comb = t;
     }
     p->pw.comb = p->comb->d;
-    p->pw.comb_c = p->comb->c;
+    p->pw.comb_windows = p->comb->windows;
     return true;
 }
 
-// The digit table of the chosen window, or of the widest candidate that can be
-// had (plan 3 outside the tuner: device-pointer calls, adopted tuning).
+// The digit table of the chosen window count, or of the largest candidate that
+// can be had (plan 3 outside the tuner: device-pointer calls, adopted tuning).
 bool ensure_comb(vkzg_prover *p) {
     if (p->comb) return true;
     if (p->comb_failed) return false;
     const std::vector<int> cands = comb_candidates(p);
     if (!cands.empty() && comb_buffers(p, cands.back()))
-        for (int c : cands)
-            if (use_comb(p, c)) return true;
+        for (int d : cands)
+            if (use_comb(p, d)) return true;
     p->comb_failed = true;
     return false;
 }
@@ -1038,7 +1044,8 @@ void save_tune_cache(const vkzg_prover *p) {
     FILE *f = fopen(p->tune_cache.c_str(), "w");
     if (!f) return;
     for (const auto &kv : p->plan_of) fprintf(f, "%s|%u|%u %d\n", p->name.c_str(), p->sm_count, kv.first, kv.second);
-    if (p->comb_c_chosen) fprintf(f, "%s|%u|window %d\n", p->name.c_str(), p->sm_count, p->comb_c_chosen);
+    if (p->comb_windows_chosen)
+        fprintf(f, "%s|%u|windows %d\n", p->name.c_str(), p->sm_count, p->comb_windows_chosen);
     fclose(f);
 }
 
@@ -1054,9 +1061,9 @@ void load_tune_cache(vkzg_prover *p) {
         unsigned c = 0;
         int plan = -1, window = 0;
         if (sscanf(l.c_str() + key.size(), "%u %d", &c, &plan) == 2 && plan >= 0 && plan < kPlans) p->plan_of[c] = plan;
-        else if (sscanf(l.c_str() + key.size(), "window %d", &window) == 1 && window >= kCombMinBits &&
-                 window <= kCombMaxBits && comb_bytes(window) <= p->comb_budget)
-            p->comb_c_chosen = window;
+        else if (sscanf(l.c_str() + key.size(), "windows %d", &window) == 1 && window >= kCombMinWindows &&
+                 window <= kCombMaxWindows && comb_bytes(window) <= p->comb_budget)
+            p->comb_windows_chosen = window;
     }
     fclose(f);
 }
@@ -1085,31 +1092,31 @@ vkzg_result tune_chunk(vkzg_prover *p, ProofWork w, uint32_t n) {
         ms[plan] = 1e30; // not available at this size or in this memory
         if (plan == 4 && !ensure_flat_b(p)) continue;
         if (plan == 3) {
-            // the digit table's window: every candidate timed, its table size
-            // the cost (the budget bounds it), the fastest kept
+            // the digit table's window count: every candidate timed, its table
+            // size the cost (the budget bounds it), the fastest kept
             const std::vector<int> cands = n >= kCombMinBlobs ? comb_candidates(p) : std::vector<int>{};
             if (cands.empty() || !comb_buffers(p, cands.back())) continue;
             std::vector<vkzg_prover::WindowTrial> trials;
-            int best_c = 0;
-            for (int c : cands) {
-                if (!use_comb(p, c)) continue;
+            int best_d = 0;
+            for (int d : cands) {
+                if (!use_comb(p, d)) continue;
                 double t = 0.0;
                 const vkzg_result rc = time_plan(3, t);
                 if (rc != VKZG_OK) return rc;
-                trials.push_back({c, p->comb->bytes, p->comb->build_ms, t});
+                trials.push_back({d, p->comb->bytes, p->comb->build_ms, t});
                 if (t < ms[3]) {
                     ms[3] = t;
-                    best_c = c;
+                    best_d = d;
                 }
             }
             p->window_trials[size_class(n)] = trials;
-            if (best_c) {
-                p->comb_c_chosen = best_c;
-                if (comb_bits_forced() < 0) {
+            if (best_d) {
+                p->comb_windows_chosen = best_d;
+                if (comb_windows_forced() < 0) {
                     std::lock_guard<std::mutex> lk(g_comb_mu);
-                    g_comb_choice[comb_choice_key(p)] = best_c;
+                    g_comb_choice[comb_choice_key(p)] = best_d;
                 }
-                if (!use_comb(p, best_c)) ms[3] = 1e30;
+                if (!use_comb(p, best_d)) ms[3] = 1e30;
             }
             continue;
         }
@@ -1753,7 +1760,7 @@ void adopt_tuning(vkzg_prover *dst, const vkzg_prover *src) {
     if (cudaSetDevice(dst->device) != cudaSuccess) return;
     bool want_comb = false, want_flat = false;
     dst->comb_budget = src->comb_budget;
-    dst->comb_c_chosen = src->comb_c_chosen;
+    dst->comb_windows_chosen = src->comb_windows_chosen;
     for (const auto &kv : src->plan_of) {
         dst->plan_of[kv.first] = kv.second;
         want_comb |= kv.second == 3;
@@ -1770,7 +1777,7 @@ int vkzg_b200_digit_table(const vkzg_prover *p, double *build_ms, uint64_t *byte
     if (!p || !p->comb) return 0;
     if (build_ms) *build_ms = p->comb->build_ms;
     if (bytes) *bytes = p->comb->bytes;
-    return p->comb->c;
+    return p->comb->windows;
 }
 
 void vkzg_b200_prover_device_bytes(const vkzg_prover *p, uint64_t *working, uint64_t *tables, uint64_t *digit_table) {
@@ -1779,7 +1786,7 @@ void vkzg_b200_prover_device_bytes(const vkzg_prover *p, uint64_t *working, uint
     if (digit_table) *digit_table = p && p->comb ? p->comb->bytes : 0;
 }
 
-int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *window_bits, uint64_t *table_bytes,
+int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *windows, uint64_t *table_bytes,
                             double *build_ms, double *ms, int cap) {
     if (!p) return 0;
     auto it = p->window_trials.find(size_class);
@@ -1787,7 +1794,7 @@ int vkzg_b200_window_trials(const vkzg_prover *p, uint32_t size_class, int *wind
     int i = 0;
     for (const auto &t : it->second) {
         if (i < cap) {
-            if (window_bits) window_bits[i] = t.c;
+            if (windows) windows[i] = t.windows;
             if (table_bytes) table_bytes[i] = t.bytes;
             if (build_ms) build_ms[i] = t.build_ms;
             if (ms) ms[i] = t.ms;
