@@ -141,7 +141,7 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
     return v;
 }
 
-static __device__ __noinline__ bool grid_sync(const GridSync &g) {
+static __device__ __forceinline__ bool grid_sync(const GridSync g) {
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
