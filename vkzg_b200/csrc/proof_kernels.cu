@@ -715,6 +715,16 @@ __device__ __forceinline__ void pair_step_down(uint32_t &o, uint32_t &i, uint32_
 #define VKZG_GATHER_PREFETCH 1
 #endif
 constexpr bool kGatherPrefetch = VKZG_GATHER_PREFETCH != 0;
+// the same staging in the later rounds, from the round's input lists (a build
+// switch, off: their pairs are coalesced runs of lists that stay largely in
+// L2, and staged they measured slower, phase A 12.04 against 11.84 ms at 256
+// blobs and 18 windows)
+#ifndef VKZG_LIST_PREFETCH
+#define VKZG_LIST_PREFETCH 0
+#endif
+constexpr bool kListPrefetch = kGatherPrefetch && VKZG_LIST_PREFETCH != 0;
+template <bool FIRST>
+constexpr bool kStaged = FIRST ? kGatherPrefetch : kListPrefetch;
 constexpr int kStageChunks = 12; // two 96-byte points
 constexpr size_t kStage1Bytes = 2 * 6 * kFlatThreads * sizeof(uint4);            // pass 1: x coordinates
 constexpr size_t kStage2Bytes = 2 * kStageChunks * kFlatThreads * sizeof(uint4); // pass 2: whole points
@@ -734,8 +744,10 @@ __device__ __forceinline__ const uint4 *comb_entry(const FlatArgs &a, uint32_t o
     return reinterpret_cast<const uint4 *>(comb_at(a.comb, comb_index(a, o, t, v)));
 }
 
-// pass 1 of the first round: the x coordinates of each pair staged one pair ahead
-__device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, uint32_t gl, uint32_t NL) {
+// pass 1 with the x coordinates of each pair staged one pair ahead, from the
+// digit table (FIRST) or from the round's input lists
+template <bool FIRST>
+__device__ __forceinline__ void flat_pass1_staged(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
     extern __shared__ uint4 stage[];
     uint4 *my = stage + threadIdx.x; // chunk c of buffer b: my[(b * 6 + c) * kFlatThreads]
     const uint32_t wg = gl >> 5;
@@ -743,18 +755,24 @@ __device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, 
     const uint32_t P = (uint32_t)a.n_lists * h;
     const uint32_t dq = NL / h, dr = NL % h;
     uint32_t *pre = a.pre + (size_t)wg * a.slots * 384;
-    const RoundIO io{nullptr, nullptr};
     auto issue = [&](int b, uint32_t o, uint32_t i, int &v0, int &v1) {
-        const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
-        v0 = d[0];
-        v1 = d[1];
-        if (v0) {
-            const uint4 *src = comb_entry(a, o, 2 * i, v0);
+        if constexpr (FIRST) {
+            const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
+            v0 = d[0];
+            v1 = d[1];
+            if (v0) {
+                const uint4 *src = comb_entry(a, o, 2 * i, v0);
+                for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + c) * kFlatThreads], src + c);
+            }
+            if (v1) {
+                const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
+                for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + 3 + c) * kFlatThreads], src + c);
+            }
+        } else {
+            v0 = v1 = 1; // list points are stored whole, infinity as (0, 0)
+            const uint4 *src = reinterpret_cast<const uint4 *>(&io.src[(size_t)o * m + 2 * i]);
             for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + c) * kFlatThreads], src + c);
-        }
-        if (v1) {
-            const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
-            for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + 3 + c) * kFlatThreads], src + c);
+            for (int c = 0; c < 3; c++) cp_async16(&my[(b * 6 + 3 + c) * kFlatThreads], src + 6 + c);
         }
         cp_async_commit();
     };
@@ -781,8 +799,8 @@ __device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, 
         }
         const Fp x = x_of(s & 1, 0, v0), y = x_of(s & 1, 1, v1);
         wb_store_pre(pre, s, acc);
-        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<true>(a, io, o, 2 * i, m); },
-                                             [&] { return flat_load<true>(a, io, o, 2 * i + 1, m); }));
+        acc = fp_mul(acc, pair_denominator_x(x, y, [&] { return flat_load<FIRST>(a, io, o, 2 * i, m); },
+                                             [&] { return flat_load<FIRST>(a, io, o, 2 * i + 1, m); }));
         o = on;
         i = in;
         v0 = w0;
@@ -793,8 +811,8 @@ __device__ __forceinline__ void flat_pass1_first(const FlatArgs &a, uint32_t m, 
 
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass1_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
-    if constexpr (FIRST && kGatherPrefetch) {
-        flat_pass1_first(a, m, gl, NL);
+    if constexpr (kStaged<FIRST>) {
+        flat_pass1_staged<FIRST>(a, io, m, gl, NL);
         return;
     }
     const uint32_t wg = gl >> 5;
@@ -850,8 +868,10 @@ static void launch_flat_invert(const Fp *tot, Fp *totinv, int n, cudaStream_t s)
 #define VKZG_PASS2_INLINE 0
 #endif
 constexpr bool kPass2Inline = VKZG_PASS2_INLINE != 0;
-// pass 2 of the first round: the two points of each pair staged one pair ahead
-__device__ __forceinline__ void flat_pass2_first(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
+// pass 2 with the two points of each pair staged one pair ahead, from the
+// digit table (FIRST) or from the round's input lists
+template <bool FIRST>
+__device__ __forceinline__ void flat_pass2_staged(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
     extern __shared__ uint4 stage[];
     uint4 *my = stage + threadIdx.x; // chunk c of buffer b: my[(b * kStageChunks + c) * kFlatThreads]
     const uint32_t wg = gl >> 5;
@@ -862,16 +882,22 @@ __device__ __forceinline__ void flat_pass2_first(const FlatArgs &a, RoundIO io, 
     Fp inv = fp_mul(ld_vec(&a.totinv[wg]), ld_vec(&a.others[gl]));
     const int S = P > gl ? (int)((P - gl + NL - 1) / NL) : 0;
     auto issue = [&](int b, uint32_t o, uint32_t i, int &v0, int &v1) {
-        const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
-        v0 = d[0];
-        v1 = d[1];
-        if (v0) {
-            const uint4 *src = comb_entry(a, o, 2 * i, v0);
-            for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + c) * kFlatThreads], src + c);
-        }
-        if (v1) {
-            const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
-            for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + 6 + c) * kFlatThreads], src + c);
+        if constexpr (FIRST) {
+            const int16_t *d = a.dig + (size_t)o * a.L + 2 * i;
+            v0 = d[0];
+            v1 = d[1];
+            if (v0) {
+                const uint4 *src = comb_entry(a, o, 2 * i, v0);
+                for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + c) * kFlatThreads], src + c);
+            }
+            if (v1) {
+                const uint4 *src = comb_entry(a, o, 2 * i + 1, v1);
+                for (int c = 0; c < 6; c++) cp_async16(&my[(b * kStageChunks + 6 + c) * kFlatThreads], src + c);
+            }
+        } else {
+            v0 = v1 = 1; // the pair's two points, 192 contiguous bytes of the list
+            const uint4 *src = reinterpret_cast<const uint4 *>(&io.src[(size_t)o * m + 2 * i]);
+            for (int c = 0; c < kStageChunks; c++) cp_async16(&my[(b * kStageChunks + c) * kFlatThreads], src + c);
         }
         cp_async_commit();
     };
@@ -918,13 +944,13 @@ __device__ __forceinline__ void flat_pass2_first(const FlatArgs &a, RoundIO io, 
     }
     if (m & 1u)
         for (uint32_t l = gl; l < (uint32_t)a.n_lists; l += NL)
-            st_vec(&io.dst[(size_t)l * m_next + h], flat_load<true>(a, io, l, m - 1, m));
+            st_vec(&io.dst[(size_t)l * m_next + h], flat_load<FIRST>(a, io, l, m - 1, m));
 }
 
 template <bool FIRST>
 __device__ __forceinline__ void flat_pass2_body(const FlatArgs &a, RoundIO io, uint32_t m, uint32_t gl, uint32_t NL) {
-    if constexpr (FIRST && kGatherPrefetch) {
-        flat_pass2_first(a, io, m, gl, NL);
+    if constexpr (kStaged<FIRST>) {
+        flat_pass2_staged<FIRST>(a, io, m, gl, NL);
         return;
     }
     const uint32_t wg = gl >> 5;
@@ -1020,11 +1046,11 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t *m_io, uin
     while (m > stop) {
         a.src = cur;
         a.dst = bufs[out];
-        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, FIRST && kGatherPrefetch ? kStage1Bytes : 0, s>>>(a, m);
-        else k_flat_pass1<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        if (first) k_flat_pass1<FIRST><<<blocks, kFlatThreads, kStaged<FIRST> ? kStage1Bytes : 0, s>>>(a, m);
+        else k_flat_pass1<false><<<blocks, kFlatThreads, kStaged<false> ? kStage1Bytes : 0, s>>>(a, m);
         launch_flat_invert(a.tot, a.totinv, warps, s);
-        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, FIRST && kGatherPrefetch ? kStage2Bytes : 0, s>>>(a, m);
-        else k_flat_pass2<false><<<blocks, kFlatThreads, 0, s>>>(a, m);
+        if (first) k_flat_pass2<FIRST><<<blocks, kFlatThreads, kStaged<FIRST> ? kStage2Bytes : 0, s>>>(a, m);
+        else k_flat_pass2<false><<<blocks, kFlatThreads, kStaged<false> ? kStage2Bytes : 0, s>>>(a, m);
         *launched += 3;
         cur = bufs[out];
         out ^= 1;
@@ -1033,6 +1059,15 @@ const G1A *run_tree_rounds(FlatArgs a, const G1A *first_src, uint32_t *m_io, uin
     }
     *m_io = m;
     return cur;
+}
+
+// The later rounds' pass kernels stage their pairs in dynamic shared memory.
+static cudaError_t configure_list_rounds() {
+    if (!kListPrefetch) return cudaSuccess;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_flat_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage1Bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_flat_pass2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage2Bytes);
 }
 
 // Sums of n_lists lists of m points (list o at lists[o m ..]) by the same
@@ -1049,6 +1084,7 @@ int launch_tree_sums(const G1A *lists, int n_lists, uint32_t m, G1A *buf0, G1A *
     a.slots = slots;
     a.n_lists = n_lists;
     int launched = 0;
+    if (configure_list_rounds() != cudaSuccess) return 0;
     const G1A *res = run_tree_rounds<false>(a, lists, &m, 1, buf0, buf1, blocks, s, &launched);
     cudaMemcpyAsync(sums, res, (size_t)n_lists * sizeof(G1A), cudaMemcpyDeviceToDevice, s);
     count_launches(launched);
@@ -2349,6 +2385,8 @@ cudaError_t configure_proof_kernels() {
     e = cudaFuncSetAttribute(k_flat_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage1Bytes);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_flat_pass2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStage2Bytes);
+    if (e != cudaSuccess) return e;
+    e = configure_list_rounds();
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_phase_b_affine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhaseBSmem);
 }
