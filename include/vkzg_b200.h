@@ -112,11 +112,11 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * k_bucket_reduce.comp); 1 = batch-affine bucket accumulation and a
  * binary-split batch-affine reduction; 2 = batch-affine accumulation with the
  * serial reduction; 3 = phase A as plain sums over a precomputed digit table
- * (every signed c-bit digit multiple of every base, c = 13 by default: 64 GB
- * of HBM, built on first use and shared by the process's provers with the same
- * setup; $VKZG_COMB_BITS picks c in 10..14 or 0 to disable it; smaller c is used
- * when free memory is short) summed in grid-wide batch-affine rounds, phase B
- * also in grid-wide rounds; 4 = phase A as plan 1, phase B as plan 3 (no digit
+ * (every signed digit multiple of every base in each of D windows, sized by a
+ * byte budget as described below, built on first use and shared by the
+ * process's provers with the same setup; a smaller table is used when free
+ * memory is short) summed in grid-wide batch-affine rounds, phase B also in
+ * grid-wide rounds; 4 = phase A as plan 1, phase B as plan 3 (no digit
  * table).  The first chunk of each
  * power-of-two size class is timed under all plans and the fastest is kept
  * (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
