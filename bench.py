@@ -683,13 +683,19 @@ def run_ours(args, rank, world, local_rank):
         build()
         c = cpu_rates(args.cpu_sample, args.cpu_sample)
         one = cpu_rates(2, 4, threads=1)
+        # all host threads at batches of 1 and 16 blobs beside the main sample
+        # (blobs run in parallel, one thread each, so a batch of 1 uses one)
+        small = {k: cpu_rates(k, k, seed=11 + k) for k in (1, 16)}
         cpu = {"value": c["combined"], "unit": "blobs/s", "cores": c["threads"], "kind": "port",
                "sample": f"{args.cpu_sample} proof blobs + {args.cpu_sample} recovery blobs of the same workload "
                          f"on {c['threads']} host threads ({c['seconds']:.1f} s)",
                "proof_blobs_per_s": c["proof_blobs_per_s"], "recovery_blobs_per_s": c["recovery_blobs_per_s"],
                "single_core": {"proof_blobs_per_s": one["proof_blobs_per_s"],
                                "recovery_blobs_per_s": one["recovery_blobs_per_s"],
-                               "sample": "2 proof blobs + 4 recovery blobs on 1 thread"}}
+                               "sample": "2 proof blobs + 4 recovery blobs on 1 thread"},
+               "all_cores_by_batch": {str(k): {"proof_blobs_per_s": r["proof_blobs_per_s"],
+                                               "recovery_blobs_per_s": r["recovery_blobs_per_s"]}
+                                      for k, r in [(1, small[1]), (16, small[16]), (args.cpu_sample, c)]}}
 
     line = {
         "metric": METRIC, "value": value, "unit": "blobs/s", "n_gpus": world, "steps": args.steps,
