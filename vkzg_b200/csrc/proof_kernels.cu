@@ -990,8 +990,9 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_flat_pass2(F
 // inversion launch each for little work.  Two threads per list, each a chain of
 // mixed additions over alternate points, then one addition.
 constexpr uint32_t kTreeTail = 10;
-__global__ void __launch_bounds__(64) k_flat_finish(const G1A *__restrict__ lists, uint32_t m, G1J *points, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// thread t of the tail: half t & 1 of list t >> 1 (all 32 lanes of a warp call
+// it together: the halves meet by a shuffle)
+__device__ __forceinline__ void flat_finish_body(const G1A *lists, uint32_t m, G1J *points, int n, int t) {
     const int o = t >> 1, h = t & 1;
     G1J acc = g1_identity();
     if (o < n) {
@@ -1006,6 +1007,9 @@ __global__ void __launch_bounds__(64) k_flat_finish(const G1A *__restrict__ list
         other.z.v[w] = __shfl_xor_sync(0xffffffffu, acc.z.v[w], 1);
     }
     if (o < n && h == 0) st_vec(&points[o], g1_add(acc, other));
+}
+__global__ void __launch_bounds__(64) k_flat_finish(const G1A *__restrict__ lists, uint32_t m, G1J *points, int n) {
+    flat_finish_body(lists, m, points, n, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 int flat_blocks() {
@@ -1132,19 +1136,28 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_tree(Fl
                                                                G1A *buf1, uint32_t m, uint32_t stop, GridSync g) {
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     RoundIO io{first_src, buf0};
-    bool first = FIRST;
-    while (m > stop) {
-        if (FIRST && first) coop_flat_pass1<true>(a, io, m, gl, NL);
-        else coop_flat_pass1<false>(a, io, m, gl, NL);
+    if constexpr (FIRST) {
+        // the first round alone (from the digit table, into buf0): its pass
+        // bodies differ from the later rounds', and one kernel holding both
+        // forms of both passes outgrew its registers and instruction cache
+        (void)buf1;
+        (void)stop;
+        coop_flat_pass1<true>(a, io, m, gl, NL);
         if (!grid_sync(g)) return;
         coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
         if (!grid_sync(g)) return;
-        if (FIRST && first) coop_flat_pass2<true>(a, io, m, gl, NL);
-        else coop_flat_pass2<false>(a, io, m, gl, NL);
+        coop_flat_pass2<true>(a, io, m, gl, NL);
+        return;
+    }
+    while (m > stop) {
+        coop_flat_pass1<false>(a, io, m, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
+        if (!grid_sync(g)) return;
+        coop_flat_pass2<false>(a, io, m, gl, NL);
         io.src = io.dst;
         io.dst = io.dst == buf0 ? buf1 : buf0;
         m = (m + 1) >> 1;
-        first = false;
         if (m > stop && !grid_sync(g)) return;
     }
 }
@@ -1217,10 +1230,18 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     uint32_t m = (uint32_t)L;
     const G1A *res;
     if (w.coop) {
+        // round 1 (digit table -> buf0), then the later rounds ping-ponging
+        // buf1, buf0, ... as the separate launches do (tree_result)
+        const uint32_t m0 = m;
         launch_coop(k_coop_tree<true>, w.flat_blocks, kStage2Bytes, s, a, (const G1A *)nullptr, w.flat_buf[0],
-                    w.flat_buf[1], m, kTreeTail, make_sync(w, n));
-        res = tree_result(nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1]);
+                    w.flat_buf[1], m0, (m0 + 1) >> 1, make_sync(w, n));
         launched++;
+        if (((m0 + 1) >> 1) > kTreeTail) {
+            launch_coop(k_coop_tree<false>, w.flat_blocks, 0, s, a, (const G1A *)w.flat_buf[0], w.flat_buf[1],
+                        w.flat_buf[0], (m0 + 1) >> 1, kTreeTail, make_sync(w, n));
+            launched++;
+        }
+        res = tree_result(nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1]);
     } else {
         res = run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s,
                                     &launched);
@@ -2360,7 +2381,7 @@ bool coop_supported(int blocks_per_sm) {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
         return false;
-    int a = 0, b = 0, c = 0, d = 0;
+    int a = 0, b = 0, c = 0, d = 0, e = 0;
     if (cudaFuncSetAttribute(k_coop_phase_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlatBSmem) !=
         cudaSuccess)
         return false;
@@ -2371,7 +2392,8 @@ bool coop_supported(int blocks_per_sm) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_coop_norm, kFlatThreads, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_coop_phase_b, kFlatThreads, kFlatBSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_coop_reduce, kFlatThreads, 0);
-    return std::min(std::min(a, b), std::min(c, d)) >= blocks_per_sm;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, k_coop_tree<false>, kFlatThreads, 0);
+    return std::min(std::min(std::min(a, b), std::min(c, d)), e) >= blocks_per_sm;
 }
 
 cudaError_t configure_proof_kernels() {
