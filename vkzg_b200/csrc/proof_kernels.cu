@@ -567,6 +567,7 @@ constexpr int kFlatBlocksPerSM = VKZG_FLAT_BLOCKS_PER_SM;
 
 struct FlatArgs {
     const int16_t *dig;  // [list][64 D] signed digits
+    const Fr *scalars;   // [list][64] phase-A scalars (the persistent form recodes them itself)
     const G1A *comb;     // digit table
     size_t per_j;        // points per column j of the table (64 per_i)
     uint32_t per_i;      // points per base column (j, i): win.entries()
@@ -661,12 +662,12 @@ __device__ __forceinline__ Fp flat_load_x(const FlatArgs &a, RoundIO io, uint32_
 // are D x 2 bytes apart from its neighbour's: direct stores would scatter).
 // n_scalars is a multiple of 128 (64 scalars per list, 128 lists per blob).
 constexpr int kDigitMaxWindows = kCombMaxWindows;
-__global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, CombWindows win,
-                                                    int n_scalars) {
-    __shared__ __align__(16) int16_t sd[128 * kDigitMaxWindows];
-    const int q0 = blockIdx.x * 128, q = q0 + threadIdx.x;
-    if (q0 >= n_scalars) return;
-    const Fr sc = ld_vec(&scalars[q]);
+// the block's group of blockDim.x scalars from q0 (a multiple of 128), staged
+// in sd (blockDim.x x D int16, 16-byte aligned); the caller syncs before
+// reusing sd
+__device__ __forceinline__ void flat_digits_group(const Fr *__restrict__ scalars, int16_t *dig, CombWindows win,
+                                                  int q0, int16_t *sd) {
+    const Fr sc = ld_vec(&scalars[q0 + threadIdx.x]);
     const int D = win.D;
     int carry = 0;
     for (int k = 0; k < D; k++) {
@@ -677,8 +678,15 @@ __global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scal
     }
     __syncthreads();
     const uint4 *src = reinterpret_cast<const uint4 *>(sd);
-    uint4 *dst = reinterpret_cast<uint4 *>(dig + (size_t)q0 * D); // 256 D bytes per block: 16-byte aligned
-    for (int x = threadIdx.x; x < 16 * D; x += 128) dst[x] = src[x];
+    uint4 *dst = reinterpret_cast<uint4 *>(dig + (size_t)q0 * D); // 256 D bytes per 128 scalars: 16-byte aligned
+    for (int x = threadIdx.x; x < (int)blockDim.x * D / 8; x += blockDim.x) dst[x] = src[x];
+}
+__global__ void __launch_bounds__(128) k_flat_digits(const Fr *__restrict__ scalars, int16_t *dig, CombWindows win,
+                                                    int n_scalars) {
+    __shared__ __align__(16) int16_t sd[128 * kDigitMaxWindows];
+    const int q0 = blockIdx.x * 128;
+    if (q0 >= n_scalars) return;
+    flat_digits_group(scalars, dig, win, q0, sd);
 }
 
 // Pair p = o h + i of a round (list o, pair i); a lane walks p = gl, gl + NL,
@@ -1137,11 +1145,23 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_tree(Fl
     const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x, NL = gridDim.x * blockDim.x;
     RoundIO io{first_src, buf0};
     if constexpr (FIRST) {
-        // the first round alone (from the digit table, into buf0): its pass
-        // bodies differ from the later rounds', and one kernel holding both
-        // forms of both passes outgrew its registers and instruction cache
+        // the scalars' digits (k_flat_digits), staged in the round's shared
+        // memory before pass 1 needs it, then the first round alone (from the
+        // digit table, into buf0): its pass bodies differ from the later
+        // rounds', and one kernel holding both forms of both passes outgrew
+        // its registers and instruction cache
         (void)buf1;
         (void)stop;
+        {
+            extern __shared__ uint4 stage[];
+            int16_t *sd = reinterpret_cast<int16_t *>(stage); // kFlatThreads x D int16 of the staging
+            const int n_scalars = a.n_lists * kCellElems;
+            for (int q0 = blockIdx.x * kFlatThreads; q0 < n_scalars; q0 += gridDim.x * kFlatThreads) {
+                flat_digits_group(a.scalars, const_cast<int16_t *>(a.dig), a.win, q0, sd);
+                __syncthreads();
+            }
+        }
+        if (!grid_sync(g)) return;
         coop_flat_pass1<true>(a, io, m, gl, NL);
         if (!grid_sync(g)) return;
         coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
@@ -1218,6 +1238,7 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.per_i = a.win.entries();
     a.per_j = (size_t)kCellElems * a.per_i;
     a.dmagic = (uint32_t)(((1ull << 32) + (uint64_t)D - 1) / (uint64_t)D);
+    a.scalars = w.scalars;
     a.L = L;
     a.pre = w.flat_pre;
     a.others = w.flat_others;
@@ -1225,8 +1246,7 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
     a.totinv = w.flat_totinv;
     a.slots = w.flat_slots;
     a.n_lists = lists;
-    int launched = 1;
-    k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, a.win, lists * kCellElems);
+    int launched = 0;
     uint32_t m = (uint32_t)L;
     const G1A *res;
     if (w.coop) {
@@ -1243,6 +1263,8 @@ int launch_phase_a_flat(const ProofWork &w, int n, cudaStream_t s) {
         }
         res = tree_result(nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1]);
     } else {
+        k_flat_digits<<<lists * kCellElems / 128, 128, 0, s>>>(w.scalars, w.flat_dig, a.win, lists * kCellElems);
+        launched++;
         res = run_tree_rounds<true>(a, nullptr, &m, kTreeTail, w.flat_buf[0], w.flat_buf[1], w.flat_blocks, s,
                                     &launched);
     }
