@@ -549,6 +549,10 @@ VK_HD Fp fp_one() { return Fp{VK_FP_ONE}; }
 #ifndef VKZG_FP_F64
 #define VKZG_FP_F64 0
 #endif
+// VKZG_FP_SQR_F64=1: squares alone on the FP64 pipe
+#ifndef VKZG_FP_SQR_F64
+#define VKZG_FP_SQR_F64 VKZG_FP_F64
+#endif
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_mul_call(Fp a, Fp b) {
 #if VKZG_FP_F64
@@ -578,7 +582,7 @@ VK_HD Fp fp_mul(const Fp &a, const Fp &b) {
 }
 #if defined(__CUDA_ARCH__) && !VKZG_FP_INLINE
 __device__ __noinline__ Fp fp_sqr_call(Fp a) {
-#if VKZG_FP_F64
+#if VKZG_FP_SQR_F64
     return f64::mont_sqr(a);
 #endif
     Fp r;
