@@ -1335,7 +1335,10 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         if (p->timing) collect_times(p->ev_rec, kRecoverStages, p->last_recover_ms);
         return VKZG_OK;
     }
-    // parts of the chunk on the side streams (after all earlier work of the prover's stream)
+    // parts of the chunk on the side streams (after all earlier work of the
+    // prover's stream, and after one copy of every blob's presence mask, so
+    // that the copy engine's queue holds only the parts' cells)
+    CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
     CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
     for (int k = 0; k < vkzg_prover::kSides; k++) CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
     for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
@@ -1347,7 +1350,6 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         w.out += off * ext;
         w.err += off;
         CK(cudaMemcpyAsync(w.cells, cells + off * ext, cnt * ext, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(w.present, present + (size_t)off * kCells, (size_t)cnt * kCells, cudaMemcpyHostToDevice, st));
         CK(launch_recover_timed(p->t, w, (int)cnt, st, nullptr));
         CK(cudaMemcpyAsync(out + off * ext, w.out, cnt * ext, cudaMemcpyDeviceToHost, st));
     }
