@@ -87,7 +87,7 @@ vkzg_result vkzg_b200_recover_cells_device_noalloc(vkzg_prover *p, uint8_t *d_ce
  * proofs only and leaves cells out (include/vkzg.h:16-18).  Same blob format and
  * error rules as vkzg_compute_proofs_batch; a chunk with an invalid blob leaves
  * its outputs untouched, except in vkzg_b200_compute_cells_batch from
- * page-locked buffers with 64 blobs or more in the chunk: that form copies
+ * page-locked buffers with 16 blobs or more in the chunk: that form copies
  * each part's cells out as the part finishes, before the error words are read,
  * and zeroes the chunk's cells when one of its blobs is invalid.
  */

@@ -1,5 +1,5 @@
 """Cells of blobs (vkzg_b200_compute_cells_batch) from page-locked host buffers
-at 64 blobs or more per chunk: the chunk runs as parts on side streams, each
+at 16 blobs or more per chunk: the chunk runs as parts on side streams, each
 copying in, computing and copying out.  Byte-exact against the pageable-buffer
 path and, for a sample, the CPU oracle; a chunk holding an invalid blob returns
 INVALID_BLOB and leaves that chunk's cells zeroed, since they went out before

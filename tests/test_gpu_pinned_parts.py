@@ -1,0 +1,71 @@
+"""Small and ragged chunks from page-locked host buffers.  From 16 blobs on, a
+recovery or cells chunk runs as parts of at least 8 blobs on side streams
+(copy in, kernel, copy out per part); 21 and 37 blobs give parts of unequal
+length.  Recovery round-trips the blobs' cells; cells match the single-call
+path from pageable memory and, for a sample, the CPU oracle."""
+import numpy as np
+import pytest
+
+import vkzg_b200
+from conftest import random_blobs
+
+pytestmark = pytest.mark.gpu
+
+EXT = 128 * 2048
+BLOB = 131072
+
+
+def _pinned(torch, data=None, n_bytes=None, fill=0):
+    t = torch.empty(n_bytes if data is None else data.size, dtype=torch.uint8).pin_memory()
+    if data is None:
+        t.fill_(fill)
+    else:
+        t.numpy()[:] = data.reshape(-1)
+    return t
+
+
+def _present(rng, n):
+    pats = [np.r_[np.ones(64), np.zeros(64)], np.tile([0, 1], 64), np.ones(128)]
+    while len(pats) < n:
+        p = np.zeros(128)
+        p[rng.choice(128, int(rng.integers(64, 128)), replace=False)] = 1
+        pats.append(p)
+    return np.stack(pats[:n]).astype(np.uint8)
+
+
+@pytest.mark.parametrize("n", [16, 21, 37])
+def test_pinned_cells_parts(n, oracle):
+    torch = pytest.importorskip("torch")
+    blobs = random_blobs(n, 900 + n).reshape(n, BLOB)
+    with vkzg_b200.Prover(max_batch_size=64) as p:
+        want = np.frombuffer(p.compute_cells_batch(blobs.tobytes(), n), np.uint8)
+        hb = _pinned(torch, blobs)
+        hc = _pinned(torch, n_bytes=n * EXT, fill=0xAB)
+        assert p.compute_cells_raw(hc.data_ptr(), hb.data_ptr(), n) == vkzg_b200.OK
+        got = hc.numpy().copy()
+    assert np.array_equal(got, want)
+    pick = [0, n - 1]
+    rc, ref = oracle.compute_cells(np.ascontiguousarray(blobs[pick]))
+    assert rc == 0
+    assert np.array_equal(ref.reshape(-1), got.reshape(n, EXT)[pick].reshape(-1))
+
+
+@pytest.mark.parametrize("n", [16, 21, 37])
+def test_pinned_recovery_parts_round_trip(n, oracle):
+    torch = pytest.importorskip("torch")
+    blobs = random_blobs(n, 950 + n).reshape(n, BLOB)
+    rng = np.random.default_rng(n)
+    present = _present(rng, n)
+    with vkzg_b200.Prover(max_batch_size=64) as p:
+        cells = np.frombuffer(p.compute_cells_batch(blobs.tobytes(), n), np.uint8).reshape(n, 128, 2048)
+        erased = cells.copy()
+        erased[present == 0] = rng.integers(0, 256, size=erased[present == 0].shape, dtype=np.uint8)
+        hi = _pinned(torch, erased)
+        hp = _pinned(torch, present)
+        ho = _pinned(torch, n_bytes=n * EXT, fill=0xCD)
+        assert p.recover_cells_raw(ho.data_ptr(), hi.data_ptr(), hp.data_ptr(), n) == vkzg_b200.OK
+        got = ho.numpy().reshape(n, 128, 2048).copy()
+    assert np.array_equal(got, cells)
+    rc, ref = oracle.compute_cells(np.ascontiguousarray(blobs[[n // 2]]))
+    assert rc == 0
+    assert np.array_equal(ref.reshape(-1), got[n // 2].reshape(-1))

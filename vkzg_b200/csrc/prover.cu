@@ -131,14 +131,16 @@ struct vkzg_prover {
     std::map<uint64_t, GraphRec> graphs;
     bool use_graphs = true;
     // side streams for host-buffer chunks, so that copies in, kernels and copies
-    // out overlap: a recovery chunk of 64 blobs or more runs as parts of at least
-    // kRecPartBlobs blobs (32 parts at 256 blobs: 116 k blobs/s through the C ABI;
-    // 8-blob parts beat 16- and 32-blob parts by 4-6 %), each copying in,
+    // out overlap: a recovery or cells chunk of kPartsFrom blobs or more runs as
+    // parts of at least kRecPartBlobs blobs (32 parts at 256 blobs: 116 k blobs/s
+    // of recovery through the C ABI; 8-blob parts beat 16- and 32-blob parts by
+    // 4-6 %; splitting from 16 blobs rather than 64 took recovery of 32 blobs from
+    // 0.62 to 0.52 ms and cells of 48 blobs from 0.60 to 0.52 ms), each copying in,
     // computing and copying out on side stream (part mod kSides); a proof chunk
     // uploads in kUploadPieces pieces (2 beat 4, 8 and 16: each piece adds a
     // launch of the per-blob front that fills only part of the GPU)
     static constexpr int kSides = 16;
-    static constexpr uint32_t kRecPartBlobs = 8, kRecMaxParts = 32;
+    static constexpr uint32_t kRecPartBlobs = 8, kRecMaxParts = 32, kPartsFrom = 16;
     static constexpr int kUploadPieces = 2;
     cudaStream_t side[kSides] = {};
     cudaEvent_t side_ev[kSides + 1] = {};
@@ -1325,7 +1327,7 @@ vkzg_result recover_chunk(vkzg_prover *p, uint8_t *out, const uint8_t *cells, co
         return VKZG_OK;
     }
     const uint32_t parts = std::min<uint32_t>(vkzg_prover::kRecMaxParts, n / vkzg_prover::kRecPartBlobs);
-    const uint32_t part = n >= 64 && p->side[0] ? (n + parts - 1) / parts : n;
+    const uint32_t part = n >= vkzg_prover::kPartsFrom && p->side[0] ? (n + parts - 1) / parts : n;
     if (p->timing || part == n) {
         CK(cudaMemcpyAsync(p->rw.cells, cells, n * ext, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(p->rw.present, present, (size_t)n * kCells, cudaMemcpyHostToDevice, s));
@@ -1577,7 +1579,7 @@ namespace {
 vkzg_result cells_chunk(vkzg_prover *p, uint8_t *cells, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
     const size_t ext = (size_t)kExtElems * 32;
-    if (!proofs && !p->timing && n >= 64 && p->side[0] && host_pinned(blobs) && host_pinned(cells)) {
+    if (!proofs && !p->timing && n >= vkzg_prover::kPartsFrom && p->side[0] && host_pinned(blobs) && host_pinned(cells)) {
         // cells only, page-locked buffers: parts of the chunk on the side
         // streams as recovery runs them (copy in, kernel, copy out per part), so
         // that the 384 KB per blob of copies overlap the kernels.  The cells go
