@@ -29,7 +29,10 @@ const char *vkzg_b200_prover_tables_source(const vkzg_prover *p);
  * from CUDA events (the reference's bench/profile.cpp wall-clocks each stage by
  * flushing the queue between dispatches, src/profile.h:12-28).  Fills up to
  * `cap` entries and returns the number of stages; names via
- * vkzg_b200_stage_name.  Timing is recorded only while enabled.
+ * vkzg_b200_stage_name.  Timing is recorded only while enabled.  The fold runs
+ * inside the ladder's launch, so "fold" reads ~0 and "ladder" holds both; on
+ * plans 3-4 the finish runs inside phase B's reduction (its Horner step and the
+ * finish share a launch), so "finish" reads ~0 and "reduce_b" holds both.
  */
 void vkzg_b200_set_stage_timing(vkzg_prover *p, int enabled);
 int vkzg_b200_last_stage_times(const vkzg_prover *p, int recovery, double *ms, int cap);

@@ -49,4 +49,4 @@ def test_cooperative_rounds_match_round_launches(monkeypatch, plan):
             launches[coop] = vkzg_b200.kernel_launches() - k0
             outs[coop] = out
     assert np.array_equal(outs["1"], outs["0"])
-    assert launches["1"] <= 14 < launches["0"]
+    assert launches["1"] <= 10 < launches["0"]

@@ -8,15 +8,16 @@
 //                        shared memory, fixed-base bucket accumulation over the
 //                        position table                     (k_phase_a_sort, k_phase_a)
 //   4 k_reduce           sum_k k * B_k, 8 lanes per output  (k_bucket_reduce)
-//   5 k_fold_points      u+- = u[j] +- u[j+64], and for plans 3-4 once more on
+//   5 k_ladder (fold)    u+- = u[j] +- u[j+64], and for plans 3-4 twice more on
 //                        the cyclic half: the convolution's parts (k_fold_ladder)
-//   6 k_ladder           L[j][d] = 2^(8d) u[j], d < 16      (k_ladder, d < 32: the
+//   6 k_ladder           L[j][d] = 2^(8d) v[j], d < 16      (k_ladder, d < 32: the
 //                        taps are split as k1 + k2 z^2 and slots 16..31 read phi(L))
 //   7 k_normalize        Jacobian -> affine, block batch inversion, phi images
 //                                                           (k_normalize)
 //   8 k_phase_b          split-circulant bucket MSM with the fixed taps (k_phase_b_split)
 //   4'k_reduce
-//   9 k_finish           unfold the parts (C+ +- C-), normalise, compress, write slot brev7(a)
+//   9 k_finish           unfold the parts (C+ +- C-), normalise, compress, write slot brev7(a);
+//                        plans 3-4: k_finish_horner, phase B's Horner step first
 //                                                           (k_combine_split, k_normalize, k_compress_proofs)
 #include "bucket_sum.cuh"
 #include "device_util.cuh"
@@ -198,44 +199,45 @@ __global__ void __launch_bounds__(kReduceThreads) k_reduce(const G1J *__restrict
     st_vec(&out[o], g1_add(w, acc));
 }
 
-// ---------------------------------------------------------------- stage 5
-__global__ void __launch_bounds__(128) k_ladder(const G1J *__restrict__ u, G1J *ladder, int n_points) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= n_points) return;
-    G1J acc = ld_vec(&u[gid]);
-    G1J *dst = ladder + (size_t)gid * kLadderDigits;
+// ---------------------------------------------------------------- stages 5-6
+// One block per blob, one thread per point.  First the parts of phase B's
+// convolution (PartLayout) in shared memory: level l folds the cyclic vector v
+// of 2m = 256 >> l points into v[j] + v[j + m] (the next cyclic vector, slots
+// [0, m)) and v[j] - v[j + m] (the negacyclic part, slots [m, 2m)); one level is
+// the reference's split of the circulant, applied to u before the ladder
+// instead of to every ladder row.  Then each thread doubles its folded point
+// along the ladder L[j][d] = 2^(8d) v[j], d < kLadderDigits.  The folded points
+// stay in shared memory: nothing else reads them.
+//
+// One level of butterflies over v[0, 2m): thread t < m writes v[t] + v[t + m],
+// thread m <= t < 2m writes v[t - m] - v[t], so that a level costs one addition
+// of latency rather than two.
+__device__ __forceinline__ void butterfly_level(G1J *v, int t, int m) {
+    G1J r;
+    if (t < 2 * m) {
+        const int j = t < m ? t : t - m;
+        const G1J y = ld_vec(&v[j + m]);
+        r = g1_add(ld_vec(&v[j]), t < m ? y : g1_neg(y));
+    }
+    __syncthreads();
+    if (t < 2 * m) st_vec(&v[t], r);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCells) k_ladder(const G1J *__restrict__ u, G1J *ladder, int levels) {
+    __shared__ G1J v[kCells];
+    const int b = blockIdx.x, t = threadIdx.x;
+    st_vec(&v[t], ld_vec(&u[(size_t)b * kCells + t]));
+    __syncthreads();
+    for (int l = 1; l <= levels; l++) butterfly_level(v, t, kCells >> l);
+    G1J acc = ld_vec(&v[t]);
+    G1J *dst = ladder + ((size_t)b * kCells + t) * kLadderDigits;
     for (int d = 0; d < kLadderDigits; d++) {
         st_vec(&dst[d], acc);
         if (d + 1 < kLadderDigits)
 #pragma unroll 1
             for (int q = 0; q < 8; q++) acc = g1_dbl_inl(acc);
     }
-}
-
-// ---------------------------------------------------------------- stage 6
-// The parts of phase B's convolution (PartLayout), in place per blob: level l
-// folds the cyclic vector v of 2m = 256 >> l points into v[j] + v[j + m] (the
-// next cyclic vector, slots [0, m)) and v[j] - v[j + m] (the negacyclic part,
-// slots [m, 2m)).  One level is the reference's k_fold_ladder split, applied to
-// u before the ladder instead of to every ladder row.
-__global__ void __launch_bounds__(kHalf) k_fold_points(G1J *points, int levels) {
-    __shared__ G1J v[kCells];
-    const int b = blockIdx.x, t = threadIdx.x;
-    G1J *pb = points + (size_t)b * kCells;
-    st_vec(&v[t], ld_vec(&pb[t]));
-    st_vec(&v[t + kHalf], ld_vec(&pb[t + kHalf]));
-    __syncthreads();
-    for (int l = 1; l <= levels; l++) {
-        const int m = kCells >> l;
-        if (t < m) {
-            const G1J x = ld_vec(&v[t]), y = ld_vec(&v[t + m]);
-            st_vec(&v[t], g1_add(x, y));
-            st_vec(&v[t + m], g1_sub(x, y));
-        }
-        __syncthreads();
-    }
-    st_vec(&pb[t], ld_vec(&v[t]));
-    st_vec(&pb[t + kHalf], ld_vec(&v[t + kHalf]));
 }
 
 // ---------------------------------------------------------------- stage 7
@@ -294,23 +296,12 @@ __global__ void __launch_bounds__(kBuckets) k_phase_b(const G1A *__restrict__ la
 
 // ---------------------------------------------------------------- stage 9
 // The parts' results unfold level by level, innermost first (the inverse
-// butterflies of k_fold_points; the taps carry the factors 1/2): y[a] = C+[a] +
-// C-[a], y[a + m] = C+[a] - C-[a].
-__global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, uint8_t *proofs, int levels) {
-    __shared__ Fp tree[2 * kCells];
-    __shared__ G1J outp[kCells];
-    const int b = blockIdx.x, t = threadIdx.x;
-    st_vec(&outp[t], ld_vec(&c[(size_t)b * kCells + t]));
+// butterflies of k_ladder's fold; the taps carry the factors 1/2): y[a] = C+[a] +
+// C-[a], y[a + m] = C+[a] - C-[a].  outp holds the blob's 128 results, one per
+// thread of the block.
+__device__ __forceinline__ void finish_blob(G1J *outp, Fp *tree, uint8_t *proofs, int b, int t, int levels) {
     __syncthreads();
-    for (int l = levels; l >= 1; l--) {
-        const int m = kCells >> l;
-        if (t < m) {
-            const G1J cp = ld_vec(&outp[t]), cm = ld_vec(&outp[t + m]);
-            st_vec(&outp[t], g1_add(cp, cm));
-            st_vec(&outp[t + m], g1_sub(cp, cm));
-        }
-        __syncthreads();
-    }
+    for (int l = levels; l >= 1; l--) butterfly_level(outp, t, kCells >> l);
     const G1J p = ld_vec(&outp[t]);
     const bool inf = fp_is_zero(p.z);
     const Fp zi = block_batch_inverse_fp<kCells>(inf ? fp_one() : p.z, tree);
@@ -330,6 +321,14 @@ __global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, ui
     dst[0] = e4[0];
     dst[1] = e4[1];
     dst[2] = e4[2];
+}
+
+__global__ void __launch_bounds__(kCells) k_finish(const G1J *__restrict__ c, uint8_t *proofs, int levels) {
+    __shared__ Fp tree[2 * kCells];
+    __shared__ G1J outp[kCells];
+    const int b = blockIdx.x, t = threadIdx.x;
+    st_vec(&outp[t], ld_vec(&c[(size_t)b * kCells + t]));
+    finish_blob(outp, tree, proofs, b, t, levels);
 }
 
 // ------------------------------------------- batch-affine phase A / phase B
@@ -2129,6 +2128,18 @@ __global__ void __launch_bounds__(128) k_flatr_horner(FlatRArgs a, G1J *out) {
     st_vec(&out[o], red_horner([&](int x) { return ld_vec(red_slot(a, o, x)); }));
 }
 
+// Phase B's Horner step and stage 9 in one launch (plans 3-4): a block is one
+// blob and its 128 threads the blob's outputs, so each thread's Horner result
+// goes to shared memory for the unfolding instead of through HBM.
+__global__ void __launch_bounds__(kCells) k_finish_horner(FlatRArgs a, uint8_t *proofs, int levels) {
+    __shared__ Fp tree[2 * kCells];
+    __shared__ G1J outp[kCells];
+    const int b = blockIdx.x, t = threadIdx.x;
+    const uint32_t o = (uint32_t)b * kCells + (uint32_t)t;
+    st_vec(&outp[t], red_horner([&](int x) { return ld_vec(red_slot(a, o, x)); }));
+    finish_blob(outp, tree, proofs, b, t, levels);
+}
+
 VKZG_COOP_FN void coop_flatr_pass1(FlatRArgs a, int r, RedRound &rr, uint32_t gl, uint32_t NL) {
     flatr_pass1_body(a, r, rr, gl, NL);
 }
@@ -2151,7 +2162,10 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_reduce(
     }
 }
 
-int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_out, cudaStream_t s) {
+// proofs non-null: the Horner step runs inside stage 9 (k_finish_horner), which
+// writes the compressed proofs; else it writes the reduction's results to out.
+int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_out, cudaStream_t s,
+                       uint8_t *proofs = nullptr) {
     // the schedule's round count, computed once (thread-safe static initialisation:
     // serving lanes launch from several threads)
     static const int rounds = [] {
@@ -2180,7 +2194,8 @@ int launch_reduce_flat(const ProofWork &w, const G1A *buckets, G1J *out, int n_o
         }
         launched += 3 * rounds;
     }
-    k_flatr_horner<<<(n_out + 127) / 128, 128, 0, s>>>(a, out);
+    if (proofs) k_finish_horner<<<n_out / kCells, kCells, 0, s>>>(a, proofs, kPartLevels);
+    else k_flatr_horner<<<(n_out + 127) / 128, 128, 0, s>>>(a, out);
     return launched;
 }
 
@@ -2325,10 +2340,12 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         return launch_proofs_timed(t, w2, n, s, ev, skip_front);
     }
     const bool hier = w.plan == 1 || w.plan == 3 || w.plan == 4;
-    int launched = skip_front ? 8 : 10;
+    // coefficients, circulant, phase A, its reduction, ladder, normalisation,
+    // phase B, its reduction, finish; the launchers add their extra rounds
+    int launched = skip_front ? 7 : 9;
     const int ba_grid = std::min(w.ba_blocks, (n_out / kWarpOutputs + kBAWarps - 1) / kBAWarps);
-    auto reduce = [&]() {
-        if (flatb) launched += launch_reduce_flat(w, w.bucket_aff, w.points, n_out, s) - 1;
+    auto reduce = [&](uint8_t *proofs) {
+        if (flatb) launched += launch_reduce_flat(w, w.bucket_aff, w.points, n_out, s, proofs) - 1;
         else if (!affine) k_reduce<<<red_blocks, kReduceThreads, 0, s>>>(w.buckets, w.points, n_out);
         else if (hier)
             k_reduce_hier<<<(n_out + kRedOutputs - 1) / kRedOutputs, kRedThreads, 0, s>>>(w.bucket_aff, w.points,
@@ -2348,13 +2365,13 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
         k_phase_a<<<dim3(kCells, n), kBuckets, 0, s>>>(w.scalars, t.pos, w.buckets);
     }
     mark();
-    if (!comb) reduce();
+    if (!comb) reduce(nullptr);
     mark();
-    // plans 3-4 split phase B into the kPartLevels parts, plans 0-2 into two halves
+    // plans 3-4 split phase B into the kPartLevels parts, plans 0-2 into two
+    // halves; the fold (stage 5) runs inside the ladder's launch
     const int levels = flatb ? kPartLevels : 1;
-    k_fold_points<<<n, kHalf, 0, s>>>(w.points, levels);
     mark();
-    k_ladder<<<(n_out + 127) / 128, 128, 0, s>>>(w.points, w.ladder, n_out);
+    k_ladder<<<n, kCells, 0, s>>>(w.points, w.ladder, levels);
     mark();
     if (flatb) launched += launch_normalize_flat(w, n, s) - 1;
     else k_normalize<<<(n_lad + kNormThreads - 1) / kNormThreads, kNormThreads, 0, s>>>(w.ladder, w.ladder_aff, n_lad);
@@ -2374,9 +2391,11 @@ cudaError_t launch_proofs_timed(const DeviceTables &t, const ProofWork &w, int n
                                                        t.tap_perm[1], w.buckets);
     }
     mark();
-    reduce();
+    // plans 3-4: phase B's Horner step runs inside stage 9's launch
+    reduce(flatb ? w.proofs : nullptr);
     mark();
-    k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs, levels);
+    if (flatb) launched--;
+    else k_finish<<<n, kCells, 0, s>>>(w.points, w.proofs, levels);
     mark();
     count_launches(launched);
     return cudaGetLastError();

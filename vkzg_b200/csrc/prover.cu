@@ -924,8 +924,8 @@ bool ensure_flat_b(vkzg_prover *p) {
     }
     w.flat_slots = z.slots;
     w.flat_blocks = z.blocks;
-    // $VKZG_COOP=1: the rounds of each phase as one cooperative launch (12
-    // launches per proof step instead of ~62); measured 5 % slower than the
+    // $VKZG_COOP=1: the rounds of each phase as one cooperative launch (10
+    // launches per proof step instead of ~60); measured 3 % slower than the
     // captured graph of separate launches (the round loop's state pushes the
     // passes past 128 registers), so it is not the default
     const char *coop = getenv("VKZG_COOP");
