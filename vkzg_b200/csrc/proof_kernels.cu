@@ -1166,18 +1166,18 @@ __global__ void __launch_bounds__(kFlatThreads, kFlatBlocksPerSM) k_coop_tree(Fl
         coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
         if (!grid_sync(g)) return;
         coop_flat_pass2<true>(a, io, m, gl, NL);
-        return;
-    }
-    while (m > stop) {
-        coop_flat_pass1<false>(a, io, m, gl, NL);
-        if (!grid_sync(g)) return;
-        coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
-        if (!grid_sync(g)) return;
-        coop_flat_pass2<false>(a, io, m, gl, NL);
-        io.src = io.dst;
-        io.dst = io.dst == buf0 ? buf1 : buf0;
-        m = (m + 1) >> 1;
-        if (m > stop && !grid_sync(g)) return;
+    } else {
+        while (m > stop) {
+            coop_flat_pass1<false>(a, io, m, gl, NL);
+            if (!grid_sync(g)) return;
+            coop_invert(a.tot, a.totinv, NL >> 5, gl, NL);
+            if (!grid_sync(g)) return;
+            coop_flat_pass2<false>(a, io, m, gl, NL);
+            io.src = io.dst;
+            io.dst = io.dst == buf0 ? buf1 : buf0;
+            m = (m + 1) >> 1;
+            if (m > stop && !grid_sync(g)) return;
+        }
     }
 }
 
