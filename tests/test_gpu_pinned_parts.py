@@ -2,7 +2,9 @@
 recovery or cells chunk runs as parts of at least 8 blobs on side streams
 (copy in, kernel, copy out per part); 21 and 37 blobs give parts of unequal
 length.  Recovery round-trips the blobs' cells; cells match the single-call
-path from pageable memory and, for a sample, the CPU oracle."""
+path from pageable memory and, for a sample, the CPU oracle.  Calls larger
+than max_batch_size keep the chunk rule on these paths: chunks before a
+failing one are written."""
 import numpy as np
 import pytest
 
@@ -69,3 +71,51 @@ def test_pinned_recovery_parts_round_trip(n, oracle):
     rc, ref = oracle.compute_cells(np.ascontiguousarray(blobs[[n // 2]]))
     assert rc == 0
     assert np.array_equal(ref.reshape(-1), got[n // 2].reshape(-1))
+
+
+def test_pinned_recovery_chunks_keep_earlier_on_error():
+    """Chunks of max_batch_size blobs (16 here: 16, 16, 5), each run as parts: a
+    blob with 65 cells missing in the second chunk returns BADARGS before that
+    chunk's device work (src/vkzg.cpp:1093-1105), with the first chunk's cells
+    written and the rest of the output untouched."""
+    torch = pytest.importorskip("torch")
+    n = 37
+    blobs = random_blobs(n, 990).reshape(n, BLOB)
+    rng = np.random.default_rng(99)
+    present = _present(rng, n)
+    present[20] = 0
+    present[20, :63] = 1
+    with vkzg_b200.Prover(max_batch_size=16) as p:
+        cells = np.frombuffer(p.compute_cells_batch(blobs.tobytes(), n), np.uint8).reshape(n, 128, 2048)
+        hi = _pinned(torch, cells)
+        hp = _pinned(torch, present)
+        ho = _pinned(torch, n_bytes=n * EXT, fill=0xCD)
+        assert p.recover_cells_raw(ho.data_ptr(), hi.data_ptr(), hp.data_ptr(), n) == vkzg_b200.ERR_BADARGS
+        got = ho.numpy().reshape(n, 128, 2048)
+        assert np.array_equal(got[:16], cells[:16])
+        assert (got[16:] == 0xCD).all()
+        # the prover stays usable: the same call without the bad blob
+        present[20, 63] = 1
+        hp2 = _pinned(torch, present)
+        assert p.recover_cells_raw(ho.data_ptr(), hi.data_ptr(), hp2.data_ptr(), n) == vkzg_b200.OK
+        assert np.array_equal(ho.numpy().reshape(n, 128, 2048), cells)
+
+
+def test_pinned_cells_chunks_keep_earlier_on_error(golden_proofs):
+    """Cells in chunks of 16 (16, 16, 5) from page-locked buffers: an invalid blob
+    in the second chunk leaves the first chunk's cells written, the second
+    chunk's zeroed (its parts' cells went out before the error words were read)
+    and the third untouched."""
+    torch = pytest.importorskip("torch")
+    n = 37
+    blobs = random_blobs(n, 991).reshape(n, BLOB)
+    blobs[21] = golden_proofs["invalid_blob_0"].reshape(-1)
+    with vkzg_b200.Prover(max_batch_size=16) as p:
+        want = np.frombuffer(p.compute_cells_batch(blobs[:16].tobytes(), 16), np.uint8)
+        hb = _pinned(torch, blobs)
+        hc = _pinned(torch, n_bytes=n * EXT, fill=0xAB)
+        assert p.compute_cells_raw(hc.data_ptr(), hb.data_ptr(), n) == vkzg_b200.ERR_INVALID_BLOB
+        got = hc.numpy()
+        assert np.array_equal(got[:16 * EXT], want)
+        assert not got[16 * EXT:32 * EXT].any()
+        assert (got[32 * EXT:] == 0xAB).all()
