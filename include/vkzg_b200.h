@@ -122,7 +122,10 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * grid-wide rounds; 4 = phase A as plan 1, phase B as plan 3 (no digit
  * table).  The first chunk of each
  * power-of-two size class is timed under all plans and the fastest is kept
- * (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).
+ * (also in $VKZG_TUNE_CACHE when set; $VKZG_PLAN forces a plan).  Plan 3 is
+ * timed at every size class of a prover whose max_batch_size is 16 or more
+ * (below 16 blobs with the fewest windows the budget allows); for a smaller
+ * prover the tuner leaves the digit table out ($VKZG_PLAN=3 still forces it).
  * vkzg_b200_autotune tunes every size class up to max_blobs (0 = the prover's
  * max_batch_size) on seeded synthetic blobs; vkzg_b200_tuning_table reports the
  * decisions (size class, plan, and VKZG_B200_PLANS times in ms per class, -1
@@ -137,9 +140,10 @@ vkzg_result vkzg_b200_recover_cells_and_proofs_batch(vkzg_prover *p, uint8_t *ce
  * 3.2 GB; 26: 9.7 GB; 24: 16.1 GB; 23: 20.9 GB; 22: 29.0 GB; 21: 40.3 GB; 20:
  * 58.0 GB; 19: 90.2 GB; 18: 141.7 GB); fewer windows mean fewer additions per
  * output (64 D - 1).  Its size is bounded by a budget: $VKZG_COMB_BUDGET_GB
- * (GiB, default 20, so D >= 24 unless raised); a serving loop uses its
- * table_budget_bytes.  When plan 3 is tuned, the fewest windows whose table
- * fits the budget and the next two counts are each built and timed, and the
+ * (GiB, default 20, so D >= 23 unless raised); a serving loop uses its
+ * table_budget_bytes.  When plan 3 is tuned at 16 blobs or more, the fewest
+ * windows whose table fits the budget and the next two counts are each built
+ * and timed, and the
  * fastest is kept (and remembered in $VKZG_TUNE_CACHE); $VKZG_COMB_WINDOWS pins
  * D (18..32), $VKZG_COMB_BITS pins the widest window instead (D =
  * ceil(256 / bits)), and 0 in either means no digit table.
