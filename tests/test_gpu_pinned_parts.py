@@ -119,3 +119,26 @@ def test_pinned_cells_chunks_keep_earlier_on_error(golden_proofs):
         assert np.array_equal(got[:16 * EXT], want)
         assert not got[16 * EXT:32 * EXT].any()
         assert (got[32 * EXT:] == 0xAB).all()
+
+
+@pytest.mark.parametrize("n", [16, 37])
+@pytest.mark.parametrize("pin_in,pin_out", [(False, False), (True, False), (False, True)])
+def test_pageable_recovery_parts_round_trip(n, pin_in, pin_out):
+    """Pageable cells or output (16 blobs or more): 8-blob parts through the
+    prover's pinned staging buffers, dealt to host threads; every combination of
+    a pageable and a page-locked side recovers the blobs' cells."""
+    torch = pytest.importorskip("torch")
+    blobs = random_blobs(n, 970 + n).reshape(n, BLOB)
+    rng = np.random.default_rng(n + 7)
+    present = _present(rng, n)
+    with vkzg_b200.Prover(max_batch_size=64) as p:
+        cells = np.frombuffer(p.compute_cells_batch(blobs.tobytes(), n), np.uint8).reshape(n, 128, 2048)
+        erased = cells.copy()
+        erased[present == 0] = 0
+        src = _pinned(torch, erased) if pin_in else np.ascontiguousarray(erased.reshape(-1))
+        dst = _pinned(torch, n_bytes=n * EXT, fill=0xCD) if pin_out else np.full(n * EXT, 0xCD, np.uint8)
+        src_ptr = src.data_ptr() if pin_in else src
+        dst_ptr = dst.data_ptr() if pin_out else dst
+        assert p.recover_cells_raw(dst_ptr, src_ptr, present, n) == vkzg_b200.OK
+        got = (dst.numpy() if pin_out else dst).reshape(n, 128, 2048)
+        assert np.array_equal(got, cells)
