@@ -142,3 +142,29 @@ def test_pageable_recovery_parts_round_trip(n, pin_in, pin_out):
         assert p.recover_cells_raw(dst_ptr, src_ptr, present, n) == vkzg_b200.OK
         got = (dst.numpy() if pin_out else dst).reshape(n, 128, 2048)
         assert np.array_equal(got, cells)
+
+
+@pytest.mark.parametrize("n", [40, 100])
+def test_pageable_proof_upload_parts(n, monkeypatch, oracle, mainnet_tables):
+    """Pageable blobs (16 or more) go up through the pinned staging in parts
+    dealt to host threads; 100 blobs take the two-piece path (parts of 9 blobs,
+    the last of 1, each piece's front waiting for the parts that hold it), 40
+    the single upload.  Proofs equal the page-locked call's and, for a sample,
+    the CPU oracle's."""
+    torch = pytest.importorskip("torch")
+    monkeypatch.delenv("VKZG_TABLES_PATH", raising=False)
+    monkeypatch.setenv("VKZG_PLAN", "3")
+    monkeypatch.setenv("VKZG_COMB_WINDOWS", "26")
+    blobs = random_blobs(n, 960 + n).reshape(n, BLOB)
+    with vkzg_b200.Prover(max_batch_size=128) as p:
+        out = np.zeros(n * 6144, np.uint8)
+        for _ in range(2):  # the first call also captures the pipeline's graph
+            out[:] = 0
+            assert p.compute_proofs_raw(out, blobs, n) == vkzg_b200.OK
+        hb = _pinned(torch, blobs)
+        hp = _pinned(torch, n_bytes=n * 6144)
+        assert p.compute_proofs_raw(hp.data_ptr(), hb.data_ptr(), n) == vkzg_b200.OK
+        assert np.array_equal(out, hp.numpy())
+    rc, want = oracle.compute_proofs(mainnet_tables, np.ascontiguousarray(blobs[[0, n - 1]]))
+    assert rc == 0
+    assert np.array_equal(want.reshape(-1), out.reshape(n, 6144)[[0, n - 1]].reshape(-1))

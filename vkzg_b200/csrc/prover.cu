@@ -1186,30 +1186,11 @@ bool host_pinned(const void *ptr) {
     return a.type == cudaMemoryTypeHost;
 }
 
-// memcpy on up to 8 host threads (one per 4 MB, at most half the cores).
 // Host threads of pageable recovery: one per hardware thread, at most kSides
 // (a 64 MB memcpy on a 16-thread host of the B200 pool: 15.7 GB/s on one
 // thread, 47 on 8, 77 on 16).
 unsigned stage_threads() {
     return std::max(1u, std::min<unsigned>(vkzg_prover::kSides, std::thread::hardware_concurrency()));
-}
-
-// A pageable proof upload's copy into the staging: half the hardware threads,
-// at most 8, 4 MB or more each (16 threads of 2 MB made the 256-blob proof call
-// from pageable blobs 0.5 ms slower).
-void host_copy(void *dst, const void *src, size_t n) {
-    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
-    const size_t threads = std::min<size_t>(std::min(8u, hw / 2), n >> 22);
-    if (threads <= 1) {
-        memcpy(dst, src, n);
-        return;
-    }
-    const size_t per = ((n + threads - 1) / threads + 4095) & ~(size_t)4095;
-    std::vector<std::thread> ts;
-    for (size_t t = 1; t < threads && t * per < n; t++)
-        ts.emplace_back([=] { memcpy((uint8_t *)dst + t * per, (const uint8_t *)src + t * per, std::min(per, n - t * per)); });
-    memcpy(dst, src, std::min(per, n));
-    for (auto &t : ts) t.join();
 }
 
 // The staging buffers, allocated on first use; false when pinned memory is
@@ -1239,34 +1220,81 @@ static bool upload_in_pieces(vkzg_prover *p, uint32_t n) {
     return n >= 64 && p->side[0] && p->use_graphs && !p->timing && tuned(p, n);
 }
 
+// Pageable blobs into the proof working set through the pinned staging: parts
+// of kRecPartBlobs blobs or more dealt to host threads (half the hardware
+// threads, at most 8; parts t, t + T, ... to thread t, on side stream t), each
+// part copied into the staging and its copy up enqueued at once, so that the
+// DMA of the first parts runs while later parts are still being copied on the
+// host (all 16 hardware threads, copying 2 MB pieces, made the 256-blob call
+// 0.5 ms slower than 8).  The copies start after the prover stream's earlier work (which may
+// still read the blobs).  On return every copy is enqueued, part k (blobs
+// [k part, (k + 1) part)) is up when p->part_ev[k] is, and *part is the part
+// size in blobs.
+vkzg_result staged_upload(vkzg_prover *p, const uint8_t *blobs, uint32_t n, uint32_t *part_out) {
+    const uint32_t parts = std::max<uint32_t>(1, std::min<uint32_t>(vkzg_prover::kRecMaxParts, n / vkzg_prover::kRecPartBlobs));
+    const uint32_t part = (n + parts - 1) / parts;
+    const uint32_t used = (n + part - 1) / part;
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const uint32_t T = std::min<uint32_t>(used, std::min(8u, hw / 2));
+    CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], p->stream));
+    for (uint32_t t = 0; t < T; t++) CK(cudaStreamWaitEvent(p->side[t], p->side_ev[vkzg_prover::kSides], 0));
+    auto run_thread = [&](uint32_t t) -> vkzg_result {
+        if (cudaSetDevice(p->device) != cudaSuccess) return VKZG_ERR_GPU;
+        for (uint32_t k = t; k < used; k += T) {
+            const size_t off = (size_t)k * part * kBlobBytes, bytes = (size_t)std::min(part, n - k * part) * kBlobBytes;
+            memcpy(p->stage_in + off, blobs + off, bytes);
+            CK(cudaMemcpyAsync(p->pw.blobs + off, p->stage_in + off, bytes, cudaMemcpyHostToDevice, p->side[t]));
+            CK(cudaEventRecord(p->part_ev[k], p->side[t]));
+        }
+        return VKZG_OK;
+    };
+    std::vector<vkzg_result> rcs(T, VKZG_OK);
+    std::vector<std::thread> ts;
+    for (uint32_t t = 1; t < T; t++) ts.emplace_back([&, t] { rcs[t] = run_thread(t); });
+    rcs[0] = run_thread(0);
+    for (auto &t : ts) t.join();
+    for (vkzg_result rc : rcs)
+        if (rc != VKZG_OK) return rc;
+    *part_out = part;
+    return VKZG_OK;
+}
+
 vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, uint32_t n) {
     cudaStream_t s = p->stream;
-    // pageable blobs: through the pinned staging buffer (piece by piece below)
+    // pageable blobs: through the pinned staging buffer in parts (staged_upload)
     const bool staged = n >= 16 && !host_pinned(blobs) && ensure_stage(p);
-    if (staged && !upload_in_pieces(p, n)) {
-        host_copy(p->stage_in, blobs, (size_t)n * kBlobBytes);
-        blobs = p->stage_in;
-    }
+    uint32_t spart = 0;
+    // the prover stream waits for the staged parts holding blobs [from, to)
+    auto wait_parts = [&](uint32_t from, uint32_t to) -> cudaError_t {
+        for (uint32_t k = from / spart; k * spart < to; k++) {
+            const cudaError_t e = cudaStreamWaitEvent(s, p->part_ev[k], 0);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
     if (upload_in_pieces(p, n)) {
         p->pw.plan = plan_for(p, n);
         const vkzg_prover::GraphRec *rec = nullptr;
         CK(proof_graph(p, p->pw, n, &rec, true));
+        if (staged) {
+            const vkzg_result rc = staged_upload(p, blobs, n, &spart);
+            if (rc != VKZG_OK) return rc;
+        }
         CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
         // the pieces' copies start after the stream's earlier work (which may still read the blobs)
-        CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
+        if (!staged) CK(cudaEventRecord(p->side_ev[vkzg_prover::kSides], s));
         const uint32_t part = (n + vkzg_prover::kUploadPieces - 1) / vkzg_prover::kUploadPieces;
         for (uint32_t off = 0, k = 0; off < n; off += part, k++) {
             const uint32_t cnt = std::min(part, n - off);
-            const uint8_t *src = blobs + (size_t)off * kBlobBytes;
             if (staged) {
-                host_copy(p->stage_in + (size_t)off * kBlobBytes, src, (size_t)cnt * kBlobBytes);
-                src = p->stage_in + (size_t)off * kBlobBytes;
+                CK(wait_parts(off, off + cnt));
+            } else {
+                CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
+                CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, blobs + (size_t)off * kBlobBytes,
+                                   (size_t)cnt * kBlobBytes, cudaMemcpyHostToDevice, p->side[k]));
+                CK(cudaEventRecord(p->side_ev[k], p->side[k]));
+                CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
             }
-            CK(cudaStreamWaitEvent(p->side[k], p->side_ev[vkzg_prover::kSides], 0));
-            CK(cudaMemcpyAsync(p->pw.blobs + (size_t)off * kBlobBytes, src, (size_t)cnt * kBlobBytes,
-                               cudaMemcpyHostToDevice, p->side[k]));
-            CK(cudaEventRecord(p->side_ev[k], p->side[k]));
-            CK(cudaStreamWaitEvent(s, p->side_ev[k], 0));
             CK(launch_proofs_front(p->t, p->pw, (int)off, (int)cnt, s));
         }
         if (rec) {
@@ -1276,7 +1304,13 @@ vkzg_result proofs_chunk(vkzg_prover *p, uint8_t *proofs, const uint8_t *blobs, 
             CK(launch_proofs_timed(p->t, p->pw, (int)n, s, nullptr, true));
         }
     } else {
-        CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
+        if (staged) {
+            const vkzg_result rc = staged_upload(p, blobs, n, &spart);
+            if (rc != VKZG_OK) return rc;
+            CK(wait_parts(0, n));
+        } else {
+            CK(cudaMemcpyAsync(p->pw.blobs, blobs, (size_t)n * kBlobBytes, cudaMemcpyHostToDevice, s));
+        }
         CK(cudaMemsetAsync(p->pw.err, 0, n * sizeof(uint32_t), s));
         if (!tuned(p, n)) {
             const vkzg_result rc = tune_chunk(p, p->pw, n);
