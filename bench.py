@@ -795,7 +795,7 @@ def main():
                 assert prover.compute_cells_raw(out, blobs, args.blobs) == 0
         else:
             # device buffers: one launch of all the blobs (host buffers of 16
-            # blobs or more would be staged in slices)
+            # blobs or more would be staged in parts)
             import torch
             cells, present = make_recovery(args.blobs, 6)
             d_cells = torch.from_numpy(cells).cuda()
