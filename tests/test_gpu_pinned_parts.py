@@ -168,3 +168,37 @@ def test_pageable_proof_upload_parts(n, monkeypatch, oracle, mainnet_tables):
     rc, want = oracle.compute_proofs(mainnet_tables, np.ascontiguousarray(blobs[[0, n - 1]]))
     assert rc == 0
     assert np.array_equal(want.reshape(-1), out.reshape(n, 6144)[[0, n - 1]].reshape(-1))
+
+
+@pytest.mark.parametrize("n", [16, 37])
+def test_pageable_cells_parts(n, golden_proofs):
+    """Cells (and cells + proofs) with pageable blobs and output, 16 blobs or
+    more: the blobs go up and the cells come down through the pinned staging in
+    parts on host threads.  Bytes equal the page-locked call's; an invalid blob
+    leaves a pageable output untouched (the cells come down only after the
+    error words are read)."""
+    torch = pytest.importorskip("torch")
+    blobs = random_blobs(n, 940 + n).reshape(n, BLOB)
+    with vkzg_b200.Prover(max_batch_size=64) as p:
+        hb = _pinned(torch, blobs)
+        hc = _pinned(torch, n_bytes=n * EXT)
+        assert p.compute_cells_raw(hc.data_ptr(), hb.data_ptr(), n) == vkzg_b200.OK
+        want = hc.numpy().copy()
+        out = np.full(n * EXT, 0xAB, np.uint8)
+        assert p.compute_cells_raw(out, np.ascontiguousarray(blobs.reshape(-1)), n) == vkzg_b200.OK
+        assert np.array_equal(out, want)
+        out[:] = 0xAB  # page-locked blobs, pageable cells
+        assert p.compute_cells_raw(out, hb.data_ptr(), n) == vkzg_b200.OK
+        assert np.array_equal(out, want)
+        cells2 = np.zeros(n * EXT, np.uint8)
+        proofs2 = np.zeros(n * 6144, np.uint8)
+        assert p.compute_cells_and_proofs_raw(cells2, proofs2, np.ascontiguousarray(blobs.reshape(-1)), n) == vkzg_b200.OK
+        assert np.array_equal(cells2, want)
+        pw = np.zeros(n * 6144, np.uint8)
+        assert p.compute_proofs_raw(pw, blobs, n) == vkzg_b200.OK
+        assert np.array_equal(proofs2, pw)
+        bad = blobs.copy()
+        bad[n // 2] = golden_proofs["invalid_blob_0"].reshape(-1)
+        out[:] = 0xAB
+        assert p.compute_cells_raw(out, np.ascontiguousarray(bad.reshape(-1)), n) == vkzg_b200.ERR_INVALID_BLOB
+        assert (out == 0xAB).all()
